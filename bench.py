@@ -1,0 +1,322 @@
+#!/usr/bin/env python
+"""Throughput of the `bwa aln` search on one or more B200s: reads/s on the aDNA workload.
+
+Workload (the reference's aDNA-batched configuration, synthetic and seeded): a 100 Mbp reference at 45% GC
+in 10 contigs with 5% interspersed 300 bp repeat families (copies at 10% divergence), indexed in BWA format;
+2,000,000 single-end reads per GPU with log-normal lengths (mean 50, 25-120 bp), 0.5% substitutions, 5' C->T
+and 3' G->A deamination (30% at the end, x0.5 per base), 3% random reads; options -l 1024 -n 0.01 -o 2.
+
+One step = one galn_aln_run_batch call (the public C ABI) over all reads of the GPU: reads from pinned host
+memory, H2D, query encoding, every search tier, D2H of n_aln/records/pops/traces and assembly of the result
+table. The L2 cache is flushed (a 512 MB write) before each step, outside the timed region.
+
+  value   reads / device span (first to last search kernel, CUDA events on the library's stream): inputs
+          already in HBM
+  e2e     reads / wall time of the whole call (H2D + device + D2H + result assembly)
+  roofline  the dominant kernel (first search tier): 32 B x its algorithmic block fetches / its time
+  cpu_baseline  the reference's own `galn aln --cpu-only` on a sample of the same reads, all host cores
+
+--impl reference times only the reference's CPU path (rank 0; other ranks exit at once).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import hashlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "reads/s, .sai md5-identical (served vs plain launch, same B200); p50/p99 latency"
+WORKLOAD_DESC = {
+    "adna": "aDNA batched: 100 Mbp reference (45% GC, 10 contigs, 5% repeats), 2,000,000 reads per GPU, "
+            "log-normal 25-120 bp, deaminated, 3% random; -l 1024 -n 0.01 -o 2",
+    "plain_small": "plain aln: 1 Mbp uniform reference, 20,000 x 100 bp reads per GPU; default options",
+    "divergent": "high divergence: 100 Mbp aDNA-like reference, 1,000,000 x 100 bp reads per GPU at 4% "
+                 "substitutions + 0.5% indels; -n 6 -o 2 -e 6 -k 3 -N",
+    "genome": "genome-scale shape (scaled): repeat-rich reference with N runs, 150 bp reads; default options",
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def prepare(workload: str, scale: float, rank: int, device: int, data_dir: str | None):
+    """Reference + BWA index (built on this GPU) + this rank's reads, cached on disk."""
+    from galn_b200 import index_build, synth
+    d = data_dir or os.path.join(tempfile.gettempdir(), f"galn_bench_{workload}_{scale}_r{rank}")
+    os.makedirs(d, exist_ok=True)
+    t = time.time()
+    ref, reads, opts = synth.workload(workload, scale, seed=1)
+    if rank:
+        _, reads, _ = synth.workload(workload, scale, seed=1 + 7919 * rank)
+    prefix = os.path.join(d, "ref")
+    if not os.path.exists(prefix + ".bwt"):
+        index_build.build_from_reference(ref, prefix, device=f"cuda:{device}")
+    log(f"[bench] rank {rank}: data ready in {time.time() - t:.1f} s ({len(reads)} reads, ref {ref.total} bp)")
+    return d, prefix, ref, reads, opts
+
+
+def clock_sampler_start(path, device):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        f = open(path, "w")
+        return subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                 "-lms", "200"], stdout=f, stderr=subprocess.DEVNULL), f
+    except OSError:
+        return None, None
+
+
+def clock_sampler_stop(proc, f, path):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+    f.close()
+    sm, mx, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in open(path):
+        parts = [x.strip() for x in line.split(",")]
+        if len(parts) < 9:
+            continue
+        try:
+            sm.append(float(parts[1]))
+            mx = max(mx, float(parts[2]))
+        except ValueError:
+            continue
+        for nm, v in zip(names, parts[5:9]):
+            if v.lower() == "active":
+                reasons.add(nm)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(prefix, reads, opts, sample, d, steps=1, warmup=0):
+    """The reference's `galn aln --cpu-only` on the first `sample` reads, all host cores."""
+    import oracle
+    from galn_b200 import synth
+    if not os.path.exists(oracle.GALN_REF):
+        return None, "reference binary oracle/_ref/galn_ref not built"
+    cores = os.cpu_count() or 1
+
+    def sample_fastq(m):
+        sub = synth.Reads(reads.names[:m], reads.seq[:int(reads.off[m])], reads.off[:m + 1].copy(),
+                          reads.qual[:int(reads.off[m])] if reads.qual is not None else None)
+        fq = os.path.join(d, f"sample_{m}.fq")
+        if not os.path.exists(fq):
+            synth.write_fastq(fq, sub)
+        return fq
+
+    # grow the sample until the reference's search takes a few seconds (its timer has 10 ms resolution)
+    n = min(sample, len(reads))
+    while True:
+        fq = sample_fastq(n)
+        info = oracle.run_galn_ref(prefix, fq, opts, os.path.join(d, "ref_sample.sai"), workers=cores)
+        if info["rc"] not in (0, 4) or "search_s" not in info:
+            return None, "reference run failed: " + info["stderr"][-200:]
+        if info["search_s"] >= 3.0 or n >= len(reads):
+            break
+        n = min(len(reads), int(n * min(8.0, 4.0 / max(info["search_s"], 0.05))))
+    vals = []
+    for i in range(warmup + steps):
+        if i > 0:
+            info = oracle.run_galn_ref(prefix, fq, opts, os.path.join(d, "ref_sample.sai"), workers=cores)
+            if info["rc"] not in (0, 4) or "search_s" not in info:
+                return None, "reference run failed: " + info["stderr"][-200:]
+        if i >= warmup:
+            vals.append(n / max(info["search_s"], 1e-3))
+    return dict(value=statistics.mean(vals), unit="reads/s", cores=cores, kind="reference",
+                sample=f"first {n} reads of the same workload, reference `galn aln --cpu-only --cpu-workers {cores}`,"
+                       f" search time from its own timing line"), None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="adna", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--engine", default="persistent", choices=["persistent", "plain"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-engine comparison")
+    ap.add_argument("--cpu-sample", type=int, default=200_000)
+    ap.add_argument("--data-dir", default=None)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        import torch  # noqa: F401  (index build)
+        d, prefix, ref, reads, opts = prepare(args.workload, args.scale, 0, local, args.data_dir)
+        cb, why = cpu_reference(prefix, reads, opts, args.cpu_sample, d, steps=args.steps, warmup=args.warmup)
+        if cb is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return 0
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "reads/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * min(args.cpu_sample, len(reads)) / cb["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic (seeded)", "config": {"workload": WORKLOAD_DESC[args.workload], "scale": args.scale},
+                "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "reads/s", "h2d_bytes_per_step": 0,
+                                            "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import galn_b200
+    from galn_b200 import build as gbuild
+    gbuild.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    d, prefix, ref, reads, opts = prepare(args.workload, args.scale, rank, local, args.data_dir)
+    n = len(reads)
+    # pinned host inputs
+    seq_h = torch.empty(len(reads.seq), dtype=torch.uint8, pin_memory=True)
+    seq_h.numpy()[:] = reads.ascii()
+    off_h = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
+    off_h.numpy()[:] = reads.off
+    R = galn_b200.Reads(seq_h.numpy(), off_h.numpy())
+    ix = galn_b200.Index(prefix, device=local)
+    engine = galn_b200.GALN_ENGINE_PERSISTENT if args.engine == "persistent" else galn_b200.GALN_ENGINE_PLAIN
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def run_steps(eng, k, w):
+        md5 = set()
+        e2e, dev, tier0, launches = [], [], [], 0
+        for i in range(w + k):
+            flush.fill_(i & 255)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            res = galn_b200.aln(ix, opts, R, eng)
+            dt = time.perf_counter() - t
+            prof = ix.last_profile()
+            st = ix.last_stats()
+            if i >= w:
+                e2e.append(dt)
+                dev.append(prof["ms_device"] / 1e3)
+                tier0.append(prof["ms_tier"][0] / 1e3)
+                launches += st["launches"]
+                md5.add(hashlib.md5(res.sai_bytes()).hexdigest())
+        return e2e, dev, tier0, launches, md5, res
+
+    # warm-up, then the timed steps bracketed by barriers and synchronisation
+    for _ in range(args.warmup):
+        galn_b200.aln(ix, opts, R, engine)
+    barrier()
+    torch.cuda.synchronize()
+    cpath = os.path.join(d, f"clocks_{rank}.csv")
+    proc, cf = clock_sampler_start(cpath, local)
+    e2e, dev, tier0, launches, md5, res = run_steps(engine, args.steps, 0)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clock_sampler_stop(proc, cf, cpath)
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    e2e_s = max_over_ranks(statistics.mean(e2e))
+    dev_s = max_over_ranks(statistics.mean(dev))
+    t0_s = statistics.mean(tier0)
+    total_reads = n * world
+
+    # roofline of the dominant kernel: algorithmic block fetches of the reads the first tier finished
+    ix.set_tuning(keep_stats=True)
+    galn_b200.aln(ix, opts, R, engine)
+    prof = ix.last_profile(n)
+    fetch_t0 = int(prof["fetch"][prof["tier"] == 0].astype(np.int64).sum())
+    fetch_all = int(prof["fetch"].astype(np.int64).sum())
+    ix.set_tuning(keep_stats=False)
+    peak, peak_kind = peaks()
+    achieved = 32.0 * fetch_t0 / t0_s / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        tj = json.load(open(tp)).get(args.workload)
+        if tj:
+            traffic = tj.get("dram_bytes_per_launch")
+
+    plain = None
+    if not args.no_plain and engine != galn_b200.GALN_ENGINE_PLAIN:
+        pe2e, pdev, _, _, pmd5, _ = run_steps(galn_b200.GALN_ENGINE_PLAIN, max(1, args.steps // 2), 1)
+        plain = {"value": total_reads / max_over_ranks(statistics.mean(pdev)),
+                 "e2e": total_reads / max_over_ranks(statistics.mean(pe2e)), "sai_md5_same": pmd5 == md5}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu, why = cpu_reference(prefix, reads, opts, args.cpu_sample, d)
+        if cpu is None:
+            log("[bench] cpu baseline unavailable:", why)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    h2d = int(len(reads.seq) + 8 * (n + 1))
+    d2h = int(4 * n + 8 * (n + 1) + 16 * n + 24 * int(res.rec_offset[-1]))
+    line = {
+        "metric": METRIC, "value": total_reads / dev_s, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * e2e_s, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic: seeded reference and reads with the workload's shapes (no public dataset here)",
+        "config": {"workload": WORKLOAD_DESC[args.workload], "scale": args.scale, "reads_per_gpu": n,
+                   "options": " ".join(opts), "engine": args.engine,
+                   "l2": "flushed before every step (512 MB device write, outside the timed region)",
+                   "parallelism": f"{world} independent GPU shards (reads split, index replicated)"},
+        "e2e": {"value": total_reads / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "search tier 0 (thread per read, persistent claim)",
+                     "algorithmic_bytes_per_launch": 32 * fetch_t0, "fetches_all_tiers": fetch_all,
+                     "ms_per_launch": 1e3 * t0_s},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "sai_md5": sorted(md5),
+        "deterministic": len(md5) == 1,
+        "ms_device_per_step": 1e3 * dev_s,
+    }
+    if plain:
+        line["plain_engine"] = plain
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,269 @@
+"""ctypes binding of include/galn_aln.h and the Python mirror of the `galn aln` interface."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+GALN_ENGINE_PLAIN = 0
+GALN_ENGINE_PERSISTENT = 1
+REC_DTYPE = np.dtype([("packed", "<u8"), ("k", "<u8"), ("l", "<u8")])
+
+
+class GalnError(RuntimeError):
+    pass
+
+
+class Options(C.Structure):
+    """gap_opt_t: the 64-byte option block written into the .sai header."""
+    _fields_ = [("s_mm", C.c_int32), ("s_gapo", C.c_int32), ("s_gape", C.c_int32), ("mode", C.c_int32),
+                ("indel_end_skip", C.c_int32), ("max_del_occ", C.c_int32), ("max_entries", C.c_int32),
+                ("fnr", C.c_float), ("max_diff", C.c_int32), ("max_gapo", C.c_int32), ("max_gape", C.c_int32),
+                ("max_seed_diff", C.c_int32), ("seed_len", C.c_int32), ("n_threads", C.c_int32),
+                ("max_top2", C.c_int32), ("trim_qual", C.c_int32)]
+
+
+class _Reads(C.Structure):
+    _fields_ = [("n_reads", C.c_int32), ("seq", C.c_void_p), ("offset", C.c_void_p), ("batch", C.c_void_p),
+                ("batch_max_len", C.c_void_p), ("n_batches", C.c_int32)]
+
+
+class _ReadSet(C.Structure):
+    _fields_ = [("reads", _Reads), ("names", C.POINTER(C.c_char_p)), ("_priv", C.c_void_p)]
+
+
+class _Results(C.Structure):
+    _fields_ = [("n_reads", C.c_int32), ("n_aln", C.POINTER(C.c_int32)), ("rec_offset", C.POINTER(C.c_int64)),
+                ("rec", C.c_void_p), ("n_pops", C.POINTER(C.c_uint64)), ("trace", C.POINTER(C.c_uint64)),
+                ("_priv", C.c_void_p)]
+
+
+def lib_path() -> str:
+    return os.path.join(HERE, "libgalnb200.so")
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises if it has not been built (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = lib_path()
+    if not os.path.exists(p):
+        raise GalnError(f"{p} is missing: build it with `python -m galn_b200.build` (no CPU fallback exists)")
+    L = C.CDLL(p)
+    vp = C.c_void_p
+    L.galn_opts_default.argtypes = [C.POINTER(Options)]
+    L.galn_opts_parse.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(Options), C.POINTER(C.c_char_p), C.c_int,
+                                  C.POINTER(C.c_int), C.POINTER(C.c_char_p), C.c_char_p, C.c_size_t]
+    L.galn_cal_maxdiff.argtypes = [C.c_int, C.c_double, C.c_double]
+    L.galn_index_open.restype = vp
+    L.galn_index_open.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_int)]
+    L.galn_index_open_mem.restype = vp
+    L.galn_index_open_mem.argtypes = [vp, C.c_size_t, C.c_int, C.POINTER(C.c_int)]
+    L.galn_index_close.argtypes = [vp]
+    L.galn_index_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.galn_fastq_read.argtypes = [C.c_char_p, C.POINTER(_ReadSet)]
+    L.galn_read_set_free.argtypes = [C.POINTER(_ReadSet)]
+    L.galn_results_free.argtypes = [C.POINTER(_Results)]
+    L.galn_aln_run_batch.argtypes = [vp, C.POINTER(Options), C.POINTER(_Reads), C.c_int, C.POINTER(_Results)]
+    L.galn_sai_write.argtypes = [C.c_char_p, C.POINTER(Options), C.POINTER(_Results)]
+    L.galn_last_run_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.galn_last_run_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), vp, vp, C.c_int32]
+    L.galn_index_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.galn_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def parse_options(args: list[str]) -> Options:
+    """The option block of `galn aln <args>` (positional arguments are not allowed here)."""
+    o = Options()
+    argv = (C.c_char_p * max(1, len(args)))(*[a.encode() for a in args])
+    pos = (C.c_char_p * 4)()
+    npos = C.c_int(0)
+    outp = C.c_char_p()
+    err = C.create_string_buffer(256)
+    rc = lib().galn_opts_parse(len(args), argv, C.byref(o), pos, 4, C.byref(npos), C.byref(outp), err, 256)
+    if rc != 0:
+        raise GalnError(err.value.decode())
+    if npos.value:
+        raise GalnError("unexpected positional argument")
+    return o
+
+
+def cal_maxdiff(length: int, err: float, thres: float) -> int:
+    return lib().galn_cal_maxdiff(length, err, thres)
+
+
+class Index:
+    """<prefix>.bwt resident on one GPU in the device occurrence layout."""
+
+    def __init__(self, prefix: str | None = None, device: int = 0, bwt_bytes: bytes | None = None):
+        err = C.c_int(0)
+        if bwt_bytes is not None:
+            buf = C.create_string_buffer(bwt_bytes, len(bwt_bytes))
+            self.h = lib().galn_index_open_mem(buf, len(bwt_bytes), device, C.byref(err))
+        else:
+            self.h = lib().galn_index_open(prefix.encode(), device, C.byref(err))
+        if not self.h:
+            raise GalnError(f"cannot open the index ({err.value})")
+        n, p, b = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        lib().galn_index_info(self.h, C.byref(n), C.byref(p), C.byref(b))
+        self.seq_len, self.primary, self.device_bytes = n.value, p.value, b.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().galn_index_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_tuning(self, t0_cap=4096, t0_aln=32, t0_block=128, t1_cap=65536, t1_aln=1024, keep_stats=False):
+        rc = lib().galn_index_set_tuning(self.h, t0_cap, t0_aln, t0_block, t1_cap, t1_aln, int(keep_stats))
+        if rc:
+            raise GalnError(f"bad tuning ({rc})")
+
+    def last_profile(self, n: int = 0) -> dict:
+        """Device span and per-tier kernel ms of the last run; with n > 0 (and keep_stats tuning) also the
+        per-read 32-byte block fetches and finishing tier."""
+        dev = C.c_double()
+        tiers = (C.c_double * 8)()
+        fetch = np.zeros(max(n, 1), np.uint32)
+        tier = np.zeros(max(n, 1), np.int8)
+        rc = lib().galn_last_run_profile(self.h, C.byref(dev), tiers, fetch.ctypes.data if n else None,
+                                         tier.ctypes.data if n else None, n)
+        if rc:
+            raise GalnError(f"no profile ({rc})")
+        out = dict(ms_device=dev.value, ms_tier=list(tiers))
+        if n:
+            out["fetch"] = fetch[:n]
+            out["tier"] = tier[:n]
+        return out
+
+    def last_stats(self) -> dict:
+        t, k, tiers, la = C.c_double(), C.c_double(), C.c_int(), C.c_int64()
+        ovf = (C.c_int64 * 8)()
+        lib().galn_last_run_stats(self.h, C.byref(t), C.byref(k), C.byref(tiers), C.byref(la), ovf)
+        return dict(ms_total=t.value, ms_kernels=k.value, tiers=tiers.value, launches=la.value, overflow=list(ovf))
+
+
+@dataclass
+class Reads:
+    """ASCII bases concatenated (uint8), n+1 int64 offsets, optional int32 batch ids."""
+    seq: np.ndarray
+    offset: np.ndarray
+    batch: np.ndarray | None = None
+    batch_max_len: np.ndarray | None = None
+    names: list[str] | None = None
+
+    def __len__(self):
+        return len(self.offset) - 1
+
+    @staticmethod
+    def from_strings(seqs: list[str | bytes]) -> "Reads":
+        bs = [s.encode() if isinstance(s, str) else s for s in seqs]
+        off = np.zeros(len(bs) + 1, np.int64)
+        off[1:] = np.cumsum([len(b) for b in bs])
+        return Reads(np.frombuffer(b"".join(bs) or b"\0", np.uint8)[:off[-1]].copy(), off)
+
+    def c_struct(self) -> tuple[_Reads, list]:
+        keep = []
+        seq = np.ascontiguousarray(self.seq, np.uint8)
+        if seq.size == 0:
+            seq = np.zeros(1, np.uint8)
+        off = np.ascontiguousarray(self.offset, np.int64)
+        keep += [seq, off]
+        r = _Reads()
+        r.n_reads = len(off) - 1
+        r.seq = seq.ctypes.data
+        r.offset = off.ctypes.data
+        if self.batch is not None:
+            b = np.ascontiguousarray(self.batch, np.int32)
+            keep.append(b)
+            r.batch = b.ctypes.data
+        if self.batch_max_len is not None:
+            m = np.ascontiguousarray(self.batch_max_len, np.int32)
+            keep.append(m)
+            r.batch_max_len = m.ctypes.data
+            r.n_batches = len(m)
+        return r, keep
+
+
+def read_fastq(path: str) -> Reads:
+    """A FASTQ/FASTA file read by the library with the reference's rules (batch ids included)."""
+    rs = _ReadSet()
+    rc = lib().galn_fastq_read(path.encode(), C.byref(rs))
+    if rc != 0:
+        raise GalnError(f"cannot read {path} ({rc})")
+    n = rs.reads.n_reads
+    off = np.ctypeslib.as_array(C.cast(rs.reads.offset, C.POINTER(C.c_int64)), (n + 1,)).copy()
+    total = int(off[-1])
+    seq = (np.ctypeslib.as_array(C.cast(rs.reads.seq, C.POINTER(C.c_uint8)), (total,)).copy()
+           if total else np.zeros(0, np.uint8))
+    batch = (np.ctypeslib.as_array(C.cast(rs.reads.batch, C.POINTER(C.c_int32)), (n,)).copy()
+             if n else np.zeros(0, np.int32))
+    names = [rs.names[i].decode() for i in range(n)]
+    lib().galn_read_set_free(C.byref(rs))
+    return Reads(seq, off, batch, None, names)
+
+
+class Results:
+    def __init__(self, r: _Results, opts: Options):
+        n = r.n_reads
+        self.opts = opts
+        self.n_aln = np.ctypeslib.as_array(r.n_aln, (max(n, 1),))[:n].copy()
+        self.rec_offset = np.ctypeslib.as_array(r.rec_offset, (n + 1,)).copy()
+        tot = int(self.rec_offset[-1])
+        self.records = (np.frombuffer((C.c_char * (24 * tot)).from_address(r.rec), REC_DTYPE).copy()
+                        if tot else np.zeros(0, REC_DTYPE))
+        self.pops = np.ctypeslib.as_array(r.n_pops, (max(n, 1),))[:n].copy()
+        self.trace = np.ctypeslib.as_array(r.trace, (max(n, 1),))[:n].copy()
+
+    def __len__(self):
+        return len(self.n_aln)
+
+    def sai_bytes(self) -> bytes:
+        out = [b"SAI\x01", bytes(self.opts)]
+        for r in range(len(self.n_aln)):
+            na = int(self.n_aln[r])
+            if na < 0:
+                na = 0
+            out.append(np.int32(na).tobytes())
+            if na:
+                out.append(self.records[self.rec_offset[r]:self.rec_offset[r] + na].tobytes())
+        return b"".join(out)
+
+    def write_sai(self, path: str) -> int:
+        with open(path, "wb") as f:
+            f.write(self.sai_bytes())
+        return 4 if (self.n_aln < 0).any() else 0
+
+
+def aln(index: Index, args: list[str] | Options, reads: Reads | str,
+        engine: int = GALN_ENGINE_PERSISTENT) -> Results:
+    """`galn aln <args>` on the reads (a Reads object or a FASTQ path) against a resident index."""
+    opts = args if isinstance(args, Options) else parse_options(list(args))
+    if isinstance(reads, str):
+        reads = read_fastq(reads)
+    cr, keep = reads.c_struct()
+    res = _Results()
+    rc = lib().galn_aln_run_batch(index.h, C.byref(opts), C.byref(cr), engine, C.byref(res))
+    if rc != 0:
+        raise GalnError(f"galn_aln_run_batch failed ({rc})")
+    out = Results(res, opts)
+    lib().galn_results_free(C.byref(res))
+    del keep
+    return out
+
+
+def write_sai(path: str, res: Results) -> int:
+    return res.write_sai(path)

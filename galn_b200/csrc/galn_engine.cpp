@@ -1,0 +1,393 @@
+// galn_engine.cpp -- one search job on the device: per-batch options, device buffers, and the tiers.
+//
+// Per-batch options follow the reference's aln_batch_opt / aln_read_maxdiff (src/aln_host.c:23-43): with -n
+// as a fraction, a batch's max_diff comes from its longest read and max_gapo is clamped to it; n_stacks =
+// score(max_diff+1, max_gapo+1, max_gape+1); each read's max_diff comes from its own length.
+//
+// Tiers (every read ends on the GPU; there is no CPU fallback):
+//   T0   bump-allocated stack of t0_cap entries per thread, t0_aln records: nearly every read ends here
+//   T1   free-list stack of t1_cap live entries, t1_aln records, for the reads that overflowed T0
+//   T2+  free-list stack of max_entries + 16 live entries (enough to reach the reference's own
+//        n_entries > max_entries cut-off exactly), records growing x16 per tier
+// A read that overflows is searched again from scratch in the next tier, as the reference re-runs a read
+// on overflow (src/aln_host.c:87-147), so results never depend on the capacities.
+// PLAIN launches T0 once per bwa batch with one thread per read (the reference's light tier, one launch per
+// chunk, src/galn.cu:835-905). PERSISTENT launches T0 once over all reads with as many threads as the
+// device keeps resident, each claiming reads from a device counter until none are left.
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <numeric>
+#include <unordered_map>
+#include <vector>
+
+#include "galn_host_internal.h"
+
+namespace galn {
+
+#define ECK(call)                                                                             \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            fprintf(stderr, "[galn] CUDA error %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return GALN_ECUDA;                                                                \
+        }                                                                                     \
+    } while (0)
+#define RCK(call)                      \
+    do {                               \
+        int r_ = (call);               \
+        if (r_) return r_;             \
+    } while (0)
+
+static double now_ms()
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+static inline int score_of(int m, int o, int e, const galn_opts *p) { return m * p->s_mm + o * p->s_gapo + e * p->s_gape; }
+
+int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine, galn_results *out)
+{
+    double t_start = now_ms();
+    const int n = in->n_reads;
+    if (n < 0 || (n > 0 && (!in->seq || !in->offset))) return GALN_EINVAL;
+    JobBufs &B = ix->ws;
+    RunStats &S = ix->last;
+    S = RunStats();
+    cudaStream_t st = ix->stream;
+    ECK(cudaSetDevice(ix->dev.device));
+
+    // ---- per-read lengths, batches, options ----
+    std::vector<int32_t> bid((size_t)std::max(n, 1));
+    int n_batches = 0, max_len = 0;
+    for (int r = 0; r < n; ++r) {
+        int64_t len = in->offset[r + 1] - in->offset[r];
+        if (len < 0 || len > 65535) return GALN_EINVAL;
+        int b = in->batch ? in->batch[r] : r / kBatchReads;
+        if (b < 0) return GALN_EINVAL;
+        bid[r] = b;
+        n_batches = std::max(n_batches, b + 1);
+        max_len = std::max(max_len, (int)len);
+    }
+    // the longest read of each batch: given by the caller when these reads are a shard of a larger input
+    if (in->batch_max_len && in->n_batches > n_batches) n_batches = in->n_batches;
+    std::vector<int> bmax((size_t)std::max(n_batches, 1), 0);
+    for (int r = 0; r < n; ++r) bmax[bid[r]] = std::max(bmax[bid[r]], (int)(in->offset[r + 1] - in->offset[r]));
+    if (in->batch_max_len) {
+        if (in->n_batches < n_batches) return GALN_EINVAL;
+        for (int b = 0; b < n_batches; ++b) bmax[b] = std::max(bmax[b], (int)in->batch_max_len[b]);
+    }
+    std::vector<HostBatchOpt> bopt((size_t)std::max(n_batches, 1));
+    int max_stacks = 1;
+    bool wide = ix->dev.seq_len >= (1ull << 38);
+    for (int b = 0; b < n_batches; ++b) {
+        HostBatchOpt &h = bopt[b];
+        memset(&h, 0, sizeof(h));
+        h.s_mm = o->s_mm; h.s_gapo = o->s_gapo; h.s_gape = o->s_gape; h.mode = o->mode;
+        h.indel_end_skip = o->indel_end_skip; h.max_del_occ = o->max_del_occ; h.max_entries = o->max_entries;
+        h.max_diff = o->max_diff; h.max_gapo = o->max_gapo; h.max_gape = o->max_gape;
+        h.max_seed_diff = o->max_seed_diff; h.seed_len = o->seed_len; h.max_top2 = o->max_top2;
+        if (o->fnr > 0.0) h.max_diff = galn_cal_maxdiff(bmax[b], 0.02, o->fnr);
+        if (h.max_diff < h.max_gapo) h.max_gapo = h.max_diff;
+        galn_opts tmp = *o;
+        tmp.max_gapo = h.max_gapo;
+        h.n_stacks = score_of(h.max_diff + 1, h.max_gapo + 1, h.max_gape + 1, &tmp);
+        max_stacks = std::max(max_stacks, h.n_stacks);
+        if (h.max_gapo > 126 || h.max_gape > 126) wide = true;
+    }
+    std::vector<int32_t> maxdiff((size_t)std::max(n, 1));
+    {
+        std::unordered_map<int, int> cache;
+        for (int r = 0; r < n; ++r) {
+            int len = (int)(in->offset[r + 1] - in->offset[r]);
+            int md;
+            if (o->fnr > 0.0) {
+                auto it = cache.find(len);
+                if (it == cache.end()) it = cache.emplace(len, galn_cal_maxdiff(len, 0.02, o->fnr)).first;
+                md = it->second;
+            } else md = bopt[bid[r]].max_diff;
+            maxdiff[r] = md;
+            if (md > 125) wide = true;
+        }
+    }
+    for (auto &h : bopt) h.wide = wide ? 1 : 0;
+
+    // ---- device buffers ----
+    const int64_t total = n > 0 ? in->offset[n] - in->offset[0] : 0;
+    const int64_t base = n > 0 ? in->offset[0] : 0;
+    size_t nn = (size_t)std::max(n, 1);
+    RCK(B.seq.ensure((size_t)std::max<int64_t>(total, 1)));
+    RCK(B.query.ensure((size_t)std::max<int64_t>(total, 1)));
+    RCK(B.off.ensure((nn + 1) * 8));
+    RCK(B.bidx.ensure(nn * 4));
+    RCK(B.maxdiff.ensure(nn * 4));
+    RCK(B.bopt.ensure(bopt.size() * sizeof(HostBatchOpt)));
+    RCK(B.out_n.ensure(nn * 4));
+    RCK(B.out_off.ensure(nn * 8));
+    RCK(B.out_pops.ensure(nn * 8));
+    RCK(B.out_trace.ensure(nn * 8));
+    RCK(B.out_peak.ensure(nn * 4));
+    RCK(B.out_fetch.ensure(nn * 4));
+    RCK(B.out_tier.ensure(nn));
+    RCK(B.list_a.ensure(nn * 4));
+    RCK(B.list_b.ensure(nn * 4));
+    RCK(B.counters.ensure(64));
+    RCK(B.rec_top.ensure(64));
+    int64_t rec_cap = (int64_t)n * 2 + 65536;
+    RCK(B.out_rec.ensure((size_t)rec_cap * 24));
+    rec_cap = (int64_t)(B.out_rec.n / 24);
+    // host staging
+    RCK(B.h_off.ensure((nn + 1) * 8));
+    RCK(B.h_list.ensure(nn * 4 * 3));
+    int64_t *h_off = (int64_t *)B.h_off.p;
+    for (int r = 0; r <= n; ++r) h_off[r] = in->offset[r] - base;
+    int32_t *h_bid = (int32_t *)B.h_list.p, *h_md = h_bid + nn, *h_list = h_md + nn;
+    memcpy(h_bid, bid.data(), (size_t)n * 4);
+    memcpy(h_md, maxdiff.data(), (size_t)n * 4);
+    // reads ordered by batch (stable): each batch is one contiguous segment of the list
+    std::vector<int> bstart((size_t)n_batches + 1, 0);
+    for (int r = 0; r < n; ++r) ++bstart[bid[r] + 1];
+    for (int b = 0; b < n_batches; ++b) bstart[b + 1] += bstart[b];
+    {
+        std::vector<int> fill(bstart.begin(), bstart.end() - 1);
+        for (int r = 0; r < n; ++r) h_list[fill[bid[r]]++] = r;
+    }
+    if (total > 0) ECK(cudaMemcpyAsync(B.seq.p, in->seq + base, (size_t)total, cudaMemcpyHostToDevice, st));
+    ECK(cudaMemcpyAsync(B.off.p, h_off, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice, st));
+    ECK(cudaMemcpyAsync(B.bidx.p, h_bid, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    ECK(cudaMemcpyAsync(B.maxdiff.p, h_md, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    ECK(cudaMemcpyAsync(B.list_a.p, h_list, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    ECK(cudaMemcpyAsync(B.bopt.p, bopt.data(), bopt.size() * sizeof(HostBatchOpt), cudaMemcpyHostToDevice, st));
+    ECK(cudaMemsetAsync(B.rec_top.p, 0, 8, st));
+
+    DevJob job;
+    job.n_reads = n; job.n_batches = n_batches;
+    job.seq = (uint8_t *)B.seq.p; job.query = (uint8_t *)B.query.p; job.off = (int64_t *)B.off.p;
+    job.bidx = (int32_t *)B.bidx.p; job.maxdiff = (int32_t *)B.maxdiff.p; job.bopt = (HostBatchOpt *)B.bopt.p;
+    job.seed_len = o->seed_len; job.max_len = max_len; job.max_stacks = max_stacks; job.any_wide = wide ? 1 : 0;
+    job.out_n = (int32_t *)B.out_n.p; job.out_off = (int64_t *)B.out_off.p; job.out_pops = (uint64_t *)B.out_pops.p;
+    job.out_trace = (uint64_t *)B.out_trace.p; job.out_peak = (int32_t *)B.out_peak.p;
+    job.out_fetch = (uint32_t *)B.out_fetch.p; job.out_tier = (int8_t *)B.out_tier.p;
+    job.out_rec = (uint64_t *)B.out_rec.p; job.rec_top = (unsigned long long *)B.rec_top.p; job.rec_cap = rec_cap;
+    job.list_a = (int32_t *)B.list_a.p; job.list_b = (int32_t *)B.list_b.p; job.counters = (int32_t *)B.counters.p;
+    if (job.seed_len < 0) job.seed_len = 0;
+    cudaEvent_t span0, span1;
+    ECK(cudaEventCreate(&span0));
+    ECK(cudaEventCreate(&span1));
+    ECK(cudaEventRecord(span0, st));
+    RCK(dev_encode(job, st));
+    if (n > 0) S.kernel_launches += 1;
+
+    size_t free_b = 0, total_b = 0;
+    ECK(cudaMemGetInfo(&free_b, &total_b));
+    size_t budget = (size_t)((double)(free_b + B.ws.n) * ix->mem_fraction);
+
+    cudaEvent_t e0, e1;
+    ECK(cudaEventCreate(&e0));
+    ECK(cudaEventCreate(&e1));
+    float k_ms = 0;
+    RCK(B.h_misc.ensure(64));
+    int32_t *h_cnt = (int32_t *)B.h_misc.p;
+
+    // run one tier over list[0..m) with overflow going to ovf; returns the overflow count
+    auto run_tier = [&](TierCfg cfg, const int32_t *list, int m, int32_t *ovf, int *n_ovf) -> int {
+        *n_ovf = 0;
+        if (m == 0) return 0;
+        if (cfg.persistent) {
+            int res = dev_resident_threads(cfg, wide, ix->dev.device);
+            if (res <= 0) return GALN_ECUDA;
+            cfg.threads = std::min(m, res);
+        } else cfg.threads = m;
+        if (cfg.threads < 1) cfg.threads = 1;
+        // fit the workspace into the budget
+        for (;;) {
+            size_t need = ws_bytes(cfg, job);
+            if (need <= budget || cfg.threads <= cfg.block) break;
+            if (!cfg.persistent) return GALN_ENOMEM;   // caller splits
+            cfg.threads = std::max(cfg.block, cfg.threads / 2);
+        }
+        RCK(B.ws.ensure(ws_bytes(cfg, job)));
+        ECK(cudaMemsetAsync(job.counters, 0, 8, st));
+        ECK(cudaEventRecord(e0, st));
+        RCK(dev_search(ix->dev, job, cfg, list, m, ovf, B.ws.p, st));
+        ECK(cudaEventRecord(e1, st));
+        ECK(cudaMemcpyAsync(h_cnt, job.counters, 8, cudaMemcpyDeviceToHost, st));
+        ECK(cudaStreamSynchronize(st));
+        float ms = 0;
+        ECK(cudaEventElapsedTime(&ms, e0, e1));
+        k_ms += ms;
+        S.ms_tier[cfg.tier] += ms;
+        S.kernel_launches += 1;
+        *n_ovf = h_cnt[1];
+        return 0;
+    };
+
+    // ---- T0 ----
+    int32_t *cur = job.list_a, *nxt = job.list_b;
+    int n_ovf = 0;
+    TierCfg t0;
+    t0.tier = 0;
+    t0.freelist = false; t0.cap = ix->t0_cap; t0.aln_cap = ix->t0_aln; t0.block = ix->t0_block;
+    if (engine == GALN_ENGINE_PERSISTENT) {
+        t0.persistent = true;
+        RCK(run_tier(t0, cur, n, nxt, &n_ovf));
+    } else {
+        // one launch per bwa batch, one thread per read; a batch too large for the memory budget is
+        // launched in equal chunks
+        t0.persistent = false;
+        int max_chunk = kBatchReads;
+        for (;;) {
+            TierCfg probe = t0;
+            probe.threads = max_chunk;
+            if (ws_bytes(probe, job) <= budget || max_chunk <= 1024) break;
+            max_chunk /= 2;
+        }
+        int acc = 0;
+        for (int b = 0; b < n_batches; ++b) {
+            for (int s0 = bstart[b]; s0 < bstart[b + 1]; s0 += max_chunk) {
+                int m = std::min(max_chunk, bstart[b + 1] - s0);
+                int got = 0;
+                RCK(run_tier(t0, cur + s0, m, nxt + acc, &got));
+                acc += got;
+            }
+        }
+        n_ovf = acc;
+    }
+    S.overflow_reads[0] = n_ovf;
+    std::swap(cur, nxt);
+
+    // ---- T1, T2, ... ----
+    int tier = 1;
+    int64_t aln_cap = ix->t1_aln;
+    while (n_ovf > 0 && tier < 8) {
+        // make room for records: grow the record buffer when it is more than half used
+        unsigned long long top = 0;
+        ECK(cudaMemcpyAsync(&top, job.rec_top, 8, cudaMemcpyDeviceToHost, st));
+        ECK(cudaStreamSynchronize(st));
+        if ((int64_t)top > job.rec_cap / 2) {
+            int64_t keep = std::min<int64_t>((int64_t)top, job.rec_cap);
+            int64_t cap2 = std::max<int64_t>(2 * job.rec_cap, (int64_t)top * 2 + 65536);
+            void *np = nullptr;
+            ECK(cudaMalloc(&np, (size_t)cap2 * 24));
+            ECK(cudaMemcpyAsync(np, job.out_rec, (size_t)keep * 24, cudaMemcpyDeviceToDevice, st));
+            ECK(cudaStreamSynchronize(st));
+            B.out_rec.release();
+            B.out_rec.p = np;
+            B.out_rec.n = (size_t)cap2 * 24;
+            job.out_rec = (uint64_t *)np;
+            job.rec_cap = cap2;
+            if ((int64_t)top > job.rec_cap) ECK(cudaMemcpyAsync(job.rec_top, &keep, 8, cudaMemcpyHostToDevice, st));
+        }
+        TierCfg t;
+        t.tier = tier;
+        t.freelist = true;
+        t.persistent = true;
+        t.block = 128;
+        t.cap = tier == 1 ? ix->t1_cap : (int)std::min<int64_t>((int64_t)o->max_entries + 16, 0x7fffffff);
+        if (t.cap < 16) t.cap = 16;
+        t.aln_cap = (int)std::min<int64_t>(aln_cap, 1 << 24);
+        int got = 0;
+        RCK(run_tier(t, cur, n_ovf, nxt, &got));
+        S.overflow_reads[tier] = got;
+        n_ovf = got;
+        std::swap(cur, nxt);
+        if (tier >= 2) aln_cap *= 16;
+        else aln_cap = 65536;
+        ++tier;
+    }
+    S.tiers = tier;
+    ECK(cudaEventRecord(span1, st));
+    ECK(cudaEventSynchronize(span1));
+    {
+        float ms = 0;
+        ECK(cudaEventElapsedTime(&ms, span0, span1));
+        S.ms_device = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(span0);
+    cudaEventDestroy(span1);
+    if (n_ovf > 0) return GALN_ENOMEM;
+
+    // ---- results ----
+    unsigned long long top = 0;
+    ECK(cudaMemcpyAsync(&top, job.rec_top, 8, cudaMemcpyDeviceToHost, st));
+    RCK(B.h_n.ensure(nn * 4));
+    RCK(B.h_off.ensure((nn + 1) * 8));
+    RCK(B.h_pops.ensure(nn * 8));
+    RCK(B.h_trace.ensure(nn * 8));
+    ECK(cudaMemcpyAsync(B.h_n.p, job.out_n, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    ECK(cudaMemcpyAsync(B.h_off.p, job.out_off, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    ECK(cudaMemcpyAsync(B.h_pops.p, job.out_pops, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    ECK(cudaMemcpyAsync(B.h_trace.p, job.out_trace, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    if (ix->keep_stats) {
+        S.fetch.resize(nn);
+        S.tier_of.resize(nn);
+        ECK(cudaMemcpyAsync(S.fetch.data(), job.out_fetch, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+        ECK(cudaMemcpyAsync(S.tier_of.data(), job.out_tier, (size_t)n, cudaMemcpyDeviceToHost, st));
+    }
+    ECK(cudaStreamSynchronize(st));
+    top = std::min<unsigned long long>(top, (unsigned long long)job.rec_cap);
+    RCK(B.h_rec.ensure((size_t)std::max<unsigned long long>(top, 1) * 24));
+    if (top) ECK(cudaMemcpyAsync(B.h_rec.p, job.out_rec, (size_t)top * 24, cudaMemcpyDeviceToHost, st));
+    ECK(cudaStreamSynchronize(st));
+    results_fill(out, n, (const int32_t *)B.h_n.p, (const int64_t *)B.h_off.p, (const uint64_t *)B.h_rec.p,
+                 (const uint64_t *)B.h_pops.p, (const uint64_t *)B.h_trace.p);
+    S.ms_kernels = k_ms;
+    S.ms_total = now_ms() - t_start;
+    return 0;
+}
+
+}  // namespace galn
+
+extern "C" int galn_aln_run_batch(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine, galn_results *out)
+{
+    if (!ix || !o || !in || !out) return GALN_EINVAL;
+    if (engine != GALN_ENGINE_PLAIN && engine != GALN_ENGINE_PERSISTENT) return GALN_EINVAL;
+    memset(out, 0, sizeof(*out));
+    std::lock_guard<std::mutex> lk(ix->mu);
+    return galn::run_job(ix, o, in, engine, out);
+}
+
+extern "C" int galn_last_run_stats(galn_index *ix, double *ms_total, double *ms_kernels, int *tiers,
+                                   int64_t *launches, int64_t *overflow /* 8 */)
+{
+    if (!ix) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    if (ms_total) *ms_total = ix->last.ms_total;
+    if (ms_kernels) *ms_kernels = ix->last.ms_kernels;
+    if (tiers) *tiers = ix->last.tiers;
+    if (launches) *launches = ix->last.kernel_launches;
+    if (overflow) memcpy(overflow, ix->last.overflow_reads, sizeof(ix->last.overflow_reads));
+    return 0;
+}
+
+extern "C" int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, uint32_t *fetch, int8_t *tier,
+                                     int32_t n)
+{
+    if (!ix) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    if (ms_device) *ms_device = ix->last.ms_device;
+    if (ms_tier) memcpy(ms_tier, ix->last.ms_tier, sizeof(ix->last.ms_tier));
+    if (fetch || tier) {
+        if ((size_t)n > ix->last.fetch.size()) return GALN_EINVAL;
+        if (fetch) memcpy(fetch, ix->last.fetch.data(), (size_t)n * 4);
+        if (tier) memcpy(tier, ix->last.tier_of.data(), (size_t)n);
+    }
+    return 0;
+}
+
+extern "C" int galn_index_set_tuning(galn_index *ix, int t0_cap, int t0_aln, int t0_block, int t1_cap, int t1_aln,
+                                     int keep_stats)
+{
+    if (!ix) return GALN_EINVAL;
+    if (t0_cap < 16 || t0_aln < 1 || t1_cap < 16 || t1_aln < 1 || (t0_block != 64 && t0_block != 128 &&
+        t0_block != 256 && t0_block != 512)) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    ix->t0_cap = t0_cap; ix->t0_aln = t0_aln; ix->t0_block = t0_block;
+    ix->t1_cap = t1_cap; ix->t1_aln = t1_aln;
+    ix->keep_stats = keep_stats != 0;
+    return 0;
+}

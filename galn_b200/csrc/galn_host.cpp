@@ -1,0 +1,419 @@
+// galn_host.cpp -- host side of galn-b200: the C ABI of include/galn_aln.h.
+//
+//   options       galn_opts_default / galn_opts_parse / galn_cal_maxdiff
+//                 (the reference's opt_default, parse_args and aln_cal_maxdiff: src/opt_build.h:23-36,
+//                 src/galn.cu:185-250, src/aln_host.c:9-21; this file is compiled with -ffp-contract=off)
+//   reads         galn_fastq_read (read_fastq's rules, src/host_io.c:151-205, kseq record semantics)
+//   index         galn_index_open (load_bwt, src/host_io.c:29-76) + the device occurrence layout
+//   search        galn_aln_run_batch: per-batch options (aln_batch_opt / aln_read_maxdiff,
+//                 src/aln_host.c:23-43) and the device tiers (galn_kernels.cu)
+//   output        galn_sai_write (src/sai_writer.h:9-21, src/galn.cu:1250-1263)
+//   serving       galn_server_* (galn_serve.cpp)
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include <ctype.h>
+#include <zlib.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/galn_aln.h"
+#include "galn_internal.h"
+#include "galn_host_internal.h"
+
+using namespace galn;
+
+extern "C" const char *galn_version(void) { return "galn-b200 0.1.0 (sm_100a)"; }
+
+// ---------------------------------------------------------------------------------------------------
+// options
+
+extern "C" int galn_opts_default(galn_opts *o)
+{
+    if (!o) return GALN_EINVAL;
+    memset(o, 0, sizeof(*o));
+    o->s_mm = 3; o->s_gapo = 11; o->s_gape = 4;
+    o->max_diff = -1; o->max_gapo = 1; o->max_gape = 6;
+    o->indel_end_skip = 5; o->max_del_occ = 10; o->max_entries = 2000000;
+    o->mode = 0x01 | 0x02;
+    o->seed_len = 32; o->max_seed_diff = 2;
+    o->fnr = 0.04f;
+    o->n_threads = 1;
+    o->max_top2 = 30;
+    o->trim_qual = 0;
+    return 0;
+}
+
+static void set_err(char *err, size_t n, const char *msg, const char *arg)
+{
+    if (err && n) snprintf(err, n, "%s%s%s", msg, arg ? " " : "", arg ? arg : "");
+}
+
+extern "C" int galn_opts_parse(int argc, const char *const *argv, galn_opts *o, const char **pos, int max_pos,
+                               int *n_pos, const char **out_path, char *err, size_t err_len)
+{
+    if (!o) return GALN_EINVAL;
+    galn_opts_default(o);
+    int opte = -1, np = 0;
+    if (out_path) *out_path = nullptr;
+    for (int i = 0; i < argc; ++i) {
+        const char *a = argv[i];
+        const char *v = i + 1 < argc ? argv[i + 1] : nullptr;
+        if (a[0] != '-' || !a[1]) {
+            if (np < max_pos && pos) pos[np] = a;
+            ++np;
+            continue;
+        }
+        if (!strcmp(a, "-L")) { o->mode |= 0x04; continue; }
+        if (!strcmp(a, "-N")) { o->mode |= 0x10; o->max_top2 = 0x7fffffff; continue; }
+        if (!v) { set_err(err, err_len, "option needs a value:", a); return GALN_EINVAL; }
+        if (!strcmp(a, "-n")) {
+            if (strchr(v, '.')) { o->fnr = (float)atof(v); o->max_diff = -1; }
+            else { o->max_diff = atoi(v); o->fnr = -1.0f; }
+        }
+        else if (!strcmp(a, "-o")) o->max_gapo = atoi(v);
+        else if (!strcmp(a, "-e")) opte = atoi(v);
+        else if (!strcmp(a, "-M")) o->s_mm = atoi(v);
+        else if (!strcmp(a, "-O")) o->s_gapo = atoi(v);
+        else if (!strcmp(a, "-E")) o->s_gape = atoi(v);
+        else if (!strcmp(a, "-d")) o->max_del_occ = atoi(v);
+        else if (!strcmp(a, "-i")) o->indel_end_skip = atoi(v);
+        else if (!strcmp(a, "-l")) o->seed_len = atoi(v);
+        else if (!strcmp(a, "-k")) o->max_seed_diff = atoi(v);
+        else if (!strcmp(a, "-m")) o->max_entries = atoi(v);
+        else if (!strcmp(a, "-dt") || !strcmp(a, "-t")) o->n_threads = atoi(v);
+        else if (!strcmp(a, "-R")) o->max_top2 = atoi(v);
+        else if (!strcmp(a, "-f")) { if (out_path) *out_path = v; }
+        else if (!strcmp(a, "-q")) {
+            if (atoi(v) >= 1) { set_err(err, err_len, "-q (quality trimming) is not supported", nullptr); return GALN_EINVAL; }
+        }
+        else { set_err(err, err_len, "unsupported option", a); return GALN_EINVAL; }
+        ++i;
+    }
+    if (opte > 0) { o->max_gape = opte; o->mode &= ~0x01; }
+    if (o->n_threads < 1) o->n_threads = 1;
+    if (n_pos) *n_pos = np;
+    return 0;
+}
+
+extern "C" int galn_cal_maxdiff(int l, double err, double thres)
+{
+    double elambda = exp(-l * err);
+    double sum = elambda, y = 1.0;
+    int x = 1;
+    for (int k = 1; k < 1000; ++k) {
+        y *= l * err;
+        x = (int)((unsigned)x * (unsigned)k);   // the reference's int factorial, wrapping
+        sum += elambda * y / x;
+        if (1.0 - sum < thres) return k;
+    }
+    return 2;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// FASTQ / FASTA reading with kseq's record rules
+
+namespace {
+
+struct Src {
+    const unsigned char *p;
+    size_t n, i;
+    int getc_() { return i < n ? p[i++] : -1; }
+};
+
+// append up to the next '\n' (consumed); drop a trailing '\r' of the whole string when longer than 1
+long read_line(Src &s, std::string &t)
+{
+    if (s.i >= s.n) return -1;
+    const unsigned char *nl = (const unsigned char *)memchr(s.p + s.i, '\n', s.n - s.i);
+    size_t e = nl ? (size_t)(nl - s.p) : s.n;
+    t.append((const char *)s.p + s.i, e - s.i);
+    s.i = nl ? e + 1 : e;
+    if (t.size() > 1 && t.back() == '\r') t.pop_back();
+    return (long)t.size();
+}
+
+struct RecordReader {
+    int last = 0;
+    std::string name, seq, qual;
+    // >= 0: sequence length; -1 end of input; -2 malformed record
+    int next(Src &s)
+    {
+        int c;
+        if (last == 0) {
+            while ((c = s.getc_()) != -1 && c != '>' && c != '@') {}
+            if (c == -1) return -1;
+            last = c;
+        }
+        name.clear(); seq.clear(); qual.clear();
+        if (s.i >= s.n) return -1;
+        size_t st = s.i;
+        while (s.i < s.n && !isspace(s.p[s.i])) ++s.i;
+        name.assign((const char *)s.p + st, s.i - st);
+        int delim = s.i < s.n ? s.p[s.i++] : 0;
+        if (delim != '\n') { std::string tmp; read_line(s, tmp); }
+        while ((c = s.getc_()) != -1 && c != '>' && c != '+' && c != '@') {
+            if (c == '\n') continue;
+            seq.push_back((char)c);
+            read_line(s, seq);
+        }
+        if (c == '>' || c == '@') last = c;
+        if (c != '+') return (int)seq.size();
+        while ((c = s.getc_()) != -1 && c != '\n') {}
+        if (c == -1) return -2;
+        while (read_line(s, qual) >= 0 && qual.size() < seq.size()) {}
+        last = 0;
+        if (seq.size() != qual.size()) return -2;
+        return (int)seq.size();
+    }
+};
+
+struct ReadSetPriv {
+    std::vector<char> seq;
+    std::vector<int64_t> off;
+    std::vector<int32_t> batch;
+    std::vector<std::string> names;
+    std::vector<char *> name_ptrs;
+};
+
+}  // namespace
+
+extern "C" int galn_fastq_read(const char *path, galn_read_set *out)
+{
+    if (!path || !out) return GALN_EINVAL;
+    memset(out, 0, sizeof(*out));
+    gzFile fp = gzopen(path, "rb");
+    if (!fp) return GALN_EIO;
+    gzbuffer(fp, 1 << 20);
+    std::vector<unsigned char> buf;
+    size_t n = 0;
+    buf.resize(1 << 22);
+    for (;;) {
+        if (buf.size() - n < (1 << 20)) buf.resize(buf.size() * 2);
+        int r = gzread(fp, buf.data() + n, (unsigned)(buf.size() - n));
+        if (r < 0) { gzclose(fp); return GALN_EIO; }
+        if (r == 0) break;
+        n += (size_t)r;
+    }
+    if (gzclose(fp) != Z_OK) return GALN_EIO;
+    auto *P = new ReadSetPriv();
+    Src s{buf.data(), n, 0};
+    RecordReader rr;
+    int batch = 0, in_batch = 0;
+    P->off.push_back(0);
+    for (;;) {
+        int l = rr.next(s);
+        if (l < 0) {
+            if (in_batch == 0 || l == -1) break;
+            ++batch; in_batch = 0;      // a malformed record ends the batch
+            continue;
+        }
+        if (rr.seq.empty()) continue;  // empty reads are skipped
+        P->seq.insert(P->seq.end(), rr.seq.begin(), rr.seq.end());
+        P->off.push_back((int64_t)P->seq.size());
+        P->batch.push_back(batch);
+        P->names.push_back(rr.name);
+        if (++in_batch == kBatchReads) { ++batch; in_batch = 0; }
+    }
+    P->name_ptrs.resize(P->names.size());
+    for (size_t i = 0; i < P->names.size(); ++i) P->name_ptrs[i] = (char *)P->names[i].c_str();
+    out->reads.n_reads = (int32_t)P->batch.size();
+    out->reads.seq = P->seq.data();
+    out->reads.offset = P->off.data();
+    out->reads.batch = P->batch.data();
+    out->names = P->name_ptrs.data();
+    out->_priv = P;
+    return 0;
+}
+
+extern "C" int galn_read_set_free(galn_read_set *rs)
+{
+    if (!rs) return GALN_EINVAL;
+    delete (ReadSetPriv *)rs->_priv;
+    memset(rs, 0, sizeof(*rs));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// index
+
+static galn_index *index_from_words(const uint64_t hdr[5], const uint32_t *body, uint64_t n_words, int device, int *err)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        if (err) *err = GALN_ECUDA;
+        return nullptr;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+        if (err) *err = GALN_ECUDA;
+        return nullptr;
+    }
+    auto *ix = new galn_index();
+    DevIndex &d = ix->dev;
+    d.device = device;
+    d.primary = hdr[0];
+    d.L2[0] = 0;
+    for (int c = 0; c < 4; ++c) d.L2[c + 1] = hdr[c + 1];
+    d.seq_len = d.L2[4];
+    uint64_t nb = (d.seq_len + 127) / 128;
+    uint64_t expect = 8 * (nb + 1) + (d.seq_len + 15) / 16;
+    if (d.seq_len == 0 || n_words != expect || d.primary == 0 || d.primary > d.seq_len) {
+        delete ix;
+        if (err) *err = GALN_EIO;
+        return nullptr;
+    }
+    ix->sms = prop.multiProcessorCount;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ix;
+        if (err) *err = GALN_ECUDA;
+        return nullptr;
+    }
+    int rc = dev_index_build(d, body, n_words, ix->stream);
+    if (rc) {
+        dev_index_free(d);
+        delete ix;
+        if (err) *err = rc;
+        return nullptr;
+    }
+    if (err) *err = 0;
+    return ix;
+}
+
+extern "C" galn_index *galn_index_open(const char *prefix, int device, int *err)
+{
+    if (!prefix) { if (err) *err = GALN_EINVAL; return nullptr; }
+    std::string fn = std::string(prefix) + ".bwt";
+    FILE *fp = fopen(fn.c_str(), "rb");
+    if (!fp) { if (err) *err = GALN_EIO; return nullptr; }
+    uint64_t hdr[5];
+    if (fread(hdr, 8, 5, fp) != 5) { fclose(fp); if (err) *err = GALN_EIO; return nullptr; }
+    fseeko(fp, 0, SEEK_END);
+    long long sz = ftello(fp);
+    fseeko(fp, 40, SEEK_SET);
+    if (sz < 40 || (sz - 40) % 4) { fclose(fp); if (err) *err = GALN_EIO; return nullptr; }
+    uint64_t n_words = (uint64_t)(sz - 40) / 4;
+    uint32_t *body = nullptr;
+    if (cudaMallocHost(&body, n_words * 4 + 4) != cudaSuccess) { fclose(fp); if (err) *err = GALN_ENOMEM; return nullptr; }
+    size_t got = 0;
+    while (got < n_words) {
+        size_t r = fread(body + got, 4, std::min<size_t>(n_words - got, (size_t)1 << 26), fp);
+        if (r == 0) break;
+        got += r;
+    }
+    fclose(fp);
+    if (got != n_words) { cudaFreeHost(body); if (err) *err = GALN_EIO; return nullptr; }
+    galn_index *ix = index_from_words(hdr, body, n_words, device, err);
+    cudaFreeHost(body);
+    return ix;
+}
+
+extern "C" galn_index *galn_index_open_mem(const void *bytes, size_t n_bytes, int device, int *err)
+{
+    if (!bytes || n_bytes < 40 || (n_bytes - 40) % 4) { if (err) *err = GALN_EINVAL; return nullptr; }
+    uint64_t hdr[5];
+    memcpy(hdr, bytes, 40);
+    return index_from_words(hdr, (const uint32_t *)((const char *)bytes + 40), (n_bytes - 40) / 4, device, err);
+}
+
+extern "C" int galn_index_close(galn_index *ix)
+{
+    if (!ix) return GALN_EINVAL;
+    cudaSetDevice(ix->dev.device);
+    ix->ws.release();
+    dev_index_free(ix->dev);
+    if (ix->stream) cudaStreamDestroy(ix->stream);
+    delete ix;
+    return 0;
+}
+
+extern "C" int galn_index_info(const galn_index *ix, uint64_t *seq_len, uint64_t *primary, uint64_t *device_bytes)
+{
+    if (!ix) return GALN_EINVAL;
+    if (seq_len) *seq_len = ix->dev.seq_len;
+    if (primary) *primary = ix->dev.primary;
+    if (device_bytes) *device_bytes = ix->dev.n_blocks * 32;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// results and .sai
+
+namespace {
+struct ResultsPriv {
+    std::vector<int32_t> n_aln;
+    std::vector<int64_t> rec_off;
+    std::vector<galn_aln1> rec;
+    std::vector<uint64_t> pops, trace;
+};
+}  // namespace
+
+void galn::results_fill(galn_results *out, int n, const int32_t *n_aln, const int64_t *dev_off,
+                        const uint64_t *rec_words, const uint64_t *pops, const uint64_t *trace)
+{
+    auto *P = new ResultsPriv();
+    P->n_aln.assign(n_aln, n_aln + n);
+    P->pops.assign(pops, pops + n);
+    P->trace.assign(trace, trace + n);
+    P->rec_off.resize((size_t)n + 1);
+    int64_t t = 0;
+    for (int r = 0; r < n; ++r) {
+        P->rec_off[r] = t;
+        if (n_aln[r] > 0) t += n_aln[r];
+    }
+    P->rec_off[n] = t;
+    P->rec.resize((size_t)std::max<int64_t>(t, 1));
+    for (int r = 0; r < n; ++r) {
+        if (n_aln[r] <= 0) continue;
+        memcpy(&P->rec[P->rec_off[r]], rec_words + 3 * dev_off[r], (size_t)n_aln[r] * sizeof(galn_aln1));
+    }
+    out->n_reads = n;
+    out->n_aln = P->n_aln.data();
+    out->rec_offset = P->rec_off.data();
+    out->rec = P->rec.data();
+    out->n_pops = P->pops.data();
+    out->trace = P->trace.data();
+    out->_priv = P;
+}
+
+extern "C" int galn_results_free(galn_results *res)
+{
+    if (!res) return GALN_EINVAL;
+    delete (ResultsPriv *)res->_priv;
+    memset(res, 0, sizeof(*res));
+    return 0;
+}
+
+extern "C" int galn_sai_write(const char *path, const galn_opts *o, const galn_results *res)
+{
+    if (!o || !res) return GALN_EINVAL;
+    FILE *fp = path ? fopen(path, "wb") : stdout;
+    if (!fp) return 5;
+    static_assert(sizeof(galn_opts) == 64, "gap_opt_t is 64 bytes");
+    static_assert(sizeof(galn_aln1) == 24, "bwt_aln1_t is 24 bytes");
+    int err = 0;
+    std::vector<char> buf;
+    buf.reserve(1 << 20);
+    auto put = [&](const void *p, size_t n) {
+        buf.insert(buf.end(), (const char *)p, (const char *)p + n);
+        if (buf.size() >= (1 << 20)) { if (fwrite(buf.data(), 1, buf.size(), fp) != buf.size()) err = 5; buf.clear(); }
+    };
+    put("SAI\1", 4);
+    put(o, sizeof(*o));
+    for (int r = 0; r < res->n_reads; ++r) {
+        int32_t na = res->n_aln[r];
+        if (na < 0) { if (!err) err = 4; na = 0; }
+        put(&na, 4);
+        if (na > 0) put(res->rec + res->rec_offset[r], (size_t)na * sizeof(galn_aln1));
+    }
+    if (!buf.empty() && fwrite(buf.data(), 1, buf.size(), fp) != buf.size()) err = 5;
+    if (fflush(fp) != 0 || ferror(fp)) err = 5;
+    if (path && fclose(fp) != 0) err = 5;
+    return err;
+}

@@ -1,0 +1,87 @@
+// galn_host_internal.h -- host-side state shared by galn_host.cpp, galn_engine.cpp and galn_serve.cpp.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <vector>
+
+#include "../../include/galn_aln.h"
+#include "galn_internal.h"
+
+namespace galn {
+
+// a grow-only device or pinned-host buffer
+struct Buf {
+    void *p = nullptr;
+    size_t n = 0;
+    bool host = false;
+    int ensure(size_t bytes)
+    {
+        if (bytes <= n) return 0;
+        release();
+        size_t want = bytes + bytes / 4 + 4096;
+        cudaError_t e = host ? cudaMallocHost(&p, want) : cudaMalloc(&p, want);
+        if (e != cudaSuccess) { cudaGetLastError(); p = nullptr; n = 0; return -23; }
+        n = want;
+        return 0;
+    }
+    void release()
+    {
+        if (p) { if (host) cudaFreeHost(p); else cudaFree(p); }
+        p = nullptr;
+        n = 0;
+    }
+};
+
+// every buffer one search job uses, kept across calls on the same index (calls are serialised)
+struct JobBufs {
+    Buf seq, query, off, bidx, maxdiff, bopt, out_n, out_off, out_pops, out_trace, out_peak, out_fetch, out_tier,
+        out_rec, rec_top, list_a, list_b, counters, ws;
+    Buf h_n, h_off, h_pops, h_trace, h_rec, h_list, h_misc;
+    JobBufs()
+    {
+        h_n.host = h_off.host = h_pops.host = h_trace.host = h_rec.host = h_list.host = h_misc.host = true;
+    }
+    void release()
+    {
+        Buf *all[] = {&seq, &query, &off, &bidx, &maxdiff, &bopt, &out_n, &out_off, &out_pops, &out_trace, &out_peak,
+                      &out_fetch, &out_tier, &out_rec, &rec_top, &list_a, &list_b, &counters, &ws, &h_n, &h_off, &h_pops, &h_trace, &h_rec,
+                      &h_list, &h_misc};
+        for (Buf *b : all) b->release();
+    }
+};
+
+// statistics of the last run (for benchmarks and tests)
+struct RunStats {
+    double ms_total = 0, ms_kernels = 0, ms_device = 0;
+    double ms_tier[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int tiers = 0;
+    int64_t overflow_reads[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t kernel_launches = 0;
+    std::vector<uint32_t> fetch;     // per read, of the last run
+    std::vector<int8_t> tier_of;     // per read, of the last run
+};
+
+}  // namespace galn
+
+struct galn_index {
+    galn::DevIndex dev;
+    cudaStream_t stream = nullptr;
+    int sms = 0;
+    std::mutex mu;
+    galn::JobBufs ws;
+    galn::RunStats last;
+    // tuning knobs (galn_tune.cpp sets them; defaults otherwise)
+    int t0_cap = 4096, t0_aln = 32, t0_block = 128;
+    int t1_cap = 65536, t1_aln = 1024;
+    double mem_fraction = 0.6;          // of free device memory a job's workspace may take
+    bool keep_stats = false;            // keep per-read fetch counts and tiers of the last run
+};
+
+namespace galn {
+void results_fill(galn_results *out, int n, const int32_t *n_aln, const int64_t *dev_off, const uint64_t *rec_words,
+                  const uint64_t *pops, const uint64_t *trace);
+int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);
+}  // namespace galn

@@ -1,0 +1,87 @@
+// galn_internal.h -- the interface between the host library (galn_host.cpp) and the CUDA code
+// (galn_kernels.cu). Not installed; the public interface is include/galn_aln.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace galn {
+
+constexpr int kBatchReads = 0x40000;   // bwa_read_seq batch (src/host_io.h:16)
+
+// per-batch options handed to the device (the layout of BatchOpt in galn_device.cuh)
+struct HostBatchOpt {
+    int s_mm, s_gapo, s_gape, mode;
+    int indel_end_skip, max_del_occ, max_entries;
+    int max_diff, max_gapo, max_gape, max_seed_diff, seed_len, max_top2;
+    int n_stacks;
+    int wide;
+    int pad_;
+};
+
+struct DevIndex {
+    int device = 0;
+    uint64_t primary = 0, seq_len = 0, n_blocks = 0;
+    uint64_t L2[5] = {0, 0, 0, 0, 0};
+    uint64_t sb[16][4] = {};
+    void *blocks = nullptr;            // n_blocks * 32 bytes, device
+};
+
+// Builds the occ64 layout on the device from the .bwt body words (host memory).
+int dev_index_build(DevIndex &ix, const uint32_t *body, uint64_t n_words, cudaStream_t st);
+void dev_index_free(DevIndex &ix);
+
+// Device buffers of one search job (all reads of a request).
+struct DevJob {
+    int n_reads = 0, n_batches = 0;
+    uint8_t *seq = nullptr;            // ASCII, as given
+    uint8_t *query = nullptr;          // encoded: reversed+complemented codes
+    int64_t *off = nullptr;            // n_reads + 1
+    int32_t *bidx = nullptr;           // batch of each read
+    int32_t *maxdiff = nullptr;        // per read
+    HostBatchOpt *bopt = nullptr;      // per batch (device copy)
+    int seed_len = 0;
+    int max_len = 0;
+    int max_stacks = 0;
+    int any_wide = 0;
+    // outputs, per read
+    int32_t *out_n = nullptr;
+    int64_t *out_off = nullptr;
+    uint64_t *out_pops = nullptr, *out_trace = nullptr;
+    int32_t *out_peak = nullptr;
+    uint32_t *out_fetch = nullptr;     // 32-byte index blocks read per read (algorithmic traffic)
+    int8_t *out_tier = nullptr;        // tier that finished each read
+    uint64_t *out_rec = nullptr;       // 3 words per record
+    unsigned long long *rec_top = nullptr;
+    int64_t rec_cap = 0;
+    // work lists
+    int32_t *list_a = nullptr, *list_b = nullptr;
+    int32_t *counters = nullptr;       // [0] claim, [1] overflow count
+};
+
+// Tier parameters of one search launch.
+struct TierCfg {
+    bool freelist = false;
+    int cap = 4096;                    // entries per slot
+    int aln_cap = 32;                  // records per slot
+    int threads = 0;                   // slots launched
+    bool persistent = false;           // claim loop over the list
+    int block = 128;
+    int tier = 0;
+};
+
+struct Workspace;
+
+// Encodes the reads (ASCII -> reversed complemented codes) on the device.
+int dev_encode(DevJob &job, cudaStream_t st);
+
+// Launches one search tier over list[0..n) of read ids, appending overflowed reads to ovf[] (count in
+// job.counters[1]). ws_mem is a device buffer of at least ws_bytes(cfg, job) bytes.
+size_t ws_bytes(const TierCfg &cfg, const DevJob &job);
+int dev_search(const DevIndex &ix, DevJob &job, const TierCfg &cfg, const int32_t *list, int n, int32_t *ovf,
+               void *ws_mem, cudaStream_t st);
+
+// Occupancy: resident threads per SM for a tier's kernel at the given block size
+int dev_resident_threads(const TierCfg &cfg, bool wide, int device);
+
+}  // namespace galn

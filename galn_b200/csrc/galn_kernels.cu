@@ -1,0 +1,312 @@
+// galn_kernels.cu -- CUDA kernels of galn-b200 (sm_100a): index layout conversion, query encoding and the
+// thread-per-read search tiers. Host-side orchestration is in galn_host.cpp.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "galn_internal.h"
+#include "galn_search.cuh"
+
+namespace galn {
+
+static_assert(sizeof(HostBatchOpt) == sizeof(BatchOpt), "BatchOpt layout");
+
+#define GALN_CUDA(call)                                                                          \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            fprintf(stderr, "[galn] CUDA error %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return -22;                                                                          \
+        }                                                                                        \
+    } while (0)
+
+// ---------------------------------------------------------------------------------------------------
+// bwa .bwt body -> occ64 blocks. Block b covers symbols [64b, 64b+64) of the $-free BWT; it sits in half
+// (b & 1) of bwa block b >> 1 (128 symbols: 4 x uint64 counts, then 8 words of 16 symbols, first symbol
+// in the top bits; src/index/idxcommon.c:72-112 writes that layout).
+__global__ void convert_kernel(const uint32_t *__restrict__ body, uint64_t n_words, uint64_t n_sym,
+                               uint64_t n_blocks, const uint64_t *__restrict__ sb, uint4 *__restrict__ out)
+{
+    uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n_blocks) return;
+    uint64_t B = b >> 1;
+    int h = (int)(b & 1);
+    const uint32_t *blk = body + B * 16;
+    uint32_t words[4];
+    for (int t = 0; t < 4; ++t) {
+        uint64_t wi = B * 16 + 8 + 4 * h + t;
+        uint64_t first_sym = 128 * B + 64 * h + 16 * t;
+        words[t] = (wi < n_words && first_sym < n_sym) ? body[wi] : 0u;
+    }
+    uint64_t cnt[4] = {0, 0, 0, 0};
+    if (B * 16 + 8 <= n_words) {
+        for (int c = 0; c < 4; ++c) cnt[c] = (uint64_t)blk[2 * c] | ((uint64_t)blk[2 * c + 1] << 32);
+    }
+    if (h) {   // add the first 64 symbols of the bwa block
+        for (int t = 0; t < 4; ++t) {
+            uint64_t wi = B * 16 + 8 + t;
+            uint32_t w = wi < n_words ? body[wi] : 0u;
+            for (int j = 0; j < 16; ++j) {
+                uint64_t sym_pos = 128 * B + 16 * t + j;
+                if (sym_pos < n_sym) ++cnt[(w >> (30 - 2 * j)) & 3];
+            }
+        }
+    }
+    uint64_t p0 = 0, p1 = 0;
+    for (int j = 0; j < 64; ++j) {
+        uint64_t pos = 64 * b + j;
+        if (pos >= n_sym) break;
+        uint32_t s = (words[j >> 4] >> (30 - 2 * (j & 15))) & 3;
+        p0 |= (uint64_t)(s & 1) << j;
+        p1 |= (uint64_t)(s >> 1) << j;
+    }
+    const uint64_t *s = sb + ((64 * b) >> 32) * 4;
+    out[2 * b] = make_uint4((uint32_t)(cnt[0] - s[0]), (uint32_t)(cnt[1] - s[1]), (uint32_t)(cnt[2] - s[2]),
+                            (uint32_t)(cnt[3] - s[3]));
+    out[2 * b + 1] = make_uint4((uint32_t)p0, (uint32_t)(p0 >> 32), (uint32_t)p1, (uint32_t)(p1 >> 32));
+}
+
+int dev_index_build(DevIndex &ix, const uint32_t *body, uint64_t n_words, cudaStream_t st)
+{
+    const uint64_t n = ix.seq_len;
+    ix.n_blocks = n / 64 + 1;
+    uint64_t n_super = (n >> 32) + 1;
+    if (n_super > 16) return -20;
+    // Occ before each superblock start (a multiple of 128: the stored counts of that bwa block)
+    for (uint64_t s = 0; s < 16; ++s)
+        for (int c = 0; c < 4; ++c) ix.sb[s][c] = 0;
+    for (uint64_t s = 1; s < n_super; ++s) {
+        uint64_t B = (s << 32) >> 7;
+        for (int c = 0; c < 4; ++c) ix.sb[s][c] = (uint64_t)body[B * 16 + 2 * c] | ((uint64_t)body[B * 16 + 2 * c + 1] << 32);
+    }
+    GALN_CUDA(cudaSetDevice(ix.device));
+    void *d_body = nullptr, *d_sb = nullptr;
+    GALN_CUDA(cudaMalloc(&ix.blocks, ix.n_blocks * 32));
+    GALN_CUDA(cudaMalloc(&d_body, n_words * 4));
+    GALN_CUDA(cudaMalloc(&d_sb, sizeof(ix.sb)));
+    GALN_CUDA(cudaMemcpyAsync(d_body, body, n_words * 4, cudaMemcpyHostToDevice, st));
+    GALN_CUDA(cudaMemcpyAsync(d_sb, ix.sb, sizeof(ix.sb), cudaMemcpyHostToDevice, st));
+    unsigned grid = (unsigned)((ix.n_blocks + 255) / 256);
+    convert_kernel<<<grid, 256, 0, st>>>((const uint32_t *)d_body, n_words, n, ix.n_blocks, (const uint64_t *)d_sb,
+                                         (uint4 *)ix.blocks);
+    GALN_CUDA(cudaGetLastError());
+    GALN_CUDA(cudaStreamSynchronize(st));
+    cudaFree(d_body);
+    cudaFree(d_sb);
+    return 0;
+}
+
+void dev_index_free(DevIndex &ix)
+{
+    if (ix.blocks) {
+        cudaSetDevice(ix.device);
+        cudaFree(ix.blocks);
+        ix.blocks = nullptr;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// query encoding: query[j] = complement(nt4(read[len-1-j])), ambiguous -> 4 (src/host_io.c:178-183)
+__global__ void encode_kernel(const uint8_t *__restrict__ seq, const int64_t *__restrict__ off, int n,
+                              uint8_t *__restrict__ query)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    int64_t s = off[r], e = off[r + 1];
+    int64_t len = e - s;
+    for (int64_t j = 0; j < len; ++j) {
+        uint8_t ch = seq[e - 1 - j];
+        uint8_t b;
+        switch (ch | 0x20) {
+        case 'a': b = 3; break;    // complement of A
+        case 'c': b = 2; break;
+        case 'g': b = 1; break;
+        case 't': b = 0; break;
+        default: b = 4;
+        }
+        query[s + j] = b;
+    }
+}
+
+int dev_encode(DevJob &job, cudaStream_t st)
+{
+    if (job.n_reads == 0) return 0;
+    encode_kernel<<<(job.n_reads + 255) / 256, 256, 0, st>>>(job.seq, job.off, job.n_reads, job.query);
+    GALN_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// search
+
+struct KArgs {
+    IndexView ix;
+    const uint8_t *query;
+    const int64_t *off;
+    const int32_t *bidx;
+    const int32_t *maxdiff;
+    const BatchOpt *bopt;
+    int seed_len;
+    const int32_t *list;
+    int n;
+    int n_slots;            // workspace slots; threads at or past it do nothing
+    int persistent;
+    int32_t *claim;
+    Workspace ws;
+    int32_t *out_n;
+    int64_t *out_off;
+    uint64_t *out_pops, *out_trace;
+    int32_t *out_peak;
+    uint32_t *out_fetch;
+    int8_t *out_tier;
+    int tier;
+    uint64_t *out_rec;
+    unsigned long long *rec_top;
+    int64_t rec_cap;
+    int32_t *ovf;
+    int32_t *ovf_n;
+};
+
+template <bool WIDE, bool FREELIST>
+__device__ __forceinline__ void run_read(const KArgs &a, int pos, int slot)
+{
+    const int r = a.list[pos];
+    const int64_t s = a.off[r];
+    const int len = (int)(a.off[r + 1] - s);
+    const uint8_t *q = a.query + s;
+    const BatchOpt bo = a.bopt[a.bidx[r]];
+    const int md = a.maxdiff[r];
+    uint64_t *W = a.ws.wid + (size_t)slot * a.ws.wcap;
+    uint64_t *SW = W + (len + 1);
+    const bool use_seed = len > a.seed_len;
+    uint32_t fetches = 0;
+    cal_width(a.ix, len, q, W, fetches);
+    if (use_seed) cal_width(a.ix, a.seed_len, q + (len - a.seed_len), SW, fetches);
+    SearchResult R = match_gap<WIDE, FREELIST>(a.ix, bo, md, len, q, W, SW, use_seed, a.ws, slot, fetches);
+    int ret = R.ret;
+    if (ret > 0) {
+        unsigned long long o = atomicAdd(a.rec_top, (unsigned long long)ret);
+        if ((int64_t)(o + ret) > a.rec_cap) ret = kErrAln;
+        else {
+            const uint64_t *src = a.ws.aln + (size_t)slot * a.ws.aln_cap * 3;
+            uint64_t *dst = a.out_rec + o * 3;
+            for (int j = 0; j < 3 * ret; ++j) dst[j] = src[j];
+            a.out_off[r] = (int64_t)o;
+        }
+    }
+    if (ret == kErrStack || ret == kErrAln) a.ovf[atomicAdd(a.ovf_n, 1)] = r;
+    a.out_n[r] = ret;
+    a.out_pops[r] = R.pops;
+    a.out_trace[r] = R.trace;
+    a.out_peak[r] = R.peak;
+    a.out_fetch[r] = R.fetches;
+    a.out_tier[r] = (int8_t)a.tier;
+}
+
+template <bool WIDE, bool FREELIST>
+__global__ void __launch_bounds__(128) search_kernel(const __grid_constant__ KArgs a)
+{
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= a.n_slots) return;
+    if (!a.persistent) {
+        if (slot < a.n) run_read<WIDE, FREELIST>(a, slot, slot);
+        return;
+    }
+    for (;;) {
+        int pos = atomicAdd(a.claim, 1);
+        if (pos >= a.n) break;
+        run_read<WIDE, FREELIST>(a, pos, slot);
+    }
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// width[] of the longest read, then seed_width[] when some read is longer than the seed
+static int width_cap(const DevJob &job)
+{
+    return job.max_len + 1 + (job.max_len > job.seed_len ? job.seed_len + 1 : 0) + 1;
+}
+
+static void ws_layout(const TierCfg &cfg, const DevJob &job, size_t off[6])
+{
+    size_t slots = (size_t)cfg.threads;
+    size_t esz = job.any_wide ? 32 : 16;
+    int wcap = width_cap(job);
+    off[0] = 0;
+    off[1] = off[0] + align256(slots * cfg.cap * esz);
+    off[2] = off[1] + align256(slots * cfg.cap * 4);
+    off[3] = off[2] + align256(slots * (size_t)job.max_stacks * 4);
+    off[4] = off[3] + align256(slots * (size_t)wcap * 8);
+    off[5] = off[4] + align256(slots * (size_t)cfg.aln_cap * 24);
+}
+
+size_t ws_bytes(const TierCfg &cfg, const DevJob &job)
+{
+    size_t off[6];
+    ws_layout(cfg, job, off);
+    return off[5];
+}
+
+template <bool WIDE, bool FREELIST>
+static int launch(const KArgs &a, int threads, int block, cudaStream_t st)
+{
+    unsigned grid = (unsigned)((threads + block - 1) / block);
+    search_kernel<WIDE, FREELIST><<<grid, block, 0, st>>>(a);
+    GALN_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int dev_search(const DevIndex &ix, DevJob &job, const TierCfg &cfg, const int32_t *list, int n, int32_t *ovf,
+               void *ws_mem, cudaStream_t st)
+{
+    if (n == 0) return 0;
+    KArgs a;
+    memset(&a, 0, sizeof(a));
+    a.ix.blk = (const uint4 *)ix.blocks;
+    a.ix.primary = ix.primary;
+    a.ix.seq_len = ix.seq_len;
+    for (int c = 0; c < 4; ++c) a.ix.C[c] = ix.L2[c];
+    memcpy(a.ix.sb, ix.sb, sizeof(a.ix.sb));
+    a.query = job.query; a.off = job.off; a.bidx = job.bidx; a.maxdiff = job.maxdiff;
+    a.bopt = (const BatchOpt *)job.bopt; a.seed_len = job.seed_len;
+    a.list = list; a.n = n; a.persistent = cfg.persistent ? 1 : 0; a.claim = job.counters;
+    a.n_slots = cfg.threads;
+    size_t off[6];
+    ws_layout(cfg, job, off);
+    char *base = (char *)ws_mem;
+    a.ws.ent = (uint4 *)(base + off[0]);
+    a.ws.link = (int32_t *)(base + off[1]);
+    a.ws.heads = (int32_t *)(base + off[2]);
+    a.ws.wid = (uint64_t *)(base + off[3]);
+    a.ws.aln = (uint64_t *)(base + off[4]);
+    a.ws.cap = cfg.cap; a.ws.hcap = job.max_stacks; a.ws.wcap = width_cap(job);
+    a.ws.aln_cap = cfg.aln_cap;
+    a.out_n = job.out_n; a.out_off = job.out_off; a.out_pops = job.out_pops; a.out_trace = job.out_trace;
+    a.out_peak = job.out_peak; a.out_fetch = job.out_fetch; a.out_tier = job.out_tier; a.tier = cfg.tier;
+    a.out_rec = job.out_rec; a.rec_top = job.rec_top; a.rec_cap = job.rec_cap;
+    a.ovf = ovf; a.ovf_n = job.counters + 1;
+    if (!cfg.persistent && cfg.threads < n) return -20;
+    int threads = cfg.persistent ? cfg.threads : n;
+    if (job.any_wide)
+        return cfg.freelist ? launch<true, true>(a, threads, cfg.block, st) : launch<true, false>(a, threads, cfg.block, st);
+    return cfg.freelist ? launch<false, true>(a, threads, cfg.block, st) : launch<false, false>(a, threads, cfg.block, st);
+}
+
+int dev_resident_threads(const TierCfg &cfg, bool wide, int device)
+{
+    int bps = 0;
+    cudaError_t e;
+    if (wide)
+        e = cfg.freelist ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<true, true>, cfg.block, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<true, false>, cfg.block, 0);
+    else
+        e = cfg.freelist ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<false, true>, cfg.block, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<false, false>, cfg.block, 0);
+    if (e != cudaSuccess) return -22;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return bps * cfg.block * sms;
+}
+
+}  // namespace galn

@@ -1,0 +1,231 @@
+// galn_main.cpp -- the `galn aln` command line on top of the C ABI (the reference's galn_aln,
+// src/galn.cu:436-1288, and its usage text, src/galn.cu:144-180).
+//
+//   galn aln [options] <prefix> <reads.fq[.gz]> [> out.sai]
+//
+// Every bwa aln option keeps its meaning and default; -dt only sets the thread count written into the .sai
+// header. Flags of the reference that pick CPU/GPU work sharing (--cpu-workers, --gpu-only, --cpu-interleave,
+// --handoff, --handoff-when, --light-cap, --warps, --pool-gb, --alloc) are accepted and ignored: all reads run
+// on the GPU. --cpu-only is refused (there is no CPU search). --device and --gpus pick the GPUs; reads are
+// split over them in contiguous shards whose batches keep the options of the whole input.
+// Exit codes follow the reference: 1 usage/option, 2 index, 3 reads, 4 a read could not be searched,
+// 5 write error, 10 CUDA error or no device (src/galn.cu:551-552, 1256-1263, 453-454, 80-83).
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/galn_aln.h"
+
+static int usage()
+{
+    fprintf(stderr,
+            "\nProgram: galn-b200 (bwa aln search on NVIDIA B200, sm_100a)\n\n"
+            "Usage:   galn aln [options] <prefix> <in.fq[.gz]>\n\n"
+            "bwa aln options (same meaning and defaults as BWA 0.7.19):\n"
+            "         -n NUM    max #diff (int) or missing prob under 0.02 err rate (float) [0.04]\n"
+            "         -o INT    maximum number of gap opens [1]\n"
+            "         -e INT    maximum number of gap extensions, -1 for disabling long gaps [-1]\n"
+            "         -i INT    do not put an indel within INT bp towards the ends [5]\n"
+            "         -d INT    maximum occurrences for extending a long deletion [10]\n"
+            "         -l INT    seed length [32]\n"
+            "         -k INT    maximum differences in the seed [2]\n"
+            "         -m INT    maximum entries in the queue [2000000]\n"
+            "         -dt INT   thread count written to the .sai header, as bwa aln -t [1]\n"
+            "         -M INT    mismatch penalty [3]\n"
+            "         -O INT    gap open penalty [11]\n"
+            "         -E INT    gap extension penalty [4]\n"
+            "         -R INT    stop searching when there are >INT equally best hits [30]\n"
+            "         -L        log-scaled gap penalty for long deletions\n"
+            "         -N        non-iterative mode: search for all n-difference hits (slooow)\n"
+            "         -f FILE   file to write output to instead of stdout\n"
+            "         (not supported: -q, -b/-0/-1/-2, -I, -Y, -B)\n\n"
+            "GPU options:\n"
+            "         --device LIST  CUDA device(s), e.g. 0 or 0,1 [all visible]\n"
+            "         --gpus INT     use the first INT visible devices [all]\n"
+            "         --engine STR   persistent (default) or plain\n"
+            "         -v             timing statistics on stderr\n\n");
+    return 1;
+}
+
+static double now_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int main(int argc, char **argv)
+{
+    if (argc < 2) return usage();
+    if (!strcmp(argv[1], "--version") || !strcmp(argv[1], "version")) { printf("%s\n", galn_version()); return 0; }
+    if (strcmp(argv[1], "aln")) {
+        fprintf(stderr, "[galn] unknown command '%s' (this build provides aln)\n", argv[1]);
+        return usage();
+    }
+    std::vector<const char *> bwa_args;
+    const char *devspec = nullptr;
+    int ngpus = 0, verbose = 0, engine = GALN_ENGINE_PERSISTENT;
+    static const char *ignored_with_value[] = {"--cpu-workers", "--cpu-interleave", "--handoff", "--handoff-when",
+                                               "--light-cap", "--warps", "--pool-gb", "--alloc"};
+    for (int i = 2; i < argc; ++i) {
+        const char *a = argv[i];
+        const char *v = i + 1 < argc ? argv[i + 1] : nullptr;
+        bool skip = false;
+        for (const char *ig : ignored_with_value)
+            if (!strcmp(a, ig)) { if (!v) return usage(); ++i; skip = true; break; }
+        if (skip) continue;
+        if (!strcmp(a, "--gpu-only") || !strcmp(a, "--verify")) continue;
+        if (!strcmp(a, "--cpu-only")) { fprintf(stderr, "[galn] --cpu-only: this build searches on the GPU only\n"); return 1; }
+        if (!strcmp(a, "-v")) { verbose = 1; continue; }
+        if (!strcmp(a, "--device")) { if (!v) return usage(); devspec = v; ++i; continue; }
+        if (!strcmp(a, "--gpus")) { if (!v) return usage(); ngpus = atoi(v); ++i; continue; }
+        if (!strcmp(a, "--engine")) {
+            if (!v) return usage();
+            if (!strcmp(v, "plain")) engine = GALN_ENGINE_PLAIN;
+            else if (!strcmp(v, "persistent")) engine = GALN_ENGINE_PERSISTENT;
+            else return usage();
+            ++i;
+            continue;
+        }
+        bwa_args.push_back(a);
+    }
+    galn_opts opt;
+    const char *pos[2] = {nullptr, nullptr};
+    int npos = 0;
+    const char *outfn = nullptr;
+    char err[256] = "";
+    if (galn_opts_parse((int)bwa_args.size(), bwa_args.data(), &opt, pos, 2, &npos, &outfn, err, sizeof(err)) != 0) {
+        fprintf(stderr, "[galn] %s\n", err);
+        return usage();
+    }
+    if (npos != 2) return usage();
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        fprintf(stderr, "[galn] no CUDA device found\n");
+        return 10;
+    }
+    std::vector<int> devs;
+    if (devspec) {
+        for (const char *p = devspec; *p;) {
+            char *e;
+            long d = strtol(p, &e, 10);
+            if (e == p || d < 0 || d >= ndev) { fprintf(stderr, "[galn] --device: no CUDA device '%s'\n", devspec); return 1; }
+            if (std::find(devs.begin(), devs.end(), (int)d) == devs.end()) devs.push_back((int)d);
+            if (*e && *e != ',') { fprintf(stderr, "[galn] --device: bad list '%s'\n", devspec); return 1; }
+            p = *e == ',' ? e + 1 : e;
+        }
+    } else {
+        int k = ngpus > 0 ? std::min(ngpus, ndev) : ndev;
+        for (int d = 0; d < k; ++d) devs.push_back(d);
+    }
+
+    double t0 = now_s();
+    galn_read_set rs;
+    int rr = 0;
+    std::thread reader([&] { rr = galn_fastq_read(pos[1], &rs); });
+    std::vector<galn_index *> ix(devs.size(), nullptr);
+    int ierr = 0;
+    for (size_t g = 0; g < devs.size(); ++g) {
+        int e = 0;
+        ix[g] = galn_index_open(pos[0], devs[g], &e);
+        if (!ix[g]) ierr = e;
+    }
+    reader.join();
+    if (ierr) {
+        fprintf(stderr, "[galn] cannot load the index %s.bwt (%d)\n", pos[0], ierr);
+        return ierr == GALN_ECUDA ? 10 : 2;
+    }
+    if (rr) { fprintf(stderr, "[galn] cannot read %s\n", pos[1]); return 3; }
+    double t_loaded = now_s();
+
+    // shards: contiguous ranges; every shard carries the whole input's longest read per batch
+    const galn_reads &all = rs.reads;
+    int n = all.n_reads;
+    int nb = 0;
+    for (int r = 0; r < n; ++r) nb = std::max(nb, all.batch[r] + 1);
+    std::vector<int32_t> bmax((size_t)std::max(nb, 1), 0);
+    for (int r = 0; r < n; ++r)
+        bmax[all.batch[r]] = std::max(bmax[all.batch[r]], (int32_t)(all.offset[r + 1] - all.offset[r]));
+    size_t G = devs.size();
+    std::vector<galn_results> res(G);
+    std::vector<int> rc(G, 0);
+    std::vector<int> s0(G + 1);
+    for (size_t g = 0; g <= G; ++g) s0[g] = (int)((int64_t)n * (int64_t)g / (int64_t)G);
+    std::vector<std::thread> th;
+    for (size_t g = 0; g < G; ++g)
+        th.emplace_back([&, g] {
+            galn_reads sh;
+            sh.n_reads = s0[g + 1] - s0[g];
+            sh.seq = all.seq;
+            sh.offset = all.offset + s0[g];
+            sh.batch = all.batch + s0[g];
+            sh.batch_max_len = bmax.data();
+            sh.n_batches = nb;
+            rc[g] = galn_aln_run_batch(ix[g], &opt, &sh, engine, &res[g]);
+        });
+    for (auto &t : th) t.join();
+    for (size_t g = 0; g < G; ++g)
+        if (rc[g]) { fprintf(stderr, "[galn] search failed on GPU %d (%d)\n", devs[g], rc[g]); return 10; }
+    double t_search = now_s();
+
+    // one result table in input order
+    galn_results merged;
+    std::vector<int32_t> m_n((size_t)std::max(n, 1));
+    std::vector<int64_t> m_off((size_t)n + 1);
+    std::vector<galn_aln1> m_rec;
+    std::vector<uint64_t> m_pops((size_t)std::max(n, 1)), m_trace((size_t)std::max(n, 1));
+    int64_t t = 0;
+    for (size_t g = 0; g < G; ++g)
+        for (int j = 0; j < res[g].n_reads; ++j) {
+            int r = s0[g] + j;
+            m_n[r] = res[g].n_aln[j];
+            m_off[r] = t;
+            m_pops[r] = res[g].n_pops[j];
+            m_trace[r] = res[g].trace[j];
+            int64_t k = res[g].rec_offset[j + 1] - res[g].rec_offset[j];
+            m_rec.insert(m_rec.end(), res[g].rec + res[g].rec_offset[j], res[g].rec + res[g].rec_offset[j] + k);
+            t += k;
+        }
+    m_off[n] = t;
+    if (m_rec.empty()) m_rec.resize(1);
+    merged.n_reads = n;
+    merged.n_aln = m_n.data();
+    merged.rec_offset = m_off.data();
+    merged.rec = m_rec.data();
+    merged.n_pops = m_pops.data();
+    merged.trace = m_trace.data();
+    merged._priv = nullptr;
+    int werr = galn_sai_write(outfn, &opt, &merged);
+    double t_end = now_s();
+    long mapped = 0;
+    for (int r = 0; r < n; ++r) mapped += m_n[r] > 0;
+    for (int r = 0; r < n; ++r)
+        if (m_n[r] < 0) fprintf(stderr, "[galn] read %d (%s): search error %d\n", r, rs.names[r], m_n[r]);
+    fprintf(stderr, "[galn] %d reads (%ld with hits, %lld records) in %.2f s: load %.2f s, search %.2f s, write %.2f s\n",
+            n, mapped, (long long)t, t_end - t0, t_loaded - t0, t_search - t_loaded, t_end - t_search);
+    if (verbose) {
+        for (size_t g = 0; g < G; ++g) {
+            double ms_tot = 0, ms_k = 0;
+            int tiers = 0;
+            int64_t launches = 0, ovf[8];
+            galn_last_run_stats(ix[g], &ms_tot, &ms_k, &tiers, &launches, ovf);
+            double pops = 0;
+            for (int j = 0; j < res[g].n_reads; ++j) pops += (double)res[g].n_pops[j];
+            fprintf(stderr, "[galn] GPU %d: %d reads, %.2f ms (kernels %.2f ms, %.3e pops/s), %d tiers, %lld launches,"
+                    " overflow T0 %lld T1 %lld T2 %lld\n", devs[g], res[g].n_reads, ms_tot, ms_k,
+                    ms_k > 0 ? pops / (ms_k / 1e3) : 0.0, tiers, (long long)launches, (long long)ovf[0],
+                    (long long)ovf[1], (long long)ovf[2]);
+        }
+    }
+    for (size_t g = 0; g < G; ++g) { galn_results_free(&res[g]); galn_index_close(ix[g]); }
+    galn_read_set_free(&rs);
+    if (werr == 5) { fprintf(stderr, "[galn] error writing the .sai\n"); return 5; }
+    return werr;
+}

@@ -1,0 +1,178 @@
+/* galn_aln.h -- C ABI of galn-b200, the sm_100a (B200) implementation of the `bwa aln` search.
+ *
+ * The reference (G-ALN 0.2.7) has no library API: its drop-in surface is the `galn aln` command line, the
+ * BWA index files and the .sai stream, and its search is reached internally through
+ *     bwtgap_match_gap(bwt, meta, cnt_table, len, seq, width, seed_width, opt, stack, aln, m_aln)
+ *         (src/bwtgap_hd.h:338-341, one read)
+ *     light_kernel(light_args) / gapw_kernel(gapw_args)  (src/galn.cu:93-135, src/gapw.cuh:86-139, 716-795:
+ *         a batch of reads as SoA: query + qoff + qlen, per-read max_diff and batch id, per-batch options)
+ * The entry points below replace those seams; each names the reference code it stands in for. All
+ * pointers are plain host pointers unless a comment says device; sizes are element counts. No call
+ * throws: 0 means success, a negative value is one of the GALN_E* codes.
+ *
+ * Thread safety: an index handle may be used from several host threads at once; calls on it are
+ * serialised internally except galn_aln_submit/galn_aln_wait, which are designed for concurrent use.
+ */
+#ifndef GALN_ALN_H
+#define GALN_ALN_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes (per read, the reference's BWTGAP_ERR_* values, src/bwtgap_hd.h:41-43) ---------- */
+#define GALN_OK            0
+#define GALN_ERR_STACK   (-1)   /* per read: stack capacity exhausted (internal; the library re-runs) */
+#define GALN_ERR_ALN     (-2)   /* per read: record buffer exhausted (internal; the library re-runs) */
+#define GALN_ERR_SCORE   (-3)   /* per read: a push scored >= n_stacks (the reference reports it too) */
+#define GALN_EINVAL      (-20)  /* bad argument */
+#define GALN_EIO         (-21)  /* file missing, short or corrupt */
+#define GALN_ECUDA       (-22)  /* CUDA error, or no sm_100 device */
+#define GALN_ENOMEM      (-23)  /* host or device allocation failed */
+#define GALN_ETIMEOUT    (-24)  /* galn_aln_wait: the request is not finished yet */
+#define GALN_EBUSY       (-25)  /* the serving queue is full */
+
+/* ---- options: BWA's gap_opt_t, 64 bytes, written verbatim as the .sai header (src/sai_format.h:16-27) */
+typedef struct {
+    int32_t s_mm, s_gapo, s_gape;
+    int32_t mode;                       /* 0x01 GAPE, 0x02 COMPREAD, 0x04 LOGGAP, 0x10 NONSTOP */
+    int32_t indel_end_skip, max_del_occ, max_entries;
+    float   fnr;                        /* -n as a fraction, else -1 */
+    int32_t max_diff, max_gapo, max_gape;
+    int32_t max_seed_diff, seed_len;
+    int32_t n_threads;                  /* only the .sai header value (-dt) */
+    int32_t max_top2;
+    int32_t trim_qual;
+} galn_opts;
+
+/* one alignment record, bwt_aln1_t (src/sai_format.h:29-33): packed = n_mm:8 n_gapo:8 n_gape:8
+ * score:20 n_ins:10 n_del:10, then the SA interval [k, l] */
+typedef struct {
+    uint64_t packed, k, l;
+} galn_aln1;
+
+/* BWA 0.7.19 defaults (gap_init_opt; the reference's opt_default, src/opt_build.h:23-36) */
+int galn_opts_default(galn_opts *o);
+
+/* Parses `galn aln` options (the reference's parse_args, src/galn.cu:185-250): every bwa aln option
+ * (-n -o -e -i -d -l -k -m -t/-dt -M -O -E -R -L -N -q0 -f). Positional arguments are returned in
+ * pos[0..*n_pos) (at most max_pos), -f in *out_path (or NULL). Returns 0 or GALN_EINVAL (message in err). */
+int galn_opts_parse(int argc, const char *const *argv, galn_opts *o, const char **pos, int max_pos, int *n_pos,
+                    const char **out_path, char *err, size_t err_len);
+
+/* bwa_cal_maxdiff (src/aln_host.c:9-21): host double arithmetic, no FMA contraction */
+int galn_cal_maxdiff(int len, double err, double thres);
+
+/* ---- index ----------------------------------------------------------------------------------------- */
+typedef struct galn_index galn_index;
+
+/* Loads <prefix>.bwt (the reference's load_bwt, src/host_io.c:29-76) onto `device` and converts it to
+ * the device occurrence layout (32-byte blocks of 64 symbols). The index is read-only afterwards.
+ * Returns NULL on error with *err set. */
+galn_index *galn_index_open(const char *prefix, int device, int *err);
+/* The same from a .bwt already in host memory: the 40-byte header and the body words, as on disk. */
+galn_index *galn_index_open_mem(const void *bwt_file_bytes, size_t n_bytes, int device, int *err);
+int galn_index_close(galn_index *ix);
+/* seq_len (= L2[4]), primary, and the device bytes the occurrence layout takes */
+int galn_index_info(const galn_index *ix, uint64_t *seq_len, uint64_t *primary, uint64_t *device_bytes);
+
+/* ---- reads ------------------------------------------------------------------------------------------- */
+/* A batch of reads as the search takes them: the bases as read (ASCII, any case; A/C/G/T, everything
+ * else ambiguous), concatenated, with n_reads+1 offsets. batch[r] is the bwa batch (bwa_read_seq, 0x40000
+ * reads, src/host_io.c:164-187) of read r; NULL means consecutive batches of 0x40000 in input order.
+ * A batch's options depend on its longest read (src/aln_host.c:23-38): when these reads are a shard of a
+ * larger input, batch_max_len[0..n_batches) gives each batch's longest read in the whole input (NULL: the
+ * longest among these reads). Reads longer than 65535 bases are rejected (GALN_EINVAL): the reference's
+ * stack entry keeps the read position in 16 bits (src/bwtgap_hd.h:365). */
+typedef struct {
+    int32_t n_reads;
+    const char *seq;
+    const int64_t *offset;
+    const int32_t *batch;
+    const int32_t *batch_max_len;
+    int32_t n_batches;
+} galn_reads;
+
+/* Reads a FASTQ/FASTA file (plain or gzip) with the reference's rules (read_fastq, src/host_io.c:151-205):
+ * empty reads skipped, a malformed record dropped and ending its batch. The library owns the memory until
+ * galn_read_set_free. */
+typedef struct {
+    galn_reads reads;
+    char **names;
+    void *_priv;
+} galn_read_set;
+int galn_fastq_read(const char *path, galn_read_set *out);
+int galn_read_set_free(galn_read_set *rs);
+
+/* ---- results ------------------------------------------------------------------------------------------ */
+/* Per read: n_aln (>= 0, or GALN_ERR_SCORE), records rec[rec_offset[r] .. rec_offset[r+1]) in discovery
+ * order (the order the reference writes them), and the instrumentation the reference's --verify compares
+ * (n_pops, trace hash; src/galn.cu:1221-1248). Owned by the library until galn_results_free. */
+typedef struct {
+    int32_t n_reads;
+    int32_t *n_aln;
+    int64_t *rec_offset;
+    galn_aln1 *rec;
+    uint64_t *n_pops;
+    uint64_t *trace;
+    void *_priv;
+} galn_results;
+int galn_results_free(galn_results *res);
+
+/* ---- search ------------------------------------------------------------------------------------------- */
+/* Engines: GALN_ENGINE_PLAIN launches one kernel per bwa batch, one thread per read, and re-runs the reads
+ * that overflow their stack in larger tiers (the reference's light tier, src/galn.cu:835-905, with its
+ * overflow kept on the GPU). GALN_ENGINE_PERSISTENT runs one persistent work-claiming launch over all
+ * batches (captured in a CUDA graph), heavy reads migrating to larger tiers on the device. Both give the
+ * same bytes. */
+#define GALN_ENGINE_PLAIN       0
+#define GALN_ENGINE_PERSISTENT  1
+
+/* Synchronous search of a whole read set (host buffers in, host results out). */
+int galn_aln_run_batch(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);
+
+/* ---- .sai ----------------------------------------------------------------------------------------------- */
+/* "SAI\1", the option block, then per read int32 n_aln and the records (src/sai_writer.h:9-21). A read
+ * with an error code is written with 0 records and the call returns 4 (src/galn.cu:1250-1263); 5 on a
+ * write error. */
+int galn_sai_write(const char *path, const galn_opts *o, const galn_results *res);
+
+/* ---- serving ---------------------------------------------------------------------------------------------- */
+/* A resident index serves requests with their own options and batch boundaries. Requests that arrive
+ * while others run are admitted as device memory for their stacks frees up and share the device with
+ * them; each request's results are the same bytes as a galn_aln_run_batch of it alone. */
+typedef struct galn_server galn_server;
+galn_server *galn_server_start(galn_index *ix, size_t stack_bytes, int *err);
+int galn_server_stop(galn_server *s);
+/* copies the request's inputs; returns a request id > 0, or an error */
+int64_t galn_aln_submit(galn_server *s, const galn_opts *o, const galn_reads *in);
+/* waits up to timeout_ms (-1: forever) for a request; on success moves its results into *out */
+int galn_aln_wait(galn_server *s, int64_t id, int timeout_ms, galn_results *out);
+
+/* Statistics of the last galn_aln_run_batch on this index (no reference counterpart; the reference prints
+ * the same kind of figures with -v, src/galn.cu:1268-1284): wall and kernel milliseconds, tiers used,
+ * kernel launches, and the reads that overflowed each tier (8 entries). */
+int galn_last_run_stats(galn_index *ix, double *ms_total, double *ms_kernels, int *tiers, int64_t *launches,
+                        int64_t *overflow);
+
+/* Device-side profile of the last run (no reference counterpart): the device span from the first to the
+ * last kernel (ms), the kernel time of each tier (8 entries), and, when the index was tuned with
+ * keep_stats, per read the 32-byte index blocks read and the tier that finished it (n entries). */
+int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, uint32_t *fetch, int8_t *tier, int32_t n);
+
+/* Tier capacities (no reference counterpart; set by the autotuner): entries and records per thread in the
+ * first tier, its block size (64/128/256/512), live entries and records per thread in the second tier, and
+ * whether to keep the per-read profile. Results never depend on these values. */
+int galn_index_set_tuning(galn_index *ix, int t0_cap, int t0_aln, int t0_block, int t1_cap, int t1_aln, int keep_stats);
+
+/* library version string */
+const char *galn_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -78,6 +78,11 @@ def parse_aln_args(args: list[str]) -> dict:
                     o["max_diff"], o["fnr"] = int(v), -1.0
             elif a == "-e":
                 opte = int(v)
+            elif a == "-q":
+                if int(v) >= 1:
+                    raise ValueError("-q (quality trimming) is not supported")
+            elif a == "-f":
+                pass
             else:
                 key = {"-o": "max_gapo", "-M": "s_mm", "-O": "s_gapo", "-E": "s_gape", "-d": "max_del_occ",
                        "-i": "indel_end_skip", "-l": "seed_len", "-k": "max_seed_diff", "-m": "max_entries",

@@ -1,0 +1,170 @@
+"""Host-side logic of the C ABI (no GPU needed): the library loads and exports every entry point of
+include/galn_aln.h; option parsing, bwa_cal_maxdiff, the FASTQ reader and the .sai writer agree with the
+oracle and with the reference's golden files."""
+import ctypes as C
+import gzip
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import galn_b200
+import oracle
+from conftest import GOLDEN, ROOT, case_paths, golden_cases
+from galn_b200 import api, build
+
+CASES = golden_cases()
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    build.build()
+    oracle.build()
+
+
+def test_library_exports_every_declared_symbol():
+    header = open(os.path.join(ROOT, "include", "galn_aln.h")).read()
+    names = set(re.findall(r"\b(galn_[a-z0-9_]+)\s*\(", header))
+    assert len(names) >= 15
+    out = subprocess.run(["nm", "-D", "--defined-only", api.lib_path()], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (galn_[a-z0-9_]+)", out))
+    missing = names - exported
+    assert not missing, missing
+    api.lib()
+    assert galn_b200.lib().galn_version().startswith(b"galn-b200")
+
+
+ARGSETS = [
+    [], ["-n", "0.01", "-l", "1024", "-o", "2"], ["-n", "6", "-o", "2", "-e", "6", "-k", "3", "-N"],
+    ["-L", "-n", "3", "-e", "2", "-R", "5", "-dt", "16"], ["-e", "0"], ["-e", "-1"], ["-t", "0"],
+    ["-M", "4", "-O", "9", "-E", "2", "-d", "5", "-i", "3", "-m", "100", "-k", "1", "-l", "20"],
+    ["-q", "0"], ["-n", "5.", "-N", "-L"], ["-n", ".5"],
+]
+
+
+@pytest.mark.parametrize("args", ARGSETS)
+def test_option_block_matches_oracle(args):
+    o = galn_b200.parse_options(args)
+    assert bytes(o) == oracle.opt_bytes(oracle.parse_aln_args(args))
+
+
+def test_option_errors():
+    for bad in (["-q", "2"], ["-x", "1"], ["-n"]):
+        with pytest.raises(galn_b200.GalnError):
+            galn_b200.parse_options(bad)
+
+
+def test_option_block_in_golden_sai(manifest):
+    for name, meta in manifest.items():
+        sai = open(case_paths(name, meta)["sai"], "rb").read()
+        assert bytes(galn_b200.parse_options(meta["opts"])) == sai[4:68], name
+
+
+def test_cal_maxdiff_matches_oracle():
+    for thres in (np.float32(0.04), np.float32(0.01), np.float32(0.001), 0.5):
+        for L in range(0, 400):
+            assert galn_b200.cal_maxdiff(L, 0.02, float(thres)) == oracle.cal_maxdiff(L, 0.02, float(thres)), (L, thres)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fastq_reader_matches_oracle(name):
+    p = case_paths(name, CASES[name])
+    mine = galn_b200.read_fastq(p["fq"])
+    ref = oracle.load_reads(p["fq"])
+    np.testing.assert_array_equal(mine.offset, ref["off"])
+    np.testing.assert_array_equal(mine.batch, ref["batch"])
+    q = oracle.encode_queries(mine.seq, mine.offset)
+    np.testing.assert_array_equal(q, ref["query"])
+
+
+READER_EDGE = [
+    b"@a\nACGT\n+\nIIII\n@b desc\nAC\r\nGT\r\n+\r\nII\r\nII\r\n",
+    b"junk line\n>f1\nACGTN\nacgt\n>f2 c\n\n>f3\nA\n",
+    b"@q1\nAAAA\n+\nII\n@q2\nCCCC\n+\nIIII\n@q3\nGG\n+\n",
+    b"@e\n\n+\n\n@x\nT\n+\nI\n",
+    b"@p\nAC-GT\n+\nIIIII\n@n\nNNNN\n+\n@@@@\n",
+    b"@r\r\nACGT\r\n+\r\nIIII\r\n",
+    b"@t\n\r\nAC\n+\nII",
+    b"@u\nACGT\n+",
+    b"",
+    b"@v\nACGTACGT\n+\nIIII\nIIII\n@w\nA\n+\nI\n",
+]
+
+
+@pytest.mark.parametrize("i", range(len(READER_EDGE)))
+def test_fastq_reader_edge_cases(i, tmp_path):
+    path = str(tmp_path / f"e{i}.fq")
+    with open(path, "wb") as f:
+        f.write(READER_EDGE[i])
+    mine = galn_b200.read_fastq(path)
+    ref = oracle.load_reads(path)
+    np.testing.assert_array_equal(mine.offset, ref["off"])
+    np.testing.assert_array_equal(mine.batch, ref["batch"])
+    np.testing.assert_array_equal(oracle.encode_queries(mine.seq, mine.offset), ref["query"])
+    gz = path + ".gz"
+    with gzip.open(gz, "wb") as f:
+        f.write(READER_EDGE[i])
+    mine2 = galn_b200.read_fastq(gz)
+    np.testing.assert_array_equal(mine2.seq, mine.seq)
+
+
+def test_fastq_reader_against_reference_harness(tmp_path):
+    """The reference's own reader (read_fastq via the dump harness) on the reader edge cases."""
+    if not oracle.ref_available():
+        pytest.skip("reference binaries not built here")
+    ob = oracle.opt_bytes(oracle.parse_aln_args([]))
+    for i, data in enumerate(READER_EDGE):
+        if not data:
+            continue
+        path = str(tmp_path / f"r{i}.fq")
+        with open(path, "wb") as f:
+            f.write(data)
+        d = oracle.ref_dump(os.path.join(GOLDEN, "small", "ref.bwt"), path, ob, str(tmp_path / "d.bin"), 1)
+        mine = galn_b200.read_fastq(path)
+        np.testing.assert_array_equal(np.diff(mine.offset), d["len"])
+        np.testing.assert_array_equal(mine.batch, d["batch"])
+
+
+def test_sai_writer_matches_golden(tmp_path):
+    """galn_sai_write over results taken from the golden .sai reproduces the file byte for byte."""
+    for name, meta in CASES.items():
+        p = case_paths(name, meta)
+        sai = oracle.read_sai(p["sai"])
+        n = len(sai["n_aln"])
+        n_aln = np.ascontiguousarray(sai["n_aln"], np.int32)
+        rec_off = np.zeros(n + 1, np.int64)
+        rec_off[1:] = np.cumsum(np.maximum(n_aln, 0))
+        recs = np.ascontiguousarray(sai["records"]) if len(sai["records"]) else np.zeros(1, api.REC_DTYPE)
+        zeros = np.zeros(max(n, 1), np.uint64)
+        r = api._Results()
+        r.n_reads = n
+        r.n_aln = n_aln.ctypes.data_as(C.POINTER(C.c_int32))
+        r.rec_offset = rec_off.ctypes.data_as(C.POINTER(C.c_int64))
+        r.rec = recs.ctypes.data
+        r.n_pops = zeros.ctypes.data_as(C.POINTER(C.c_uint64))
+        r.trace = zeros.ctypes.data_as(C.POINTER(C.c_uint64))
+        o = galn_b200.parse_options(meta["opts"])
+        out = str(tmp_path / (name + ".sai"))
+        rc = galn_b200.lib().galn_sai_write(out.encode(), C.byref(o), C.byref(r))
+        assert rc == 0
+        assert open(out, "rb").read() == open(p["sai"], "rb").read(), name
+
+
+def test_index_open_without_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(galn_b200.GalnError):
+        galn_b200.Index(os.path.join(GOLDEN, "small", "ref"))
+
+
+def test_cli_usage_and_errors(tmp_path):
+    cli = build.CLI
+    p = subprocess.run([cli], capture_output=True, text=True)
+    assert p.returncode == 1 and "galn aln" in p.stderr
+    p = subprocess.run([cli, "aln", "-q", "3", "a", "b"], capture_output=True, text=True)
+    assert p.returncode == 1
+    p = subprocess.run([cli, "aln", "--cpu-only", "a", "b"], capture_output=True, text=True)
+    assert p.returncode == 1
