@@ -164,6 +164,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-engine comparison")
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--data-dir", default=None)
+    ap.add_argument("--trace", action="store_true", help="compute per-read trace hashes (verification mode)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -206,6 +207,7 @@ def main():
     off_h.numpy()[:] = reads.off
     R = galn_b200.Reads(seq_h.numpy(), off_h.numpy())
     ix = galn_b200.Index(prefix, device=local)
+    ix.set_trace(args.trace)
     engine = galn_b200.GALN_ENGINE_PERSISTENT if args.engine == "persistent" else galn_b200.GALN_ENGINE_PLAIN
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
@@ -260,6 +262,9 @@ def main():
     ix.set_tuning(keep_stats=True)
     galn_b200.aln(ix, opts, R, engine)
     prof = ix.last_profile(n)
+    tiers_info = {"ms": [round(x, 3) for x in prof["ms_tier"]], "reads": prof["tier_reads"],
+                  "threads": prof["tier_threads"],
+                  "fetches_finished": [int(prof["fetch"][prof["tier"] == t].astype(np.int64).sum()) for t in range(8)]}
     fetch_t0 = int(prof["fetch"][prof["tier"] == 0].astype(np.int64).sum())
     fetch_all = int(prof["fetch"].astype(np.int64).sum())
     ix.set_tuning(keep_stats=False)
@@ -279,7 +284,7 @@ def main():
                  "e2e": total_reads / max_over_ranks(statistics.mean(pe2e)), "sai_md5_same": pmd5 == md5}
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_sample > 0:
         cpu, why = cpu_reference(prefix, reads, opts, args.cpu_sample, d)
         if cpu is None:
             log("[bench] cpu baseline unavailable:", why)
@@ -296,7 +301,7 @@ def main():
         "vs_baseline": None, "dtype": "int64",
         "data": "synthetic: seeded reference and reads with the workload's shapes (no public dataset here)",
         "config": {"workload": WORKLOAD_DESC[args.workload], "scale": args.scale, "reads_per_gpu": n,
-                   "options": " ".join(opts), "engine": args.engine,
+                   "options": " ".join(opts), "engine": args.engine, "trace_hashes": bool(args.trace),
                    "l2": "flushed before every step (512 MB device write, outside the timed region)",
                    "parallelism": f"{world} independent GPU shards (reads split, index replicated)"},
         "e2e": {"value": total_reads / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -311,6 +316,7 @@ def main():
         "sai_md5": sorted(md5),
         "deterministic": len(md5) == 1,
         "ms_device_per_step": 1e3 * dev_s,
+        "tiers": tiers_info,
     }
     if plain:
         line["plain_engine"] = plain

@@ -76,8 +76,9 @@ def lib():
     L.galn_sai_write.argtypes = [C.c_char_p, C.POINTER(Options), C.POINTER(_Results)]
     L.galn_last_run_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
-    L.galn_last_run_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), vp, vp, C.c_int32]
+    L.galn_last_run_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), vp, vp, vp, vp, C.c_int32]
     L.galn_index_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.galn_index_set_trace.argtypes = [vp, C.c_int]
     L.galn_version.restype = C.c_char_p
     _lib = L
     return L
@@ -132,18 +133,24 @@ class Index:
         if rc:
             raise GalnError(f"bad tuning ({rc})")
 
+    def set_trace(self, on: bool):
+        lib().galn_index_set_trace(self.h, int(on))
+
     def last_profile(self, n: int = 0) -> dict:
         """Device span and per-tier kernel ms of the last run; with n > 0 (and keep_stats tuning) also the
         per-read 32-byte block fetches and finishing tier."""
         dev = C.c_double()
         tiers = (C.c_double * 8)()
+        treads = np.zeros(8, np.int64)
+        tthreads = np.zeros(8, np.int64)
         fetch = np.zeros(max(n, 1), np.uint32)
         tier = np.zeros(max(n, 1), np.int8)
-        rc = lib().galn_last_run_profile(self.h, C.byref(dev), tiers, fetch.ctypes.data if n else None,
-                                         tier.ctypes.data if n else None, n)
+        rc = lib().galn_last_run_profile(self.h, C.byref(dev), tiers, treads.ctypes.data, tthreads.ctypes.data,
+                                         fetch.ctypes.data if n else None, tier.ctypes.data if n else None, n)
         if rc:
             raise GalnError(f"no profile ({rc})")
-        out = dict(ms_device=dev.value, ms_tier=list(tiers))
+        out = dict(ms_device=dev.value, ms_tier=list(tiers), tier_reads=treads.tolist(),
+                   tier_threads=tthreads.tolist())
         if n:
             out["fetch"] = fetch[:n]
             out["tier"] = tier[:n]

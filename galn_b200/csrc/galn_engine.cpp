@@ -167,6 +167,7 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
     job.seq = (uint8_t *)B.seq.p; job.query = (uint8_t *)B.query.p; job.off = (int64_t *)B.off.p;
     job.bidx = (int32_t *)B.bidx.p; job.maxdiff = (int32_t *)B.maxdiff.p; job.bopt = (HostBatchOpt *)B.bopt.p;
     job.seed_len = o->seed_len; job.max_len = max_len; job.max_stacks = max_stacks; job.any_wide = wide ? 1 : 0;
+    job.trace = ix->trace ? 1 : 0;
     job.out_n = (int32_t *)B.out_n.p; job.out_off = (int64_t *)B.out_off.p; job.out_pops = (uint64_t *)B.out_pops.p;
     job.out_trace = (uint64_t *)B.out_trace.p; job.out_peak = (int32_t *)B.out_peak.p;
     job.out_fetch = (uint32_t *)B.out_fetch.p; job.out_tier = (int8_t *)B.out_tier.p;
@@ -209,6 +210,8 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
             cfg.threads = std::max(cfg.block, cfg.threads / 2);
         }
         RCK(B.ws.ensure(ws_bytes(cfg, job)));
+        S.tier_threads[cfg.tier] = std::max<int64_t>(S.tier_threads[cfg.tier], cfg.threads);
+        S.tier_reads[cfg.tier] += m;
         ECK(cudaMemsetAsync(job.counters, 0, 8, st));
         ECK(cudaEventRecord(e0, st));
         RCK(dev_search(ix->dev, job, cfg, list, m, ovf, B.ws.p, st));
@@ -285,7 +288,9 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
         t.freelist = true;
         t.persistent = true;
         t.block = 128;
-        t.cap = tier == 1 ? ix->t1_cap : (int)std::min<int64_t>((int64_t)o->max_entries + 16, 0x7fffffff);
+        // live entries: t1_cap, then 2^19, then enough for the max_entries cut-off
+        int64_t full = std::min<int64_t>((int64_t)o->max_entries + 16, 0x7fffffff);
+        t.cap = tier == 1 ? ix->t1_cap : tier == 2 ? (int)std::min<int64_t>(full, 1 << 19) : (int)full;
         if (t.cap < 16) t.cap = 16;
         t.aln_cap = (int)std::min<int64_t>(aln_cap, 1 << 24);
         int got = 0;
@@ -364,18 +369,28 @@ extern "C" int galn_last_run_stats(galn_index *ix, double *ms_total, double *ms_
     return 0;
 }
 
-extern "C" int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, uint32_t *fetch, int8_t *tier,
-                                     int32_t n)
+extern "C" int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, int64_t *tier_reads,
+                                     int64_t *tier_threads, uint32_t *fetch, int8_t *tier, int32_t n)
 {
     if (!ix) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
     if (ms_device) *ms_device = ix->last.ms_device;
     if (ms_tier) memcpy(ms_tier, ix->last.ms_tier, sizeof(ix->last.ms_tier));
+    if (tier_reads) memcpy(tier_reads, ix->last.tier_reads, sizeof(ix->last.tier_reads));
+    if (tier_threads) memcpy(tier_threads, ix->last.tier_threads, sizeof(ix->last.tier_threads));
     if (fetch || tier) {
         if ((size_t)n > ix->last.fetch.size()) return GALN_EINVAL;
         if (fetch) memcpy(fetch, ix->last.fetch.data(), (size_t)n * 4);
         if (tier) memcpy(tier, ix->last.tier_of.data(), (size_t)n);
     }
+    return 0;
+}
+
+extern "C" int galn_index_set_trace(galn_index *ix, int on)
+{
+    if (!ix) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    ix->trace = on != 0;
     return 0;
 }
 

@@ -59,6 +59,8 @@ struct RunStats {
     double ms_tier[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int tiers = 0;
     int64_t overflow_reads[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t tier_threads[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t tier_reads[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t kernel_launches = 0;
     std::vector<uint32_t> fetch;     // per read, of the last run
     std::vector<int8_t> tier_of;     // per read, of the last run
@@ -78,6 +80,7 @@ struct galn_index {
     int t1_cap = 65536, t1_aln = 1024;
     double mem_fraction = 0.6;          // of free device memory a job's workspace may take
     bool keep_stats = false;            // keep per-read fetch counts and tiers of the last run
+    bool trace = true;                  // compute the per-read trace hash (the reference's --verify data)
 };
 
 namespace galn {

@@ -44,6 +44,7 @@ struct DevJob {
     int max_len = 0;
     int max_stacks = 0;
     int any_wide = 0;
+    int trace = 0;                     // fold every pop into the per-read trace hash
     // outputs, per read
     int32_t *out_n = nullptr;
     int64_t *out_off = nullptr;

@@ -161,6 +161,7 @@ struct KArgs {
     uint32_t *out_fetch;
     int8_t *out_tier;
     int tier;
+    int trace;
     uint64_t *out_rec;
     unsigned long long *rec_top;
     int64_t rec_cap;
@@ -168,7 +169,7 @@ struct KArgs {
     int32_t *ovf_n;
 };
 
-template <bool WIDE, bool FREELIST>
+template <bool WIDE, bool FREELIST, bool TRACE>
 __device__ __forceinline__ void run_read(const KArgs &a, int pos, int slot)
 {
     const int r = a.list[pos];
@@ -183,7 +184,7 @@ __device__ __forceinline__ void run_read(const KArgs &a, int pos, int slot)
     uint32_t fetches = 0;
     cal_width(a.ix, len, q, W, fetches);
     if (use_seed) cal_width(a.ix, a.seed_len, q + (len - a.seed_len), SW, fetches);
-    SearchResult R = match_gap<WIDE, FREELIST>(a.ix, bo, md, len, q, W, SW, use_seed, a.ws, slot, fetches);
+    SearchResult R = match_gap<WIDE, FREELIST, TRACE>(a.ix, bo, md, len, q, W, SW, use_seed, a.ws, slot, fetches);
     int ret = R.ret;
     if (ret > 0) {
         unsigned long long o = atomicAdd(a.rec_top, (unsigned long long)ret);
@@ -204,19 +205,19 @@ __device__ __forceinline__ void run_read(const KArgs &a, int pos, int slot)
     a.out_tier[r] = (int8_t)a.tier;
 }
 
-template <bool WIDE, bool FREELIST>
-__global__ void __launch_bounds__(128) search_kernel(const __grid_constant__ KArgs a)
+template <bool WIDE, bool FREELIST, bool TRACE>
+__global__ void __launch_bounds__(512) search_kernel(const __grid_constant__ KArgs a)
 {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= a.n_slots) return;
     if (!a.persistent) {
-        if (slot < a.n) run_read<WIDE, FREELIST>(a, slot, slot);
+        if (slot < a.n) run_read<WIDE, FREELIST, TRACE>(a, slot, slot);
         return;
     }
     for (;;) {
         int pos = atomicAdd(a.claim, 1);
         if (pos >= a.n) break;
-        run_read<WIDE, FREELIST>(a, pos, slot);
+        run_read<WIDE, FREELIST, TRACE>(a, pos, slot);
     }
 }
 
@@ -252,7 +253,8 @@ template <bool WIDE, bool FREELIST>
 static int launch(const KArgs &a, int threads, int block, cudaStream_t st)
 {
     unsigned grid = (unsigned)((threads + block - 1) / block);
-    search_kernel<WIDE, FREELIST><<<grid, block, 0, st>>>(a);
+    if (a.trace) search_kernel<WIDE, FREELIST, true><<<grid, block, 0, st>>>(a);
+    else search_kernel<WIDE, FREELIST, false><<<grid, block, 0, st>>>(a);
     GALN_CUDA(cudaGetLastError());
     return 0;
 }
@@ -284,6 +286,7 @@ int dev_search(const DevIndex &ix, DevJob &job, const TierCfg &cfg, const int32_
     a.ws.aln_cap = cfg.aln_cap;
     a.out_n = job.out_n; a.out_off = job.out_off; a.out_pops = job.out_pops; a.out_trace = job.out_trace;
     a.out_peak = job.out_peak; a.out_fetch = job.out_fetch; a.out_tier = job.out_tier; a.tier = cfg.tier;
+    a.trace = job.trace;
     a.out_rec = job.out_rec; a.rec_top = job.rec_top; a.rec_cap = job.rec_cap;
     a.ovf = ovf; a.ovf_n = job.counters + 1;
     if (!cfg.persistent && cfg.threads < n) return -20;
@@ -298,11 +301,11 @@ int dev_resident_threads(const TierCfg &cfg, bool wide, int device)
     int bps = 0;
     cudaError_t e;
     if (wide)
-        e = cfg.freelist ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<true, true>, cfg.block, 0)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<true, false>, cfg.block, 0);
+        e = cfg.freelist ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<true, true, true>, cfg.block, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<true, false, true>, cfg.block, 0);
     else
-        e = cfg.freelist ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<false, true>, cfg.block, 0)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<false, false>, cfg.block, 0);
+        e = cfg.freelist ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<false, true, true>, cfg.block, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<false, false, true>, cfg.block, 0);
     if (e != cudaSuccess) return -22;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);

@@ -88,6 +88,12 @@ __device__ __forceinline__ int match_exact_alt(const IndexView &ix, int len, con
     return (int)(l - k + 1);
 }
 
+__device__ __forceinline__ uint64_t sel4(int c, uint64_t a0, uint64_t a1, uint64_t a2, uint64_t a3)
+{
+    uint64_t lo = (c & 1) ? a1 : a0, hi = (c & 1) ? a3 : a2;
+    return (c & 2) ? hi : lo;
+}
+
 struct Entry {
     uint64_t k, l;
     uint32_t info;
@@ -147,7 +153,7 @@ __device__ __forceinline__ void load_entry(const uint4 *ent, int idx, int score,
 
 // One read. q: reversed+complemented codes (0..3, 4 ambiguous). W / SW: width and seed width, already
 // computed. Records go to aln (3 uint64 each). Returns the search result (n_aln or an error code).
-template <bool WIDE, bool FREELIST>
+template <bool WIDE, bool FREELIST, bool TRACE>
 __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int max_diff0, int len, const uint8_t *q,
                                   uint64_t *W, uint64_t *SW, bool use_seed, const Workspace &ws, int slot,
                                   uint32_t fetches)
@@ -222,7 +228,7 @@ __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int ma
                 }
             }
             ++pops;
-            {
+            if (TRACE) {
                 uint64_t h = trace;
                 h = trace_mix(h, e.info);
                 h = trace_mix(h, e.k);
@@ -287,6 +293,11 @@ __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int ma
             --i;
             uint64_t ck[4], cl[4];
             occ4_pair(ix, k - 1, l, ck, cl, fetches);
+            // child intervals of the four bases, in registers
+            const uint64_t kk0 = ix.C[0] + ck[0] + 1, ll0 = ix.C[0] + cl[0];
+            const uint64_t kk1 = ix.C[1] + ck[1] + 1, ll1 = ix.C[1] + cl[1];
+            const uint64_t kk2 = ix.C[2] + ck[2] + 1, ll2 = ix.C[2] + cl[2];
+            const uint64_t kk3 = ix.C[3] + ck[3] + 1, ll3 = ix.C[3] + cl[3];
             uint64_t occ = l - k + 1;
             int allow_diff = 1, allow_M = 1;
             if (i > 0) {
@@ -309,8 +320,9 @@ __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int ma
                 if (e.state == kStM) {
                     if (e.n_gapo < O.max_gapo) {
                         GALN_PUSH(b0 + s_gapo, i, k, l, e.n_mm, e.n_gapo + 1, e.n_gape, e.n_ins + 1, e.n_del, kStI, 1);
+#pragma unroll
                         for (int c = 0; c < 4; ++c) {
-                            uint64_t kk = ix.C[c] + ck[c] + 1, ll = ix.C[c] + cl[c];
+                            uint64_t kk = sel4(c, kk0, kk1, kk2, kk3), ll = sel4(c, ll0, ll1, ll2, ll3);
                             if (kk <= ll)
                                 GALN_PUSH(b0 + s_gapo, i + 1, kk, ll, e.n_mm, e.n_gapo + 1, e.n_gape, e.n_ins, e.n_del + 1, kStD, 1);
                         }
@@ -320,8 +332,9 @@ __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int ma
                         GALN_PUSH(b0 + s_gape, i, k, l, e.n_mm, e.n_gapo, e.n_gape + 1, e.n_ins + 1, e.n_del, kStI, 1);
                 } else if (e.state == kStD) {
                     if (e.n_gape < O.max_gape && (gaps < max_diff || occ < (uint64_t)(int64_t)O.max_del_occ)) {
+#pragma unroll
                         for (int c = 0; c < 4; ++c) {
-                            uint64_t kk = ix.C[c] + ck[c] + 1, ll = ix.C[c] + cl[c];
+                            uint64_t kk = sel4(c, kk0, kk1, kk2, kk3), ll = sel4(c, ll0, ll1, ll2, ll3);
                             if (kk <= ll)
                                 GALN_PUSH(b0 + s_gape, i + 1, kk, ll, e.n_mm, e.n_gapo, e.n_gape + 1, e.n_ins, e.n_del + 1, kStD, 1);
                         }
@@ -330,10 +343,11 @@ __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int ma
             }
             const int base = q[i];
             if (allow_diff && allow_M) {
+#pragma unroll
                 for (int j = 1; j <= 4; ++j) {
                     int c = (base + j) & 3;
                     int mm = j != 4 || base > 3;
-                    uint64_t kk = ix.C[c] + ck[c] + 1, ll = ix.C[c] + cl[c];
+                    uint64_t kk = sel4(c, kk0, kk1, kk2, kk3), ll = sel4(c, ll0, ll1, ll2, ll3);
                     if (kk <= ll) {
                         if (!mm && fuse) {
                             e.k = kk; e.l = ll; e.info = (uint32_t)b0 << 21 | (uint32_t)i; e.ldp = 0; e.state = kStM;
@@ -344,7 +358,7 @@ __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int ma
                     }
                 }
             } else if (base < 4) {
-                uint64_t kk = ix.C[base] + ck[base] + 1, ll = ix.C[base] + cl[base];
+                uint64_t kk = sel4(base, kk0, kk1, kk2, kk3), ll = sel4(base, ll0, ll1, ll2, ll3);
                 if (kk <= ll) {
                     if (fuse) {
                         e.k = kk; e.l = ll; e.info = (uint32_t)b0 << 21 | (uint32_t)i; e.ldp = 0; e.state = kStM;

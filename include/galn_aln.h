@@ -159,14 +159,21 @@ int galn_last_run_stats(galn_index *ix, double *ms_total, double *ms_kernels, in
                         int64_t *overflow);
 
 /* Device-side profile of the last run (no reference counterpart): the device span from the first to the
- * last kernel (ms), the kernel time of each tier (8 entries), and, when the index was tuned with
- * keep_stats, per read the 32-byte index blocks read and the tier that finished it (n entries). */
-int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, uint32_t *fetch, int8_t *tier, int32_t n);
+ * last kernel (ms); per tier (8 entries each) its kernel ms, the reads it was given and the threads it
+ * ran; and, when the index was tuned with keep_stats, per read the 32-byte index blocks read and the tier
+ * that finished it (n entries). Any pointer may be NULL. */
+int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, int64_t *tier_reads, int64_t *tier_threads,
+                          uint32_t *fetch, int8_t *tier, int32_t n);
 
 /* Tier capacities (no reference counterpart; set by the autotuner): entries and records per thread in the
  * first tier, its block size (64/128/256/512), live entries and records per thread in the second tier, and
  * whether to keep the per-read profile. Results never depend on these values. */
 int galn_index_set_tuning(galn_index *ix, int t0_cap, int t0_aln, int t0_block, int t1_cap, int t1_aln, int keep_stats);
+
+/* Trace hashes on or off (on by default). The reference computes them only in its --verify mode
+ * (gapw_kernel<TRACE>, src/gapw.cuh:716-795); off, the kernels skip the hash and results carry 0 in
+ * trace[]. n_aln, records and n_pops are unaffected. */
+int galn_index_set_trace(galn_index *ix, int on);
 
 /* library version string */
 const char *galn_version(void);
