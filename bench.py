@@ -165,6 +165,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--data-dir", default=None)
     ap.add_argument("--trace", action="store_true", help="compute per-read trace hashes (verification mode)")
+    ap.add_argument("--t0-cap", type=int, default=4096, help="first-tier stack entries per thread")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -208,6 +209,7 @@ def main():
     R = galn_b200.Reads(seq_h.numpy(), off_h.numpy())
     ix = galn_b200.Index(prefix, device=local)
     ix.set_trace(args.trace)
+    ix.set_tuning(t0_cap=args.t0_cap)
     engine = galn_b200.GALN_ENGINE_PERSISTENT if args.engine == "persistent" else galn_b200.GALN_ENGINE_PLAIN
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
@@ -259,7 +261,7 @@ def main():
     total_reads = n * world
 
     # roofline of the dominant kernel: algorithmic block fetches of the reads the first tier finished
-    ix.set_tuning(keep_stats=True)
+    ix.set_tuning(t0_cap=args.t0_cap, keep_stats=True)
     galn_b200.aln(ix, opts, R, engine)
     prof = ix.last_profile(n)
     tiers_info = {"ms": [round(x, 3) for x in prof["ms_tier"]], "reads": prof["tier_reads"],
@@ -267,7 +269,7 @@ def main():
                   "fetches_finished": [int(prof["fetch"][prof["tier"] == t].astype(np.int64).sum()) for t in range(8)]}
     fetch_t0 = int(prof["fetch"][prof["tier"] == 0].astype(np.int64).sum())
     fetch_all = int(prof["fetch"].astype(np.int64).sum())
-    ix.set_tuning(keep_stats=False)
+    ix.set_tuning(t0_cap=args.t0_cap, keep_stats=False)
     peak, peak_kind = peaks()
     achieved = 32.0 * fetch_t0 / t0_s / 1e9
     traffic = None
