@@ -79,6 +79,7 @@ def lib():
     L.galn_last_run_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), vp, vp, vp, vp, C.c_int32]
     L.galn_index_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L.galn_index_set_trace.argtypes = [vp, C.c_int]
+    L.galn_index_set_warp_tier.argtypes = [vp, C.c_int, C.c_int]
     L.galn_version.restype = C.c_char_p
     _lib = L
     return L
@@ -132,6 +133,10 @@ class Index:
         rc = lib().galn_index_set_tuning(self.h, t0_cap, t0_aln, t0_block, t1_cap, t1_aln, int(keep_stats))
         if rc:
             raise GalnError(f"bad tuning ({rc})")
+
+    def set_warp_tier(self, on: bool, arena_chunks: int = 1 << 14):
+        if lib().galn_index_set_warp_tier(self.h, int(on), arena_chunks):
+            raise GalnError("bad warp tier setting")
 
     def set_trace(self, on: bool):
         lib().galn_index_set_trace(self.h, int(on))

@@ -261,8 +261,59 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
     S.overflow_reads[0] = n_ovf;
     std::swap(cur, nxt);
 
-    // ---- T1, T2, ... ----
-    int tier = 1;
+    // ---- W: the warp tier for the reads that overflowed T0 (those it can take) ----
+    const bool warp_ok = ix->use_warp && !wide && o->s_mm > 0 && o->s_gapo > 0 && o->s_gape > 0;
+    if (warp_ok && n_ovf > 0) {
+        std::vector<int32_t> ov((size_t)n_ovf), elig, rest;
+        ECK(cudaMemcpyAsync(ov.data(), cur, (size_t)n_ovf * 4, cudaMemcpyDeviceToHost, st));
+        ECK(cudaStreamSynchronize(st));
+        for (int32_t r : ov) {
+            int len = (int)(in->offset[r + 1] - in->offset[r]);
+            if (len <= kWarpMaxLen && bopt[bid[r]].n_stacks <= kWarpMaxStacks && bopt[bid[r]].n_stacks > 0) elig.push_back(r);
+            else rest.push_back(r);
+        }
+        int ne = (int)elig.size();
+        if (ne > 0) {
+            int res_w = warp_resident(ix->dev.device);
+            if (res_w <= 0) return GALN_ECUDA;
+            int nw = std::min(ne, res_w);
+            int arena = ix->warp_arena;
+            const int aln_cap_w = 4096;
+            while (nw > 1 && warp_ws_bytes(nw, arena, aln_cap_w) > budget) nw /= 2;
+            while (arena > 1024 && warp_ws_bytes(nw, arena, aln_cap_w) > budget) arena /= 2;
+            RCK(B.ws.ensure(warp_ws_bytes(nw, arena, aln_cap_w)));
+            ECK(cudaMemcpyAsync(cur, elig.data(), (size_t)ne * 4, cudaMemcpyHostToDevice, st));
+            ECK(cudaMemsetAsync(job.counters, 0, 8, st));
+            ECK(cudaEventRecord(e0, st));
+            RCK(dev_search_warp(ix->dev, job, nw, arena, aln_cap_w, 1, cur, ne, nxt, B.ws.p, st));
+            ECK(cudaEventRecord(e1, st));
+            ECK(cudaMemcpyAsync(h_cnt, job.counters, 8, cudaMemcpyDeviceToHost, st));
+            ECK(cudaStreamSynchronize(st));
+            float ms = 0;
+            ECK(cudaEventElapsedTime(&ms, e0, e1));
+            k_ms += ms;
+            S.ms_tier[1] += ms;
+            S.tier_threads[1] = (int64_t)nw * 32;
+            S.tier_reads[1] = ne;
+            S.kernel_launches += 1;
+            int got = h_cnt[1];
+            S.overflow_reads[1] = got;
+            std::vector<int32_t> wov((size_t)got);
+            if (got) {
+                ECK(cudaMemcpyAsync(wov.data(), nxt, (size_t)got * 4, cudaMemcpyDeviceToHost, st));
+                ECK(cudaStreamSynchronize(st));
+            }
+            rest.insert(rest.end(), wov.begin(), wov.end());
+        }
+        n_ovf = (int)rest.size();
+        if (n_ovf) {
+            ECK(cudaMemcpyAsync(cur, rest.data(), (size_t)n_ovf * 4, cudaMemcpyHostToDevice, st));
+            ECK(cudaStreamSynchronize(st));
+        }
+    }
+
+    // ---- T1, T2, ... (tiers 2..7 in the statistics) ----
+    int tier = 2;
     int64_t aln_cap = ix->t1_aln;
     while (n_ovf > 0 && tier < 8) {
         // make room for records: grow the record buffer when it is more than half used
@@ -290,7 +341,7 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
         t.block = 128;
         // live entries: t1_cap, then 2^19, then enough for the max_entries cut-off
         int64_t full = std::min<int64_t>((int64_t)o->max_entries + 16, 0x7fffffff);
-        t.cap = tier == 1 ? ix->t1_cap : tier == 2 ? (int)std::min<int64_t>(full, 1 << 19) : (int)full;
+        t.cap = tier == 2 ? ix->t1_cap : tier == 3 ? (int)std::min<int64_t>(full, 1 << 19) : (int)full;
         if (t.cap < 16) t.cap = 16;
         t.aln_cap = (int)std::min<int64_t>(aln_cap, 1 << 24);
         int got = 0;
@@ -298,7 +349,7 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
         S.overflow_reads[tier] = got;
         n_ovf = got;
         std::swap(cur, nxt);
-        if (tier >= 2) aln_cap *= 16;
+        if (tier >= 3) aln_cap *= 16;
         else aln_cap = 65536;
         ++tier;
     }
@@ -383,6 +434,15 @@ extern "C" int galn_last_run_profile(galn_index *ix, double *ms_device, double *
         if (fetch) memcpy(fetch, ix->last.fetch.data(), (size_t)n * 4);
         if (tier) memcpy(tier, ix->last.tier_of.data(), (size_t)n);
     }
+    return 0;
+}
+
+extern "C" int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks)
+{
+    if (!ix || arena_chunks < 64) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    ix->use_warp = on != 0;
+    ix->warp_arena = arena_chunks;
     return 0;
 }
 

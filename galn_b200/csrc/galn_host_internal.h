@@ -81,6 +81,8 @@ struct galn_index {
     double mem_fraction = 0.6;          // of free device memory a job's workspace may take
     bool keep_stats = false;            // keep per-read fetch counts and tiers of the last run
     bool trace = true;                  // compute the per-read trace hash (the reference's --verify data)
+    bool use_warp = true;               // the warp tier for reads that overflow T0
+    int warp_arena = 1 << 14;           // 32-entry chunks per warp
 };
 
 namespace galn {

@@ -85,4 +85,13 @@ int dev_search(const DevIndex &ix, DevJob &job, const TierCfg &cfg, const int32_
 // Occupancy: resident threads per SM for a tier's kernel at the given block size
 int dev_resident_threads(const TierCfg &cfg, bool wide, int device);
 
+// The warp tier: one warp per read over list[0..n), each warp with an arena of arena_chunks 32-entry chunks
+// and aln_cap records; reads it cannot finish go to ovf[]. ws_mem holds warp_ws_bytes(...) bytes.
+constexpr int kWarpMaxLen = 256, kWarpMaxStacks = 256;
+size_t warp_smem_bytes();
+int warp_resident(int device);
+size_t warp_ws_bytes(int n_warps, int arena_chunks, int aln_cap);
+int dev_search_warp(const DevIndex &ix, DevJob &job, int n_warps, int arena_chunks, int aln_cap, int tier,
+                    const int32_t *list, int n, int32_t *ovf, void *ws_mem, cudaStream_t st);
+
 }  // namespace galn

@@ -7,6 +7,7 @@
 
 #include "galn_internal.h"
 #include "galn_search.cuh"
+#include "galn_warp.cuh"
 
 namespace galn {
 
@@ -310,6 +311,62 @@ int dev_resident_threads(const TierCfg &cfg, bool wide, int device)
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return bps * cfg.block * sms;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// the warp tier
+
+size_t warp_smem_bytes() { return sizeof(WarpSmem); }
+
+int warp_resident(int device)
+{
+    int bps = 0;
+    size_t smem = sizeof(WarpSmem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, warp_kernel<false>, 32, smem) != cudaSuccess) return -22;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return bps * sms;
+}
+
+size_t warp_ws_bytes(int n_warps, int arena_chunks, int aln_cap)
+{
+    size_t w = (size_t)n_warps;
+    return align256(w * arena_chunks * kWCH * 16) + 2 * align256(w * arena_chunks * 4) + align256(w * aln_cap * 24);
+}
+
+int dev_search_warp(const DevIndex &ix, DevJob &job, int n_warps, int arena_chunks, int aln_cap, int tier,
+                    const int32_t *list, int n, int32_t *ovf, void *ws_mem, cudaStream_t st)
+{
+    if (n == 0) return 0;
+    WArgs a;
+    memset(&a, 0, sizeof(a));
+    a.ix.blk = (const uint4 *)ix.blocks;
+    a.ix.primary = ix.primary;
+    a.ix.seq_len = ix.seq_len;
+    for (int c = 0; c < 4; ++c) a.ix.C[c] = ix.L2[c];
+    memcpy(a.ix.sb, ix.sb, sizeof(a.ix.sb));
+    a.query = job.query; a.off = job.off; a.bidx = job.bidx; a.maxdiff = job.maxdiff;
+    a.bopt = (const BatchOpt *)job.bopt; a.seed_len = job.seed_len;
+    a.list = list; a.n = n; a.claim = job.counters; a.n_warps = n_warps;
+    size_t w = (size_t)n_warps;
+    char *base = (char *)ws_mem;
+    a.chunks = (uint4 *)base;
+    base += align256(w * arena_chunks * kWCH * 16);
+    a.chunk_prev = (int32_t *)base;
+    base += align256(w * arena_chunks * 4);
+    a.free_ids = (int32_t *)base;
+    base += align256(w * arena_chunks * 4);
+    a.aln = (uint64_t *)base;
+    a.arena_chunks = arena_chunks; a.aln_cap = aln_cap;
+    a.out_n = job.out_n; a.out_off = job.out_off; a.out_pops = job.out_pops; a.out_trace = job.out_trace;
+    a.out_peak = job.out_peak; a.out_fetch = job.out_fetch; a.out_tier = job.out_tier; a.tier = tier;
+    a.out_rec = job.out_rec; a.rec_top = job.rec_top; a.rec_cap = job.rec_cap;
+    a.ovf = ovf; a.ovf_n = job.counters + 1;
+    size_t smem = sizeof(WarpSmem);
+    if (job.trace) warp_kernel<true><<<n_warps, 32, smem, st>>>(a);
+    else warp_kernel<false><<<n_warps, 32, smem, st>>>(a);
+    GALN_CUDA(cudaGetLastError());
+    return 0;
 }
 
 }  // namespace galn

@@ -170,6 +170,10 @@ int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, in
  * whether to keep the per-read profile. Results never depend on these values. */
 int galn_index_set_tuning(galn_index *ix, int t0_cap, int t0_aln, int t0_block, int t1_cap, int t1_aln, int keep_stats);
 
+/* The heavy-read warp tier on or off, and its stack arena per warp in 32-entry chunks (no reference
+ * counterpart; on by default with 16384 chunks). Results never depend on it. */
+int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks);
+
 /* Trace hashes on or off (on by default). The reference computes them only in its --verify mode
  * (gapw_kernel<TRACE>, src/gapw.cuh:716-795); off, the kernels skip the hash and results carry 0 in
  * trace[]. n_aln, records and n_pops are unaffected. */

@@ -46,20 +46,30 @@ def test_golden_case(name, engine):
     np.testing.assert_array_equal(res.trace, pr["trace"])
 
 
+@pytest.mark.parametrize("warp", [(True, 16384), (True, 64), (False, 64)])
 @pytest.mark.parametrize("caps", [(16, 1, 64, 16, 1), (64, 2, 256, 128, 2), (300, 4, 128, 1000, 3)])
-def test_tier_migration_gives_same_bytes(caps):
-    """Tiny first- and second-tier capacities push many reads through every tier; the bytes stay the same."""
+def test_tier_migration_gives_same_bytes(caps, warp):
+    """Tiny first- and second-tier capacities push many reads through every tier (the warp tier with a
+    normal and a tiny arena, or without it); the bytes and traces stay the reference's."""
     ix = galn_b200.Index(os.path.join(GOLDEN, "small", "ref"))
     t0_cap, t0_aln, block, t1_cap, t1_aln = caps
     ix.set_tuning(t0_cap, t0_aln, block, t1_cap, t1_aln, keep_stats=True)
+    ix.set_warp_tier(*warp)
     for name in ("adna", "divergent", "edge_nonstop", "tiny_queue"):
         meta = CASES[name]
         p = case_paths(name, meta)
+        rd = oracle.load_reads(p["fq"])
+        o = oracle.aln(oracle.Index(os.path.join(GOLDEN, meta["ref"], "ref.bwt")),
+                       oracle.opt_bytes(oracle.parse_aln_args(meta["opts"])), rd["query"], rd["off"], rd["len"],
+                       rd["batch"], 4)
         for engine in ENGINES:
             res = galn_b200.aln(ix, meta["opts"], p["fq"], engine)
             assert res.sai_bytes() == open(p["sai"], "rb").read(), (name, engine)
             pr = np.load(p["per_read"])
             np.testing.assert_array_equal(res.trace, pr["trace"])
+            np.testing.assert_array_equal(res.pops, pr["pops"])
+            prof = ix.last_profile(len(res))
+            np.testing.assert_array_equal(prof["fetch"].astype(np.uint64), o.fetch64)
         st = ix.last_stats()
         assert st["tiers"] >= 2 or name in ("edge_nonstop", "tiny_queue")
 
