@@ -50,7 +50,7 @@ struct WarpSmem {
     uint4 hz[32];                     // hazard entry of each lane
     uint64_t hk[32], hl[32];          // its interval after the exact tail
     int32_t lane_np[32], lane_end[32], lane_nb[32];
-    uint32_t lane_f[32];              // index blocks read by each lane's chain
+    uint16_t pf[32][kWR];             // index blocks read by each pop of each lane's chain
     uint4 lane_x[32];                 // pending exact child of a lane that stopped mid-chain
     int32_t newc[32];                 // chunks allocated for one commit
 };
@@ -139,7 +139,6 @@ __device__ __forceinline__ void lane_chain(const IndexView &ix, const BatchOpt &
                                            WEnt x, int b, uint32_t &fetches)
 {
     int np = 0, nb = 0, endc = 0;
-    const uint32_t f_start = fetches;
     // a push of the expansion below; a score at or past n_stacks ends the read
 #define WPUSH(BKT, ...)                                                                 \
     do {                                                                                \
@@ -151,24 +150,27 @@ __device__ __forceinline__ void lane_chain(const IndexView &ix, const BatchOpt &
     } while (0)
     for (;;) {
         bool err = false;
+        const uint32_t f_pop = fetches;
         if (TRACE) S->prec[lane][np] = wpack(x);
         int diffs = x.n_mm + x.n_gapo + (c.gape ? x.n_gape : 0);
         int m = c.max_diff - diffs;
         int i = x.i;
         uint8_t npu = 0, hx = 0;
         if (m < 0 || (i > 0 && m < (int)(S->W[i - 1] >> 48))) {
-            S->npush[lane][np] = 0; S->hasx[lane][np] = 0; ++np; endc = 0; break;
+            S->npush[lane][np] = 0; S->hasx[lane][np] = 0; S->pf[lane][np] = 0; ++np; endc = 0; break;
         }
         if (i == 0) {
             S->hz[lane] = wpack(x); S->hk[lane] = x.k; S->hl[lane] = x.l;
-            S->npush[lane][np] = 0; S->hasx[lane][np] = 0; ++np; endc = 1; break;
+            S->npush[lane][np] = 0; S->hasx[lane][np] = 0; S->pf[lane][np] = 0; ++np; endc = 1; break;
         }
         if (m == 0 && (x.state == kStM || c.gape || x.n_gape == O.max_gape)) {
             uint64_t k = x.k, l = x.l;
-            S->npush[lane][np] = 0; S->hasx[lane][np] = 0; ++np;
+            S->npush[lane][np] = 0; S->hasx[lane][np] = 0;
             if (match_exact_alt(ix, i, S->q, k, l, fetches)) {
                 S->hz[lane] = wpack(x); S->hk[lane] = k; S->hl[lane] = l; endc = 1;
             } else endc = 0;
+            S->pf[lane][np] = (uint16_t)(fetches - f_pop);
+            ++np;
             break;
         }
         --i;
@@ -237,6 +239,7 @@ __device__ __forceinline__ void lane_chain(const IndexView &ix, const BatchOpt &
             uint64_t kk = sel4(base, kk0, kk1, kk2, kk3), ll = sel4(base, ll0, ll1, ll2, ll3);
             if (kk <= ll) { exact = true; ek = kk; el = ll; }
         }
+        S->pf[lane][np] = (uint16_t)(fetches - f_pop);
         if (err) {   // the read ends at this pop with BWTGAP_ERR_SCORE
             S->npush[lane][np] = 0; S->hasx[lane][np] = 0; ++np; endc = 3; break;
         }
@@ -251,7 +254,6 @@ __device__ __forceinline__ void lane_chain(const IndexView &ix, const BatchOpt &
     S->lane_np[lane] = np;
     S->lane_end[lane] = endc;
     S->lane_nb[lane] = nb;
-    S->lane_f[lane] = fetches - f_start;
 }
 
 // the warp's chunk allocator (warp-uniform state; lane 0 writes)
@@ -390,6 +392,7 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                     if (n_entries > O.max_entries) { search_end = true; stop = true; break; }
                     --n_entries;
                     ++pops;
+                    f_alg += S->pf[j][t];
                     if (TRACE) {
                         WEnt y = wunpack(S->prec[j][t]);
                         uint64_t h = trace;
@@ -459,7 +462,6 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                 consumed = j + 1;
                 if (endc == 2) { new_pend = true; stop = true; }
             }
-            for (int j = 0; j < consumed; ++j) f_alg += S->lane_f[j];
             if (search_end) break;
             // take the consumed entries off bucket b (lane 0 of the wave may have been the pending child)
             int C = consumed - (pend ? 1 : 0);
