@@ -232,13 +232,20 @@ class Results:
     def __init__(self, r: _Results, opts: Options):
         n = r.n_reads
         self.opts = opts
-        self.n_aln = np.ctypeslib.as_array(r.n_aln, (max(n, 1),))[:n].copy()
+        if n == 0:
+            self.n_aln = np.zeros(0, np.int32)
+            self.rec_offset = np.zeros(1, np.int64)
+            self.records = np.zeros(0, REC_DTYPE)
+            self.pops = np.zeros(0, np.uint64)
+            self.trace = np.zeros(0, np.uint64)
+            return
+        self.n_aln = np.ctypeslib.as_array(r.n_aln, (n,)).copy()
         self.rec_offset = np.ctypeslib.as_array(r.rec_offset, (n + 1,)).copy()
         tot = int(self.rec_offset[-1])
         self.records = (np.frombuffer((C.c_char * (24 * tot)).from_address(r.rec), REC_DTYPE).copy()
                         if tot else np.zeros(0, REC_DTYPE))
-        self.pops = np.ctypeslib.as_array(r.n_pops, (max(n, 1),))[:n].copy()
-        self.trace = np.ctypeslib.as_array(r.trace, (max(n, 1),))[:n].copy()
+        self.pops = np.ctypeslib.as_array(r.n_pops, (n,)).copy()
+        self.trace = np.ctypeslib.as_array(r.trace, (n,)).copy()
 
     def __len__(self):
         return len(self.n_aln)
