@@ -152,6 +152,27 @@ int64_t galn_aln_submit(galn_server *s, const galn_opts *o, const galn_reads *in
 /* waits up to timeout_ms (-1: forever) for a request; on success moves its results into *out */
 int galn_aln_wait(galn_server *s, int64_t id, int timeout_ms, galn_results *out);
 
+/* ---- search without device allocation --------------------------------------------------------------
+ * No counterpart in the reference. For callers that may not allocate or free device memory while they
+ * search (a host framework that owns all GPU memory through its own pool, a stage running under a fixed
+ * memory budget, or code that must not trigger the device synchronisation cudaFree implies): the first
+ * search tier on reads that already sit in the caller's device buffers, with every byte of scratch taken
+ * from one 32 MiB array inside the library (a __device__ array: every GPU that loads the library keeps it
+ * until the process exits). Nothing is allocated: no cudaMalloc, cudaFree or allocating library call.
+ *   d_seq, d_offset   device: ASCII reads and n_reads+1 offsets; all reads are one bwa batch (at most
+ *                     0x40000 reads) whose longest read is max_len (<= 1024 bases)
+ *   d_n_aln           device, n_reads: n_aln, GALN_ERR_SCORE, or GALN_ERR_STACK / GALN_ERR_ALN when the read
+ *                     needed more than the fixed per-thread stack (2048 entries) or more than rec_per_read
+ *                     records (<= 256); such reads can be searched again with galn_aln_run_batch
+ *   d_rec             device, n_reads * rec_per_read records; read r's at d_rec[r * rec_per_read]
+ * Runs asynchronously on `stream` (a cudaStream_t; NULL for the default stream). The first call on a device
+ * looks up the array's device address and should come before any stream capture. All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the caller. Sizes past the limits
+ * above return GALN_EINVAL; options that need more than 512 score buckets or negative penalties too. */
+int galn_aln_run_noalloc(galn_index *ix, const galn_opts *o, int32_t n_reads, int32_t max_len, const char *d_seq,
+                         const int64_t *d_offset, int32_t *d_n_aln, galn_aln1 *d_rec, int32_t rec_per_read,
+                         void *stream);
+
 /* Statistics of the last galn_aln_run_batch on this index (no reference counterpart; the reference prints
  * the same kind of figures with -v, src/galn.cu:1268-1284): wall and kernel milliseconds, tiers used,
  * kernel launches, and the reads that overflowed each tier (8 entries). */
