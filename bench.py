@@ -267,6 +267,7 @@ def main():
     tiers_info = {"ms": [round(x, 3) for x in prof["ms_tier"]], "reads": prof["tier_reads"],
                   "threads": prof["tier_threads"],
                   "fetches_finished": [int(prof["fetch"][prof["tier"] == t].astype(np.int64).sum()) for t in range(8)]}
+    tiers_info["warp_counters"] = ix.warp_counters()
     fetch_t0 = int(prof["fetch"][prof["tier"] == 0].astype(np.int64).sum())
     fetch_all = int(prof["fetch"].astype(np.int64).sum())
     ix.set_tuning(t0_cap=args.t0_cap, keep_stats=False)

@@ -80,6 +80,7 @@ def lib():
     L.galn_index_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L.galn_index_set_trace.argtypes = [vp, C.c_int]
     L.galn_index_set_warp_tier.argtypes = [vp, C.c_int, C.c_int]
+    L.galn_last_warp_counters.argtypes = [vp, vp, C.c_int]
     L.galn_version.restype = C.c_char_p
     _lib = L
     return L
@@ -137,6 +138,13 @@ class Index:
     def set_warp_tier(self, on: bool, arena_chunks: int = 1 << 14):
         if lib().galn_index_set_warp_tier(self.h, int(on), arena_chunks):
             raise GalnError("bad warp tier setting")
+
+    def warp_counters(self) -> dict:
+        v = np.zeros(12, np.uint64)
+        lib().galn_last_warp_counters(self.h, v.ctypes.data, 12)
+        names = ["reads", "waves", "lanes", "consumed", "pops", "continued", "hits", "cyc_chain", "cyc_replay",
+                 "cyc_commit", "cyc_load", "chain_pops"]
+        return {k: int(x) for k, x in zip(names, v)}
 
     def set_trace(self, on: bool):
         lib().galn_index_set_trace(self.h, int(on))

@@ -272,39 +272,58 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
             if (len <= kWarpMaxLen && bopt[bid[r]].n_stacks <= kWarpMaxStacks && bopt[bid[r]].n_stacks > 0) elig.push_back(r);
             else rest.push_back(r);
         }
-        int ne = (int)elig.size();
-        if (ne > 0) {
+        // pass 1 with the tuned arena; pass 2 for its overflow with arenas that hold the max_entries cut-off
+        const int aln_cap_w = 4096;
+        for (int pass = 0; pass < 2 && !elig.empty(); ++pass) {
+            int ne = (int)elig.size();
             int res_w = warp_resident(ix->dev.device);
             if (res_w <= 0) return GALN_ECUDA;
             int nw = std::min(ne, res_w);
             int arena = ix->warp_arena;
-            const int aln_cap_w = 4096;
+            if (pass == 1) {
+                int64_t full = ((int64_t)o->max_entries + 16 + kWarpMaxStacks * 32) / 32 + 1;
+                arena = (int)std::min<int64_t>(std::max<int64_t>(full, arena), 1 << 22);
+            }
             while (nw > 1 && warp_ws_bytes(nw, arena, aln_cap_w) > budget) nw /= 2;
-            while (arena > 1024 && warp_ws_bytes(nw, arena, aln_cap_w) > budget) arena /= 2;
+            if (pass == 0)
+                while (arena > 1024 && warp_ws_bytes(nw, arena, aln_cap_w) > budget) arena /= 2;
             RCK(B.ws.ensure(warp_ws_bytes(nw, arena, aln_cap_w)));
             ECK(cudaMemcpyAsync(cur, elig.data(), (size_t)ne * 4, cudaMemcpyHostToDevice, st));
             ECK(cudaMemsetAsync(job.counters, 0, 8, st));
+            unsigned long long *dbg = nullptr;
+            if (ix->keep_stats) {
+                RCK(B.dbg.ensure(kWarpDbg * 8));
+                dbg = (unsigned long long *)B.dbg.p;
+                ECK(cudaMemsetAsync(dbg, 0, kWarpDbg * 8, st));
+            }
             ECK(cudaEventRecord(e0, st));
-            RCK(dev_search_warp(ix->dev, job, nw, arena, aln_cap_w, 1, cur, ne, nxt, B.ws.p, st));
+            RCK(dev_search_warp(ix->dev, job, nw, arena, aln_cap_w, 1, cur, ne, nxt, B.ws.p, st, dbg));
             ECK(cudaEventRecord(e1, st));
             ECK(cudaMemcpyAsync(h_cnt, job.counters, 8, cudaMemcpyDeviceToHost, st));
+            if (dbg) {
+                unsigned long long hd[kWarpDbg];
+                ECK(cudaMemcpyAsync(hd, dbg, sizeof(hd), cudaMemcpyDeviceToHost, st));
+                ECK(cudaStreamSynchronize(st));
+                for (int q = 0; q < kWarpDbg; ++q) S.warp_dbg[q] += hd[q];
+            }
             ECK(cudaStreamSynchronize(st));
             float ms = 0;
             ECK(cudaEventElapsedTime(&ms, e0, e1));
             k_ms += ms;
             S.ms_tier[1] += ms;
-            S.tier_threads[1] = (int64_t)nw * 32;
-            S.tier_reads[1] = ne;
+            S.tier_threads[1] = std::max<int64_t>(S.tier_threads[1], (int64_t)nw * 32);
+            S.tier_reads[1] += ne;
             S.kernel_launches += 1;
             int got = h_cnt[1];
-            S.overflow_reads[1] = got;
             std::vector<int32_t> wov((size_t)got);
             if (got) {
                 ECK(cudaMemcpyAsync(wov.data(), nxt, (size_t)got * 4, cudaMemcpyDeviceToHost, st));
                 ECK(cudaStreamSynchronize(st));
             }
-            rest.insert(rest.end(), wov.begin(), wov.end());
+            if (pass == 1) S.overflow_reads[1] = got;
+            elig.swap(wov);
         }
+        rest.insert(rest.end(), elig.begin(), elig.end());
         n_ovf = (int)rest.size();
         if (n_ovf) {
             ECK(cudaMemcpyAsync(cur, rest.data(), (size_t)n_ovf * 4, cudaMemcpyHostToDevice, st));
@@ -434,6 +453,14 @@ extern "C" int galn_last_run_profile(galn_index *ix, double *ms_device, double *
         if (fetch) memcpy(fetch, ix->last.fetch.data(), (size_t)n * 4);
         if (tier) memcpy(tier, ix->last.tier_of.data(), (size_t)n);
     }
+    return 0;
+}
+
+extern "C" int galn_last_warp_counters(galn_index *ix, uint64_t *counters, int n)
+{
+    if (!ix || !counters || n < 1) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    for (int q = 0; q < n && q < kWarpDbg; ++q) counters[q] = ix->last.warp_dbg[q];
     return 0;
 }
 

@@ -38,7 +38,7 @@ struct Buf {
 // every buffer one search job uses, kept across calls on the same index (calls are serialised)
 struct JobBufs {
     Buf seq, query, off, bidx, maxdiff, bopt, out_n, out_off, out_pops, out_trace, out_peak, out_fetch, out_tier,
-        out_rec, rec_top, list_a, list_b, counters, ws;
+        out_rec, rec_top, list_a, list_b, counters, ws, dbg;
     Buf h_n, h_off, h_pops, h_trace, h_rec, h_list, h_misc;
     JobBufs()
     {
@@ -47,7 +47,7 @@ struct JobBufs {
     void release()
     {
         Buf *all[] = {&seq, &query, &off, &bidx, &maxdiff, &bopt, &out_n, &out_off, &out_pops, &out_trace, &out_peak,
-                      &out_fetch, &out_tier, &out_rec, &rec_top, &list_a, &list_b, &counters, &ws, &h_n, &h_off, &h_pops, &h_trace, &h_rec,
+                      &out_fetch, &out_tier, &dbg, &out_rec, &rec_top, &list_a, &list_b, &counters, &ws, &h_n, &h_off, &h_pops, &h_trace, &h_rec,
                       &h_list, &h_misc};
         for (Buf *b : all) b->release();
     }
@@ -62,6 +62,7 @@ struct RunStats {
     int64_t tier_threads[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t tier_reads[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t kernel_launches = 0;
+    uint64_t warp_dbg[16] = {};      // warp-tier counters (keep_stats runs)
     std::vector<uint32_t> fetch;     // per read, of the last run
     std::vector<int8_t> tier_of;     // per read, of the last run
 };

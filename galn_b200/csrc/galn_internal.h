@@ -91,7 +91,8 @@ constexpr int kWarpMaxLen = 256, kWarpMaxStacks = 256;
 size_t warp_smem_bytes();
 int warp_resident(int device);
 size_t warp_ws_bytes(int n_warps, int arena_chunks, int aln_cap);
+constexpr int kWarpDbg = 12;   // counters of the warp tier when profiling is on
 int dev_search_warp(const DevIndex &ix, DevJob &job, int n_warps, int arena_chunks, int aln_cap, int tier,
-                    const int32_t *list, int n, int32_t *ovf, void *ws_mem, cudaStream_t st);
+                    const int32_t *list, int n, int32_t *ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg);
 
 }  // namespace galn

@@ -335,7 +335,7 @@ size_t warp_ws_bytes(int n_warps, int arena_chunks, int aln_cap)
 }
 
 int dev_search_warp(const DevIndex &ix, DevJob &job, int n_warps, int arena_chunks, int aln_cap, int tier,
-                    const int32_t *list, int n, int32_t *ovf, void *ws_mem, cudaStream_t st)
+                    const int32_t *list, int n, int32_t *ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg)
 {
     if (n == 0) return 0;
     WArgs a;
@@ -362,6 +362,7 @@ int dev_search_warp(const DevIndex &ix, DevJob &job, int n_warps, int arena_chun
     a.out_peak = job.out_peak; a.out_fetch = job.out_fetch; a.out_tier = job.out_tier; a.tier = tier;
     a.out_rec = job.out_rec; a.rec_top = job.rec_top; a.rec_cap = job.rec_cap;
     a.ovf = ovf; a.ovf_n = job.counters + 1;
+    a.dbg = dbg;
     size_t smem = sizeof(WarpSmem);
     if (job.trace) warp_kernel<true><<<n_warps, 32, smem, st>>>(a);
     else warp_kernel<false><<<n_warps, 32, smem, st>>>(a);

@@ -85,7 +85,12 @@ struct WArgs {
     int64_t rec_cap;
     int32_t *ovf;
     int32_t *ovf_n;
+    unsigned long long *dbg;  // optional counters (kWDbg entries), or NULL
 };
+
+// optional counters of the warp tier (per launch, summed over warps)
+enum { kDbgReads, kDbgWaves, kDbgLanes, kDbgConsumed, kDbgPops, kDbgCont, kDbgHazard, kDbgCycChain,
+       kDbgCycReplay, kDbgCycCommit, kDbgCycLoad, kDbgChainPops, kWDbg };
 
 // an entry in registers (the score is the bucket of the wave)
 struct WEnt {
@@ -309,6 +314,9 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
     int best_score = (max_diff0 + 1) * O.s_mm + (O.max_gapo + 1) * O.s_gapo + (O.max_gape + 1) * O.s_gape;
     int best_cnt = 0, n_aln = 0, ret = 0, n_entries = 0, peak = 0;
     uint64_t pops = 0, trace = kTraceInit;
+    unsigned long long d_waves = 0, d_lanes = 0, d_cons = 0, d_cont = 0, d_hz = 0, d_chainpops = 0;
+    long long c_chain = 0, c_replay = 0, c_commit = 0, c_load = 0, t_mark = 0;
+    const bool dbg = a.dbg != nullptr;
 
     int n_amb = 0;
     for (int j = 0; j < len; ++j) n_amb += S->q[j] > 3;
@@ -336,6 +344,7 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
             }
             if (b >= kWMaxB || (!pend && S->n_in[b] <= 0)) { ret = kErrStack; break; }   // inconsistent: re-run elsewhere
             const uint32_t binfo = (uint32_t)b << 21;
+            if (dbg) t_mark = clock64();
             const int navail = (pend ? 1 : 0) + S->n_in[b];
             const int Wn = navail < 32 ? navail : 32;
             // load the wave's entries: lane 0 the pending child (if any), then the bucket from the top
@@ -381,8 +390,14 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                 break;
             }
             // speculative chains
+            if (dbg) { long long t = clock64(); c_load += t - t_mark; t_mark = t; }
             if (lane < Wn) lane_chain<TRACE>(ix, O, c, S, lane, x, b, fetches);
             __syncwarp();
+            if (dbg) {
+                long long t = clock64(); c_chain += t - t_mark; t_mark = t;
+                ++d_waves; d_lanes += Wn;
+                for (int j = 0; j < Wn; ++j) d_chainpops += S->lane_np[j];
+            }
             // replay in sequential order
             int consumed = 0;          // lanes whose entries are consumed
             bool stop = false, search_end = false, new_pend = false;
@@ -461,6 +476,11 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                 if (stop) break;
                 consumed = j + 1;
                 if (endc == 2) { new_pend = true; stop = true; }
+            }
+            if (dbg) {
+                long long t = clock64(); c_replay += t - t_mark; t_mark = t;
+                d_cons += consumed; d_cont += new_pend ? 1 : 0;
+                if (consumed > 0 && S->lane_end[consumed - 1] == 1) ++d_hz;
             }
             if (search_end) break;
             // take the consumed entries off bucket b (lane 0 of the wave may have been the pending child)
@@ -543,6 +563,7 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                 }
                 __syncwarp();
             }
+            if (dbg) { long long t = clock64(); c_commit += t - t_mark; }
             if (fail) break;
         }
         if (ret == 0) ret = n_aln;
@@ -557,6 +578,20 @@ publish:
             for (int j = lane; j < 3 * ret; j += 32) a.out_rec[o * 3 + j] = aln[j];
             if (lane == 0) a.out_off[r] = (int64_t)o;
         }
+    }
+    if (dbg && lane == 0) {
+        atomicAdd(a.dbg + kDbgReads, 1ull);
+        atomicAdd(a.dbg + kDbgWaves, d_waves);
+        atomicAdd(a.dbg + kDbgLanes, d_lanes);
+        atomicAdd(a.dbg + kDbgConsumed, d_cons);
+        atomicAdd(a.dbg + kDbgPops, (unsigned long long)pops);
+        atomicAdd(a.dbg + kDbgCont, d_cont);
+        atomicAdd(a.dbg + kDbgHazard, d_hz);
+        atomicAdd(a.dbg + kDbgCycChain, (unsigned long long)c_chain);
+        atomicAdd(a.dbg + kDbgCycReplay, (unsigned long long)c_replay);
+        atomicAdd(a.dbg + kDbgCycCommit, (unsigned long long)c_commit);
+        atomicAdd(a.dbg + kDbgCycLoad, (unsigned long long)c_load);
+        atomicAdd(a.dbg + kDbgChainPops, d_chainpops);
     }
     if (lane == 0) {
         if (ret == kErrStack || ret == kErrAln) a.ovf[atomicAdd(a.ovf_n, 1)] = r;

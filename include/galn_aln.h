@@ -186,6 +186,11 @@ int galn_last_run_stats(galn_index *ix, double *ms_total, double *ms_kernels, in
 int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, int64_t *tier_reads, int64_t *tier_threads,
                           uint32_t *fetch, int8_t *tier, int32_t n);
 
+/* Counters of the warp tier in the last keep_stats run (no reference counterpart): reads, waves, lanes
+ * given entries, lanes replayed, pops, chains continued, hits, SM cycles in chains / replay / commit /
+ * wave loads (summed over warps), pops run speculatively. */
+int galn_last_warp_counters(galn_index *ix, uint64_t *counters, int n);
+
 /* Tier capacities (no reference counterpart; set by the autotuner): entries and records per thread in the
  * first tier, its block size (64/128/256/512), live entries and records per thread in the second tier, and
  * whether to keep the per-read profile. Results never depend on these values. */
