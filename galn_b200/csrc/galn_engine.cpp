@@ -460,7 +460,7 @@ extern "C" int galn_last_warp_counters(galn_index *ix, uint64_t *counters, int n
 {
     if (!ix || !counters || n < 1) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
-    for (int q = 0; q < n && q < kWarpDbg; ++q) counters[q] = ix->last.warp_dbg[q];
+    for (int q = 0; q < n && q < galn::kWarpDbg; ++q) counters[q] = ix->last.warp_dbg[q];
     return 0;
 }
 
