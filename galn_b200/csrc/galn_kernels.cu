@@ -331,7 +331,8 @@ int warp_resident(int device)
 size_t warp_ws_bytes(int n_warps, int arena_chunks, int aln_cap)
 {
     size_t w = (size_t)n_warps;
-    return align256(w * arena_chunks * kWCH * 16) + 2 * align256(w * arena_chunks * 4) + align256(w * aln_cap * 24);
+    return align256(w * arena_chunks * kWCH * 16) + 2 * align256(w * arena_chunks * 4) + align256(w * aln_cap * 24)
+         + align256(w * 3 * 32 * kWL * 16) + align256(w * 32 * kWR * 16);
 }
 
 int dev_search_warp(const DevIndex &ix, DevJob &job, int n_warps, int arena_chunks, int aln_cap, int tier,
@@ -357,6 +358,10 @@ int dev_search_warp(const DevIndex &ix, DevJob &job, int n_warps, int arena_chun
     a.free_ids = (int32_t *)base;
     base += align256(w * arena_chunks * 4);
     a.aln = (uint64_t *)base;
+    base += align256(w * aln_cap * 24);
+    a.stage = (uint4 *)base;
+    base += align256(w * 3 * 32 * kWL * 16);
+    a.prec = (uint4 *)base;
     a.arena_chunks = arena_chunks; a.aln_cap = aln_cap;
     a.out_n = job.out_n; a.out_off = job.out_off; a.out_pops = job.out_pops; a.out_trace = job.out_trace;
     a.out_peak = job.out_peak; a.out_fetch = job.out_fetch; a.out_tier = job.out_tier; a.tier = tier;

@@ -9,8 +9,9 @@
 // top W <= 32 entries of bucket b can be expanded at the same time, one per lane.
 //
 // One wave: lane j takes the j-th entry from the top of bucket b (lane 0 takes a pending exact child left
-// by the previous wave), runs its chain for up to kWR pops, recording the pushes of each pop (in the order
-// bwt_match_gap pushes them) in shared memory and stopping at a hit (a "hazard"). Then the warp replays the
+// by the previous wave), runs its chain for up to kWR pops, staging the pushes of each pop (in the order
+// bwt_match_gap pushes them) in global memory, one list per distinct target bucket (b+s_mm, b+s_gapo,
+// b+s_gape), with 4 bytes of per-pop data in shared memory, and stopping at a hit (a "hazard"). Then the warp replays the
 // lanes in order exactly as the sequential search would pop them: the max_entries test before each pop,
 // n_entries after each pop and push, the pop count, the trace hash, the first hit (handled sequentially:
 // best_score, max_diff, -R, gapped-hit de-duplication, gap_shadow, the record). Replay stops at a hit or at a
@@ -19,8 +20,8 @@
 // then pop order), so every bucket is the same LIFO as in the sequential search.
 //
 // Storage: each bucket is a chain of 32-entry chunks in the warp's arena (global memory), with its top
-// chunk, fill and entry count in shared memory. Widths, the query and the per-lane buffers are in shared
-// memory. Reads the tier cannot take (length > 256, n_stacks > 256, a penalty <= 0, 32-byte entries) or
+// chunk, fill and entry count in shared memory. Widths, the query and the per-pop data are in shared
+// memory; staged pushes (and, in trace mode, popped entries) in a per-warp global staging area. Reads the tier cannot take (length > 256, n_stacks > 256, a penalty <= 0, 32-byte entries) or
 // that outgrow the arena or the record buffer go to the thread tiers (the host routes them).
 #pragma once
 
@@ -30,9 +31,10 @@ namespace galn {
 
 constexpr int kWMaxB = 256;      // buckets
 constexpr int kWMaxLen = 256;    // read length
-constexpr int kWR = 8;           // pops per lane per wave
-constexpr int kWPB = 24;         // pushes per lane per wave
+constexpr int kWR = 32;          // pops per lane per wave
+constexpr int kWL = 128;         // staged pushes per lane and target list per wave
 constexpr int kWCH = 32;         // entries per chunk
+constexpr int kWNewC = (kWCH + 32 * kWL) / kWCH + 2;   // chunks one commit may allocate
 
 struct WarpSmem {
     int32_t top_chunk[kWMaxB];
@@ -42,17 +44,15 @@ struct WarpSmem {
     uint64_t W[kWMaxLen + 1];
     uint64_t SW[kWMaxLen + 1];
     uint8_t q[kWMaxLen];
-    uint4 pbuf[32][kWPB];             // pushes of each lane, packed 16-byte entries
-    uint8_t pbkt[32][kWPB];           // their buckets
-    uint8_t npush[32][kWR];           // pushes of each pop (the fused exact child not counted)
-    uint8_t hasx[32][kWR];            // the pop has an exact child (it is the next pop of the chain)
-    uint4 prec[32][kWR];              // popped entries (trace mode)
+    // per pop of each lane: pushes (bits 0-7, the fused exact child not counted), has an exact child
+    // (bit 8), index blocks read (bits 16-31)
+    uint32_t meta[32][kWR];
     uint4 hz[32];                     // hazard entry of each lane
     uint64_t hk[32], hl[32];          // its interval after the exact tail
-    int32_t lane_np[32], lane_end[32], lane_nb[32];
-    uint16_t pf[32][kWR];             // index blocks read by each pop of each lane's chain
+    int32_t lane_np[32], lane_end[32];
+    uint16_t lane_nl[32][3];          // staged pushes of each lane per target list
     uint4 lane_x[32];                 // pending exact child of a lane that stopped mid-chain
-    int32_t newc[32];                 // chunks allocated for one commit
+    int32_t newc[kWNewC];             // chunks allocated for one commit
 };
 
 struct WArgs {
@@ -73,6 +73,8 @@ struct WArgs {
     int arena_chunks;
     uint64_t *aln;            // n_warps * aln_cap * 3
     int aln_cap;
+    uint4 *stage;             // n_warps * 3 lists * 32 lanes * kWL staged pushes
+    uint4 *prec;              // n_warps * 32 lanes * kWR popped entries (trace mode)
     int32_t *out_n;
     int64_t *out_off;
     uint64_t *out_pops, *out_trace;
@@ -138,43 +140,49 @@ struct WCtx {
 };
 
 // one lane's chain: end code 0 = finished, 1 = hazard (a hit) at its last pop, 2 = stopped with x pending,
-// 3 = its last pop pushes a score >= n_stacks (bwt_match_gap returns BWTGAP_ERR_SCORE there)
+// 3 = its last pop pushes a score >= n_stacks (bwt_match_gap returns BWTGAP_ERR_SCORE there).
+// st: this lane's three staging lists (kWL apart, 32 * kWL between lists); tl: list of each push kind
+// (mismatch, gap open, gap extension); pr: this lane's popped-entry records (trace mode)
 template <bool TRACE>
 __device__ __forceinline__ void lane_chain(const IndexView &ix, const BatchOpt &O, const WCtx &c, WarpSmem *S, int lane,
-                                           WEnt x, int b, uint32_t &fetches)
+                                           WEnt x, int b, uint32_t &fetches, uint4 *st, const int tl[3], uint4 *pr)
 {
-    int np = 0, nb = 0, endc = 0;
-    // a push of the expansion below; a score at or past n_stacks ends the read
-#define WPUSH(BKT, ...)                                                                 \
+    int np = 0, endc = 0;
+    int nl0 = 0, nl1 = 0, nl2 = 0;
+    const size_t lstride = (size_t)32 * kWL;
+    // a push of the given kind (0 mismatch, 1 gap open, 2 gap extension); a score at or past n_stacks ends
+    // the read
+#define WPUSH(KIND, BKT, ...)                                                           \
     do {                                                                                \
         int bk_ = (BKT);                                                                \
         if (bk_ >= O.n_stacks) { err = true; break; }                                   \
-        S->pbuf[lane][nb] = wpack_child(__VA_ARGS__);                                   \
-        S->pbkt[lane][nb++] = (uint8_t)bk_;                                             \
+        int L_ = tl[KIND];                                                              \
+        int &n_ = L_ == 0 ? nl0 : (L_ == 1 ? nl1 : nl2);                                \
+        st[L_ * lstride + n_] = wpack_child(__VA_ARGS__);                               \
+        ++n_;                                                                           \
         ++npu;                                                                          \
     } while (0)
     for (;;) {
         bool err = false;
         const uint32_t f_pop = fetches;
-        if (TRACE) S->prec[lane][np] = wpack(x);
+        if (TRACE) pr[np] = wpack(x);
         int diffs = x.n_mm + x.n_gapo + (c.gape ? x.n_gape : 0);
         int m = c.max_diff - diffs;
         int i = x.i;
-        uint8_t npu = 0, hx = 0;
+        uint32_t npu = 0, hx = 0;
         if (m < 0 || (i > 0 && m < (int)(S->W[i - 1] >> 48))) {
-            S->npush[lane][np] = 0; S->hasx[lane][np] = 0; S->pf[lane][np] = 0; ++np; endc = 0; break;
+            S->meta[lane][np] = 0; ++np; endc = 0; break;
         }
         if (i == 0) {
             S->hz[lane] = wpack(x); S->hk[lane] = x.k; S->hl[lane] = x.l;
-            S->npush[lane][np] = 0; S->hasx[lane][np] = 0; S->pf[lane][np] = 0; ++np; endc = 1; break;
+            S->meta[lane][np] = 0; ++np; endc = 1; break;
         }
         if (m == 0 && (x.state == kStM || c.gape || x.n_gape == O.max_gape)) {
             uint64_t k = x.k, l = x.l;
-            S->npush[lane][np] = 0; S->hasx[lane][np] = 0;
             if (match_exact_alt(ix, i, S->q, k, l, fetches)) {
                 S->hz[lane] = wpack(x); S->hk[lane] = k; S->hl[lane] = l; endc = 1;
             } else endc = 0;
-            S->pf[lane][np] = (uint16_t)(fetches - f_pop);
+            S->meta[lane][np] = (fetches - f_pop) << 16;
             ++np;
             break;
         }
@@ -206,21 +214,24 @@ __device__ __forceinline__ void lane_chain(const IndexView &ix, const BatchOpt &
         if (allow_diff && i >= O.indel_end_skip + tmp && c.len - i >= O.indel_end_skip + tmp) {
             if (x.state == kStM) {
                 if (x.n_gapo < O.max_gapo) {
-                    WPUSH(b + O.s_gapo, x.k, x.l, i, x.n_mm, x.n_gapo + 1, x.n_gape, x.n_ins + 1, kStI, 1);
+                    WPUSH(1, b + O.s_gapo, x.k, x.l, i, x.n_mm, x.n_gapo + 1, x.n_gape, x.n_ins + 1, kStI, 1);
 #pragma unroll
                     for (int cc = 0; cc < 4; ++cc) {
                         uint64_t kk = sel4(cc, kk0, kk1, kk2, kk3), ll = sel4(cc, ll0, ll1, ll2, ll3);
-                        if (!err && kk <= ll) WPUSH(b + O.s_gapo, kk, ll, i + 1, x.n_mm, x.n_gapo + 1, x.n_gape, x.n_ins, kStD, 1);
+                        if (!err && kk <= ll)
+                            WPUSH(1, b + O.s_gapo, kk, ll, i + 1, x.n_mm, x.n_gapo + 1, x.n_gape, x.n_ins, kStD, 1);
                     }
                 }
             } else if (x.state == kStI) {
-                if (x.n_gape < O.max_gape) WPUSH(b + O.s_gape, x.k, x.l, i, x.n_mm, x.n_gapo, x.n_gape + 1, x.n_ins + 1, kStI, 1);
+                if (x.n_gape < O.max_gape)
+                    WPUSH(2, b + O.s_gape, x.k, x.l, i, x.n_mm, x.n_gapo, x.n_gape + 1, x.n_ins + 1, kStI, 1);
             } else if (x.state == kStD) {
                 if (x.n_gape < O.max_gape && (gaps < c.max_diff || occ < (uint64_t)(int64_t)O.max_del_occ)) {
 #pragma unroll
                     for (int cc = 0; cc < 4; ++cc) {
                         uint64_t kk = sel4(cc, kk0, kk1, kk2, kk3), ll = sel4(cc, ll0, ll1, ll2, ll3);
-                        if (!err && kk <= ll) WPUSH(b + O.s_gape, kk, ll, i + 1, x.n_mm, x.n_gapo, x.n_gape + 1, x.n_ins, kStD, 1);
+                        if (!err && kk <= ll)
+                            WPUSH(2, b + O.s_gape, kk, ll, i + 1, x.n_mm, x.n_gapo, x.n_gape + 1, x.n_ins, kStD, 1);
                     }
                 }
             }
@@ -237,39 +248,55 @@ __device__ __forceinline__ void lane_chain(const IndexView &ix, const BatchOpt &
                 uint64_t kk = sel4(cc, kk0, kk1, kk2, kk3), ll = sel4(cc, ll0, ll1, ll2, ll3);
                 if (!err && kk <= ll) {
                     if (!mm) { exact = true; ek = kk; el = ll; }
-                    else WPUSH(b + O.s_mm, kk, ll, i, x.n_mm + 1, x.n_gapo, x.n_gape, x.n_ins, kStM, 1);
+                    else WPUSH(0, b + O.s_mm, kk, ll, i, x.n_mm + 1, x.n_gapo, x.n_gape, x.n_ins, kStM, 1);
                 }
             }
         } else if (base < 4) {
             uint64_t kk = sel4(base, kk0, kk1, kk2, kk3), ll = sel4(base, ll0, ll1, ll2, ll3);
             if (kk <= ll) { exact = true; ek = kk; el = ll; }
         }
-        S->pf[lane][np] = (uint16_t)(fetches - f_pop);
+        const uint32_t fpop = (fetches - f_pop) << 16;
         if (err) {   // the read ends at this pop with BWTGAP_ERR_SCORE
-            S->npush[lane][np] = 0; S->hasx[lane][np] = 0; ++np; endc = 3; break;
+            S->meta[lane][np] = fpop; ++np; endc = 3; break;
         }
         if (exact) hx = 1;
-        S->npush[lane][np] = npu; S->hasx[lane][np] = hx;
+        S->meta[lane][np] = npu | (hx << 8) | fpop;
         ++np;
         if (!exact) { endc = 0; break; }
         x.k = ek; x.l = el; x.i = i; x.isdiff = 0; x.state = kStM;
-        if (np == kWR || nb + 9 > kWPB) { endc = 2; S->lane_x[lane] = wpack(x); break; }   // a pop pushes <= 9
+        // room for one more pop: at most 9 pushes, all possibly in one list
+        if (np == kWR || nl0 + 9 > kWL || nl1 + 9 > kWL || nl2 + 9 > kWL) { endc = 2; S->lane_x[lane] = wpack(x); break; }
     }
 #undef WPUSH
     S->lane_np[lane] = np;
     S->lane_end[lane] = endc;
-    S->lane_nb[lane] = nb;
+    S->lane_nl[lane][0] = (uint16_t)nl0;
+    S->lane_nl[lane][1] = (uint16_t)nl1;
+    S->lane_nl[lane][2] = (uint16_t)nl2;
 }
 
-// the warp's chunk allocator (warp-uniform state; lane 0 writes)
+// the warp's chunk allocator (warp-uniform state; every lane holds the same copy)
 struct WAlloc {
-    int32_t *prev, *free_ids;
+    int32_t *free_ids;
     int base, cap, bump, free_top;
-    __device__ __forceinline__ int alloc()
+    // `need` chunk ids into out[0..need), lane-parallel; false if the arena is exhausted
+    __device__ __forceinline__ bool alloc_n(int need, int32_t *out, int lane)
     {
-        if (free_top > 0) return free_ids[--free_top];
-        if (bump < cap) return base + bump++;
-        return -1;
+        bool ok = true;
+        for (int t0 = 0; t0 < need; t0 += 32) {
+            int t = t0 + lane;
+            if (t < need) {
+                int id;
+                if (t < free_top) id = free_ids[free_top - 1 - t];
+                else id = bump + (t - free_top) < cap ? base + bump + (t - free_top) : -1;
+                out[t] = id;
+            }
+        }
+        int from_free = need < free_top ? need : free_top;
+        if (bump + (need - from_free) > cap) ok = false;
+        else { free_top -= from_free; bump += need - from_free; }
+        __syncwarp();
+        return ok;
     }
     __device__ __forceinline__ void release(int id, int lane)
     {
@@ -302,8 +329,17 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
     uint32_t f_alg = __shfl_sync(FULL, fetches, 0);   // algorithmic count: widths, then replayed chains
     uint4 *chunks = a.chunks;
     WAlloc A;
-    A.prev = a.chunk_prev; A.free_ids = a.free_ids + (size_t)wid * a.arena_chunks;
+    A.free_ids = a.free_ids + (size_t)wid * a.arena_chunks;
     A.base = wid * a.arena_chunks; A.cap = a.arena_chunks; A.bump = 0; A.free_top = 0;
+    uint4 *stage_lane = a.stage + (size_t)wid * 3 * 32 * kWL + (size_t)lane * kWL;
+    uint4 *prec_w = a.prec + (size_t)wid * 32 * kWR;
+    // the staging list of each push kind: kinds whose target buckets coincide share a list, so the
+    // bucket keeps the push order
+    int tl[3];
+    tl[0] = 0;
+    tl[1] = O.s_gapo == O.s_mm ? 0 : 1;
+    tl[2] = O.s_gape == O.s_mm ? 0 : (O.s_gape == O.s_gapo ? tl[1] : 2);
+    const int lst_pen[3] = {O.s_mm, tl[1] == 1 ? O.s_gapo : -1, tl[2] == 2 ? O.s_gape : -1};
     uint64_t *aln = a.aln + (size_t)wid * a.aln_cap * 3;
 
     WCtx c;
@@ -391,7 +427,7 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
             }
             // speculative chains
             if (dbg) { long long t = clock64(); c_load += t - t_mark; t_mark = t; }
-            if (lane < Wn) lane_chain<TRACE>(ix, O, c, S, lane, x, b, fetches);
+            if (lane < Wn) lane_chain<TRACE>(ix, O, c, S, lane, x, b, fetches, stage_lane, tl, prec_w + (size_t)lane * kWR);
             __syncwarp();
             if (dbg) {
                 long long t = clock64(); c_chain += t - t_mark; t_mark = t;
@@ -407,9 +443,10 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                     if (n_entries > O.max_entries) { search_end = true; stop = true; break; }
                     --n_entries;
                     ++pops;
-                    f_alg += S->pf[j][t];
+                    const uint32_t meta = S->meta[j][t];
+                    f_alg += meta >> 16;
                     if (TRACE) {
-                        WEnt y = wunpack(S->prec[j][t]);
+                        WEnt y = wunpack(prec_w[(size_t)j * kWR + t]);
                         uint64_t h = trace;
                         h = trace_mix(h, binfo | (uint32_t)y.i);
                         h = trace_mix(h, y.k);
@@ -470,7 +507,7 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                         }
                         break;
                     }
-                    n_entries += S->npush[j][t] + S->hasx[j][t];
+                    n_entries += (int)(meta & 0xff) + (int)((meta >> 8) & 1);
                     if (n_entries > peak) peak = n_entries;
                 }
                 if (stop) break;
@@ -513,50 +550,38 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                 pend_b = b;
                 px = wunpack(S->lane_x[consumed - 1]);
             }
-            // commit the pushes of the consumed lanes, bucket by bucket, in replay order
-            int tgt[3] = {b + O.s_mm, b + O.s_gapo, b + O.s_gape};
+            // commit the pushes of the consumed lanes, list by list (one list per target bucket), in replay
+            // order: lane order, then the order the lane staged them
             bool fail = false;
-            for (int u = 0; u < 3 && !fail; ++u) {
-                int X = tgt[u];
-                if ((u == 1 && X == tgt[0]) || (u == 2 && (X == tgt[0] || X == tgt[1]))) continue;
-                int nb = lane < consumed ? S->lane_nb[lane] : 0;
-                int cntX = 0;
-                for (int t = 0; t < nb; ++t) cntX += S->pbkt[lane][t] == X;
-                // exclusive scan over lanes
+            for (int L = 0; L < 3 && !fail; ++L) {
+                if (lst_pen[L] < 0) continue;
+                const int X = b + lst_pen[L];
+                int cntX = lane < consumed ? (int)S->lane_nl[lane][L] : 0;
                 int incl = cntX;
                 for (int o = 1; o < 32; o <<= 1) {
                     int v = __shfl_up_sync(FULL, incl, o);
                     if (lane >= o) incl += v;
                 }
-                int T = __shfl_sync(FULL, incl, 31);
+                const int T = __shfl_sync(FULL, incl, 31);
                 if (T == 0) continue;
                 if (X >= n_stacks || X >= kWMaxB) { ret = kErrScore; fail = true; break; }
-                int c0 = S->top_chunk[X], cnt0 = c0 >= 0 ? S->top_cnt[X] : 0;
-                int need = (cnt0 + T + kWCH - 1) / kWCH - (c0 >= 0 ? 1 : 0);
-                // allocate `need` chunks (uniform), chain them on top of c0
-                int prevc = c0;
-                for (int t = 0; t < need; ++t) {
-                    int id = A.alloc();
-                    if (id < 0) { fail = true; break; }
-                    if (lane == 0) { a.chunk_prev[id] = prevc; S->newc[t] = id; }
-                    prevc = id;
-                }
-                if (fail) { ret = kErrStack; break; }
-                __syncwarp();
-                int o = incl - cntX;   // this lane's first position
-                for (int t = 0; t < nb; ++t) {
-                    if (S->pbkt[lane][t] != X) continue;
-                    int g = cnt0 + o;
+                const int c0 = S->top_chunk[X], cnt0 = c0 >= 0 ? S->top_cnt[X] : 0;
+                const int need = (cnt0 + T + kWCH - 1) / kWCH - (c0 >= 0 ? 1 : 0);
+                if (need > kWNewC || !A.alloc_n(need, S->newc, lane)) { ret = kErrStack; fail = true; break; }
+                // chain the new chunks on top of c0
+                for (int t = lane; t < need; t += 32) a.chunk_prev[S->newc[t]] = t == 0 ? c0 : S->newc[t - 1];
+                const uint4 *src = stage_lane + (size_t)L * 32 * kWL;
+                int g = cnt0 + (incl - cntX);
+                for (int t = 0; t < cntX; ++t, ++g) {
                     int ci = g / kWCH;
-                    int chunk = (c0 >= 0) ? (ci == 0 ? c0 : S->newc[ci - 1]) : S->newc[ci];
-                    chunks[(size_t)chunk * kWCH + (g % kWCH)] = S->pbuf[lane][t];
-                    ++o;
+                    int chunk = c0 >= 0 ? (ci == 0 ? c0 : S->newc[ci - 1]) : S->newc[ci];
+                    chunks[(size_t)chunk * kWCH + (g % kWCH)] = src[t];
                 }
                 __syncwarp();
                 if (lane == 0) {
                     int last = cnt0 + T - 1;
                     int ci = last / kWCH;
-                    S->top_chunk[X] = (c0 >= 0) ? (ci == 0 ? c0 : S->newc[ci - 1]) : S->newc[ci];
+                    S->top_chunk[X] = c0 >= 0 ? (ci == 0 ? c0 : S->newc[ci - 1]) : S->newc[ci];
                     S->top_cnt[X] = (uint16_t)(last % kWCH + 1);
                     S->n_in[X] += T;
                     S->mask[X >> 5] |= 1u << (X & 31);
