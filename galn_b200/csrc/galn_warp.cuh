@@ -434,10 +434,44 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                 ++d_waves; d_lanes += Wn;
                 for (int j = 0; j < Wn; ++j) d_chainpops += S->lane_np[j];
             }
-            // replay in sequential order
+            // replay in sequential order. Without the trace hash, the lanes before the first lane that
+            // stops the replay (a hit, an error, an unfinished chain, or the max_entries cut-off inside its
+            // chain) are replayed at once from prefix sums; that lane, and in trace mode every lane, one pop
+            // at a time.
             int consumed = 0;          // lanes whose entries are consumed
             bool stop = false, search_end = false, new_pend = false;
-            for (int j = 0; j < Wn && !stop; ++j) {
+            int j_first = 0;
+            if (!TRACE) {
+                const int npl = lane < Wn ? S->lane_np[lane] : 0;
+                const int endl = lane < Wn ? S->lane_end[lane] : 0;
+                int pre = 0, mpre = 0, pmax = 0;
+                uint32_t fsum = 0;
+                for (int t = 0; t < npl; ++t) {
+                    const uint32_t meta = S->meta[lane][t];
+                    if (pre > mpre) mpre = pre;          // n_entries before pop t, relative to the chain start
+                    pre += (int)(meta & 0xff) + (int)((meta >> 8) & 1) - 1;
+                    if (pre > pmax) pmax = pre;
+                    fsum += meta >> 16;
+                }
+                int incl = pre;
+                for (int o = 1; o < 32; o <<= 1) {
+                    int v = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int nstart = n_entries + incl - pre;
+                const bool cross = lane < Wn && nstart + mpre > O.max_entries;
+                const unsigned bal = __ballot_sync(FULL, lane < Wn && (cross || endl != 0));
+                const int sstar = bal ? __ffs(bal) - 1 : Wn;
+                const bool take = lane < sstar;
+                pops += (uint64_t)__reduce_add_sync(FULL, take ? (unsigned)npl : 0u);
+                n_entries += (int)__reduce_add_sync(FULL, take ? (unsigned)pre : 0u);
+                f_alg += __reduce_add_sync(FULL, take ? fsum : 0u);
+                const int pk = (int)__reduce_max_sync(FULL, take ? (unsigned)(nstart + pmax) : 0u);
+                if (pk > peak) peak = pk;
+                consumed = sstar;
+                j_first = sstar;
+            }
+            for (int j = j_first; j < Wn && !stop && (TRACE || j == j_first); ++j) {
                 const int np = S->lane_np[j], endc = S->lane_end[j];
                 for (int t = 0; t < np; ++t) {
                     if (n_entries > O.max_entries) { search_end = true; stop = true; break; }

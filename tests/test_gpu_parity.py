@@ -46,15 +46,17 @@ def test_golden_case(name, engine):
     np.testing.assert_array_equal(res.trace, pr["trace"])
 
 
+@pytest.mark.parametrize("trace", [True, False])
 @pytest.mark.parametrize("warp", [(True, 16384), (True, 64), (False, 64)])
 @pytest.mark.parametrize("caps", [(16, 1, 64, 16, 1), (64, 2, 256, 128, 2), (300, 4, 128, 1000, 3)])
-def test_tier_migration_gives_same_bytes(caps, warp):
+def test_tier_migration_gives_same_bytes(caps, warp, trace):
     """Tiny first- and second-tier capacities push many reads through every tier (the warp tier with a
     normal and a tiny arena, or without it); the bytes and traces stay the reference's."""
     ix = galn_b200.Index(os.path.join(GOLDEN, "small", "ref"))
     t0_cap, t0_aln, block, t1_cap, t1_aln = caps
     ix.set_tuning(t0_cap, t0_aln, block, t1_cap, t1_aln, keep_stats=True)
     ix.set_warp_tier(*warp)
+    ix.set_trace(trace)
     for name in ("adna", "divergent", "edge_nonstop", "tiny_queue"):
         meta = CASES[name]
         p = case_paths(name, meta)
@@ -66,7 +68,8 @@ def test_tier_migration_gives_same_bytes(caps, warp):
             res = galn_b200.aln(ix, meta["opts"], p["fq"], engine)
             assert res.sai_bytes() == open(p["sai"], "rb").read(), (name, engine)
             pr = np.load(p["per_read"])
-            np.testing.assert_array_equal(res.trace, pr["trace"])
+            if trace:
+                np.testing.assert_array_equal(res.trace, pr["trace"])
             np.testing.assert_array_equal(res.pops, pr["pops"])
             prof = ix.last_profile(len(res))
             np.testing.assert_array_equal(prof["fetch"].astype(np.uint64), o.fetch64)
@@ -99,8 +102,9 @@ def test_index_from_memory():
     assert res.sai_bytes() == open(p["sai"], "rb").read()
 
 
-def _compare_with_oracle(prefix, reads, opts, engines=ENGINES):
+def _compare_with_oracle(prefix, reads, opts, engines=ENGINES, trace=True):
     ix = galn_b200.Index(prefix)
+    ix.set_trace(trace)
     q = oracle.encode_queries(reads.seq, reads.offset)
     batch = reads.batch if reads.batch is not None else oracle.batches_for(len(reads))
     o = oracle.aln(oracle.Index(prefix + ".bwt"), oracle.opt_bytes(oracle.parse_aln_args(opts)), q, reads.offset,
@@ -109,7 +113,8 @@ def _compare_with_oracle(prefix, reads, opts, engines=ENGINES):
         res = galn_b200.aln(ix, opts, reads, engine)
         np.testing.assert_array_equal(res.n_aln, o.n_aln)
         np.testing.assert_array_equal(res.pops, o.pops)
-        np.testing.assert_array_equal(res.trace, o.trace)
+        if trace:
+            np.testing.assert_array_equal(res.trace, o.trace)
         np.testing.assert_array_equal(res.rec_offset, o.rec_off)
         assert res.records.tobytes() == o.records.tobytes()
 
@@ -122,8 +127,9 @@ def adna_index(tmp_path_factory):
     return ref, str(d / "ref")
 
 
+@pytest.mark.parametrize("trace", [True, False])
 @pytest.mark.parametrize("workload,n,seed", [("adna", 40_000, 31), ("divergent", 300, 32), ("plain", 20_000, 33)])
-def test_synthetic_against_oracle(adna_index, workload, n, seed):
+def test_synthetic_against_oracle(adna_index, workload, n, seed, trace):
     ref, prefix = adna_index
     if workload == "adna":
         r = synth.simulate_reads(ref, n, seed, synth.adna_lengths, sub_rate=0.005, random_frac=0.03, deaminate=0.3)
@@ -135,7 +141,7 @@ def test_synthetic_against_oracle(adna_index, workload, n, seed):
         r = synth.simulate_reads(ref, n, seed, 100, sub_rate=0.01, indel_rate=0.001, random_frac=0.02)
         opts = []
     reads = galn_b200.Reads(r.ascii(), r.off)
-    _compare_with_oracle(prefix, reads, opts)
+    _compare_with_oracle(prefix, reads, opts, trace=trace)
 
 
 def test_batch_boundary_mixed_lengths(adna_index):
