@@ -165,7 +165,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--data-dir", default=None)
     ap.add_argument("--trace", action="store_true", help="compute per-read trace hashes (verification mode)")
-    ap.add_argument("--t0-cap", type=int, default=4096, help="first-tier stack entries per thread")
+    ap.add_argument("--t0-cap", type=int, default=1024, help="first-tier stack entries per thread")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

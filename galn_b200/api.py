@@ -130,7 +130,7 @@ class Index:
     def __del__(self):
         self.close()
 
-    def set_tuning(self, t0_cap=4096, t0_aln=32, t0_block=128, t1_cap=65536, t1_aln=1024, keep_stats=False):
+    def set_tuning(self, t0_cap=1024, t0_aln=32, t0_block=128, t1_cap=65536, t1_aln=1024, keep_stats=False):
         rc = lib().galn_index_set_tuning(self.h, t0_cap, t0_aln, t0_block, t1_cap, t1_aln, int(keep_stats))
         if rc:
             raise GalnError(f"bad tuning ({rc})")

@@ -77,7 +77,7 @@ struct galn_index {
     galn::JobBufs ws;
     galn::RunStats last;
     // tuning knobs (galn_tune.cpp sets them; defaults otherwise)
-    int t0_cap = 4096, t0_aln = 32, t0_block = 128;
+    int t0_cap = 1024, t0_aln = 32, t0_block = 128;
     int t1_cap = 65536, t1_aln = 1024;
     double mem_fraction = 0.6;          // of free device memory a job's workspace may take
     bool keep_stats = false;            // keep per-read fetch counts and tiers of the last run

@@ -53,6 +53,7 @@ struct WarpSmem {
     uint16_t lane_nl[32][3];          // staged pushes of each lane per target list
     uint4 lane_x[32];                 // pending exact child of a lane that stopped mid-chain
     int32_t newc[kWNewC];             // chunks allocated for one commit
+    int32_t incl[32];                 // inclusive scan of the lanes' counts in one commit
 };
 
 struct WArgs {
@@ -331,7 +332,7 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
     WAlloc A;
     A.free_ids = a.free_ids + (size_t)wid * a.arena_chunks;
     A.base = wid * a.arena_chunks; A.cap = a.arena_chunks; A.bump = 0; A.free_top = 0;
-    uint4 *stage_lane = a.stage + (size_t)wid * 3 * 32 * kWL + (size_t)lane * kWL;
+    uint4 *stage_lane = a.stage + (size_t)wid * 3 * 32 * kWL + (size_t)lane * kWL;   // list L at + L * 32 * kWL
     uint4 *prec_w = a.prec + (size_t)wid * 32 * kWR;
     // the staging list of each push kind: kinds whose target buckets coincide share a list, so the
     // bucket keeps the push order
@@ -604,12 +605,24 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                 if (need > kWNewC || !A.alloc_n(need, S->newc, lane)) { ret = kErrStack; fail = true; break; }
                 // chain the new chunks on top of c0
                 for (int t = lane; t < need; t += 32) a.chunk_prev[S->newc[t]] = t == 0 ? c0 : S->newc[t - 1];
-                const uint4 *src = stage_lane + (size_t)L * 32 * kWL;
-                int g = cnt0 + (incl - cntX);
-                for (int t = 0; t < cntX; ++t, ++g) {
-                    int ci = g / kWCH;
-                    int chunk = c0 >= 0 ? (ci == 0 ? c0 : S->newc[ci - 1]) : S->newc[ci];
-                    chunks[(size_t)chunk * kWCH + (g % kWCH)] = src[t];
+                // copy: output position p (0..T) comes from the lane j with incl[j-1] <= p < incl[j]
+                S->incl[lane] = incl;
+                __syncwarp();
+                const uint4 *stw = a.stage + (size_t)wid * 3 * 32 * kWL + (size_t)L * 32 * kWL;
+                for (int p0 = 0; p0 < T; p0 += 32) {
+                    const int p = p0 + lane;
+                    if (p < T) {
+                        int lo = 0, hi = 31;          // first lane whose inclusive count exceeds p
+                        while (lo < hi) {
+                            int mid = (lo + hi) >> 1;
+                            if (S->incl[mid] > p) hi = mid; else lo = mid + 1;
+                        }
+                        const int before = lo ? S->incl[lo - 1] : 0;
+                        const int g = cnt0 + p;
+                        const int ci = g / kWCH;
+                        const int chunk = c0 >= 0 ? (ci == 0 ? c0 : S->newc[ci - 1]) : S->newc[ci];
+                        chunks[(size_t)chunk * kWCH + (g % kWCH)] = stw[(size_t)lo * kWL + (p - before)];
+                    }
                 }
                 __syncwarp();
                 if (lane == 0) {
@@ -665,7 +678,7 @@ publish:
 }
 
 template <bool TRACE>
-__global__ void __launch_bounds__(32) warp_kernel(const __grid_constant__ WArgs a)
+__global__ void __launch_bounds__(32, 16) warp_kernel(const __grid_constant__ WArgs a)
 {
     extern __shared__ __align__(16) unsigned char wsm_raw[];
     WarpSmem *S = (WarpSmem *)wsm_raw;
