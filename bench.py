@@ -166,6 +166,7 @@ def main():
     ap.add_argument("--data-dir", default=None)
     ap.add_argument("--trace", action="store_true", help="compute per-read trace hashes (verification mode)")
     ap.add_argument("--t0-cap", type=int, default=1024, help="first-tier stack entries per thread")
+    ap.add_argument("--warp-arena", type=int, default=16384, help="warp-tier stack chunks (32 entries) per warp")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -210,6 +211,7 @@ def main():
     ix = galn_b200.Index(prefix, device=local)
     ix.set_trace(args.trace)
     ix.set_tuning(t0_cap=args.t0_cap)
+    ix.set_warp_tier(True, args.warp_arena)
     engine = galn_b200.GALN_ENGINE_PERSISTENT if args.engine == "persistent" else galn_b200.GALN_ENGINE_PLAIN
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 

@@ -678,7 +678,7 @@ publish:
 }
 
 template <bool TRACE>
-__global__ void __launch_bounds__(32, 16) warp_kernel(const __grid_constant__ WArgs a)
+__global__ void __launch_bounds__(32) warp_kernel(const __grid_constant__ WArgs a)
 {
     extern __shared__ __align__(16) unsigned char wsm_raw[];
     WarpSmem *S = (WarpSmem *)wsm_raw;
