@@ -281,6 +281,7 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
             int nw = std::min(ne, res_w);
             int arena = ix->warp_arena;
             if (pass == 1) {
+                nw = std::min(nw, 256);   // few reads get here; keep the big arenas' footprint bounded
                 int64_t full = ((int64_t)o->max_entries + 16 + kWarpMaxStacks * 32) / 32 + 1;
                 arena = (int)std::min<int64_t>(std::max<int64_t>(full, arena), 1 << 22);
             }

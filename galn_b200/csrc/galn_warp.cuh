@@ -46,11 +46,11 @@ struct WarpSmem {
     uint8_t q[kWMaxLen];
     // per pop of each lane: pushes (bits 0-7, the fused exact child not counted), has an exact child
     // (bit 8), index blocks read (bits 16-31)
-    uint32_t meta[32][kWR];
+    uint32_t meta[32][kWR + 1];       // one word of padding per row: lanes writing the same pop hit distinct banks
     uint4 hz[32];                     // hazard entry of each lane
     uint64_t hk[32], hl[32];          // its interval after the exact tail
     int32_t lane_np[32], lane_end[32];
-    uint16_t lane_nl[32][3];          // staged pushes of each lane per target list
+    uint32_t lane_nl[32][3];          // staged pushes of each lane per target list
     uint4 lane_x[32];                 // pending exact child of a lane that stopped mid-chain
     int32_t newc[kWNewC];             // chunks allocated for one commit
     int32_t incl[32];                 // inclusive scan of the lanes' counts in one commit
@@ -271,9 +271,9 @@ __device__ __forceinline__ void lane_chain(const IndexView &ix, const BatchOpt &
 #undef WPUSH
     S->lane_np[lane] = np;
     S->lane_end[lane] = endc;
-    S->lane_nl[lane][0] = (uint16_t)nl0;
-    S->lane_nl[lane][1] = (uint16_t)nl1;
-    S->lane_nl[lane][2] = (uint16_t)nl2;
+    S->lane_nl[lane][0] = (uint32_t)nl0;
+    S->lane_nl[lane][1] = (uint32_t)nl1;
+    S->lane_nl[lane][2] = (uint32_t)nl2;
 }
 
 // the warp's chunk allocator (warp-uniform state; every lane holds the same copy)
