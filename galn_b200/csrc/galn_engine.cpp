@@ -50,7 +50,15 @@ static inline int score_of(int m, int o, int e, const galn_opts *p) { return m *
 
 int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine, galn_results *out)
 {
+    return run_job_multi(ix, o, 1, nullptr, in, engine, out);
+}
+
+// sets[batch_set[b]] are the options of bwa batch b (all sets[0] when batch_set is NULL)
+int run_job_multi(galn_index *ix, const galn_opts *sets, int n_sets, const int32_t *batch_set, const galn_reads *in,
+                  int engine, galn_results *out)
+{
     double t_start = now_ms();
+    if (!sets || n_sets < 1) return GALN_EINVAL;
     const int n = in->n_reads;
     if (n < 0 || (n > 0 && (!in->seq || !in->offset))) return GALN_EINVAL;
     JobBufs &B = ix->ws;
@@ -82,7 +90,19 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
     std::vector<HostBatchOpt> bopt((size_t)std::max(n_batches, 1));
     int max_stacks = 1;
     bool wide = ix->dev.seq_len >= (1ull << 38);
+    std::vector<const galn_opts *> bset((size_t)std::max(n_batches, 1), &sets[0]);
     for (int b = 0; b < n_batches; ++b) {
+        if (batch_set) {
+            if (batch_set[b] < 0 || batch_set[b] >= n_sets) return GALN_EINVAL;
+            bset[b] = &sets[batch_set[b]];
+        }
+    }
+    int64_t max_entries_all = 0;
+    int seed_part = 0;
+    for (int b = 0; b < n_batches; ++b) {
+        const galn_opts *o = bset[b];
+        max_entries_all = std::max<int64_t>(max_entries_all, o->max_entries);
+        if (o->seed_len >= 0 && o->seed_len < max_len) seed_part = std::max(seed_part, o->seed_len);
         HostBatchOpt &h = bopt[b];
         memset(&h, 0, sizeof(h));
         h.s_mm = o->s_mm; h.s_gapo = o->s_gapo; h.s_gape = o->s_gape; h.mode = o->mode;
@@ -99,13 +119,17 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
     }
     std::vector<int32_t> maxdiff((size_t)std::max(n, 1));
     {
-        std::unordered_map<int, int> cache;
+        std::unordered_map<uint64_t, int> cache;   // (fnr bits, length) -> max_diff
         for (int r = 0; r < n; ++r) {
             int len = (int)(in->offset[r + 1] - in->offset[r]);
+            const galn_opts *o = bset[bid[r]];
             int md;
             if (o->fnr > 0.0) {
-                auto it = cache.find(len);
-                if (it == cache.end()) it = cache.emplace(len, galn_cal_maxdiff(len, 0.02, o->fnr)).first;
+                uint32_t fb;
+                memcpy(&fb, &o->fnr, 4);
+                uint64_t key = ((uint64_t)fb << 32) | (uint32_t)len;
+                auto it = cache.find(key);
+                if (it == cache.end()) it = cache.emplace(key, galn_cal_maxdiff(len, 0.02, o->fnr)).first;
                 md = it->second;
             } else md = bopt[bid[r]].max_diff;
             maxdiff[r] = md;
@@ -166,7 +190,7 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
     job.n_reads = n; job.n_batches = n_batches;
     job.seq = (uint8_t *)B.seq.p; job.query = (uint8_t *)B.query.p; job.off = (int64_t *)B.off.p;
     job.bidx = (int32_t *)B.bidx.p; job.maxdiff = (int32_t *)B.maxdiff.p; job.bopt = (HostBatchOpt *)B.bopt.p;
-    job.seed_len = o->seed_len; job.max_len = max_len; job.max_stacks = max_stacks; job.any_wide = wide ? 1 : 0;
+    job.seed_len = seed_part; job.max_len = max_len; job.max_stacks = max_stacks; job.any_wide = wide ? 1 : 0;
     job.trace = ix->trace ? 1 : 0;
     job.out_n = (int32_t *)B.out_n.p; job.out_off = (int64_t *)B.out_off.p; job.out_pops = (uint64_t *)B.out_pops.p;
     job.out_trace = (uint64_t *)B.out_trace.p; job.out_peak = (int32_t *)B.out_peak.p;
@@ -262,14 +286,16 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
     std::swap(cur, nxt);
 
     // ---- W: the warp tier for the reads that overflowed T0 (those it can take) ----
-    const bool warp_ok = ix->use_warp && !wide && o->s_mm > 0 && o->s_gapo > 0 && o->s_gape > 0;
+    const bool warp_ok = ix->use_warp && !wide;
     if (warp_ok && n_ovf > 0) {
         std::vector<int32_t> ov((size_t)n_ovf), elig, rest;
         ECK(cudaMemcpyAsync(ov.data(), cur, (size_t)n_ovf * 4, cudaMemcpyDeviceToHost, st));
         ECK(cudaStreamSynchronize(st));
         for (int32_t r : ov) {
             int len = (int)(in->offset[r + 1] - in->offset[r]);
-            if (len <= kWarpMaxLen && bopt[bid[r]].n_stacks <= kWarpMaxStacks && bopt[bid[r]].n_stacks > 0) elig.push_back(r);
+            const HostBatchOpt &h = bopt[bid[r]];
+            if (len <= kWarpMaxLen && h.n_stacks <= kWarpMaxStacks && h.n_stacks > 0 && h.s_mm > 0 && h.s_gapo > 0 &&
+                h.s_gape > 0) elig.push_back(r);
             else rest.push_back(r);
         }
         // pass 1 with the tuned arena; pass 2 for its overflow with arenas that hold the max_entries cut-off
@@ -282,7 +308,7 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
             int arena = ix->warp_arena;
             if (pass == 1) {
                 nw = std::min(nw, 256);   // few reads get here; keep the big arenas' footprint bounded
-                int64_t full = ((int64_t)o->max_entries + 16 + kWarpMaxStacks * 32) / 32 + 1;
+                int64_t full = (max_entries_all + 16 + kWarpMaxStacks * 32) / 32 + 1;
                 arena = (int)std::min<int64_t>(std::max<int64_t>(full, arena), 1 << 22);
             }
             while (nw > 1 && warp_ws_bytes(nw, arena, aln_cap_w) > budget) nw /= 2;
@@ -360,7 +386,7 @@ int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine
         t.persistent = true;
         t.block = 128;
         // live entries: t1_cap, then 2^19, then enough for the max_entries cut-off
-        int64_t full = std::min<int64_t>((int64_t)o->max_entries + 16, 0x7fffffff);
+        int64_t full = std::min<int64_t>(max_entries_all + 16, 0x7fffffff);
         t.cap = tier == 2 ? ix->t1_cap : tier == 3 ? (int)std::min<int64_t>(full, 1 << 19) : (int)full;
         if (t.cap < 16) t.cap = 16;
         t.aln_cap = (int)std::min<int64_t>(aln_cap, 1 << 24);

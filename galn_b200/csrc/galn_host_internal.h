@@ -90,4 +90,6 @@ namespace galn {
 void results_fill(galn_results *out, int n, const int32_t *n_aln, const int64_t *dev_off, const uint64_t *rec_words,
                   const uint64_t *pops, const uint64_t *trace);
 int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);
+int run_job_multi(galn_index *ix, const galn_opts *sets, int n_sets, const int32_t *batch_set, const galn_reads *in,
+                  int engine, galn_results *out);
 }  // namespace galn

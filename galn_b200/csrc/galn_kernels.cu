@@ -181,10 +181,10 @@ __device__ __forceinline__ void run_read(const KArgs &a, int pos, int slot)
     const int md = a.maxdiff[r];
     uint64_t *W = a.ws.wid + (size_t)slot * a.ws.wcap;
     uint64_t *SW = W + (len + 1);
-    const bool use_seed = len > a.seed_len;
+    const bool use_seed = len > bo.seed_len;
     uint32_t fetches = 0;
     cal_width(a.ix, len, q, W, fetches);
-    if (use_seed) cal_width(a.ix, a.seed_len, q + (len - a.seed_len), SW, fetches);
+    if (use_seed) cal_width(a.ix, bo.seed_len, q + (len - bo.seed_len), SW, fetches);
     SearchResult R = match_gap<WIDE, FREELIST, TRACE>(a.ix, bo, md, len, q, W, SW, use_seed, a.ws, slot, fetches);
     int ret = R.ret;
     if (ret > 0) {

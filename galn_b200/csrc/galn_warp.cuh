@@ -321,10 +321,10 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
     if (lane < kWMaxB / 32) S->mask[lane] = 0;
     __syncwarp();
     uint32_t fetches = 0;   // index blocks read by this lane (chains include discarded speculation)
-    const bool use_seed = len > a.seed_len;
+    const bool use_seed = len > O.seed_len;
     if (lane == 0) {
         cal_width(ix, len, S->q, S->W, fetches);
-        if (use_seed) cal_width(ix, a.seed_len, S->q + (len - a.seed_len), S->SW, fetches);
+        if (use_seed) cal_width(ix, O.seed_len, S->q + (len - O.seed_len), S->SW, fetches);
     }
     __syncwarp();
     uint32_t f_alg = __shfl_sync(FULL, fetches, 0);   // algorithmic count: widths, then replayed chains
