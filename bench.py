@@ -152,6 +152,54 @@ def cpu_reference(prefix, reads, opts, sample, d, steps=1, warmup=0):
                        f" search time from its own timing line"), None
 
 
+def serving_run(ix, ref, n_requests: int, seed: int, rate_hz: float, scale: float):
+    """The serving configuration on the resident index: Poisson arrivals, requests of 1k-500k reads
+    (log-uniform, times `scale`), lengths 36-150 bp, half default and half aDNA options. Returns reads/s and
+    submit-to-result latency percentiles, next to the same requests as plain per-request launches in
+    arrival order (one at a time), and whether every request's .sai is the same both ways."""
+    import numpy as np
+
+    import galn_b200
+    from galn_b200 import synth
+    t = time.time()
+    reqs = synth.serving_requests(n_requests, seed, ref, scale=scale, rate_hz=rate_hz)
+    items = [(r["t_arrival"], r["opts"], galn_b200.Reads(r["reads"].ascii(), r["reads"].off.copy())) for r in reqs]
+    total = sum(len(x[2]) for x in items)
+    log(f"[bench] serving: {len(items)} requests, {total} reads generated in {time.time() - t:.1f} s")
+    srv = galn_b200.Server(ix)
+    t0 = time.perf_counter()
+    ids, t_sub = [], []
+    for t_arr, opts, reads in items:
+        dt = t_arr - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        t_sub.append(time.perf_counter() - t0)
+        ids.append(srv.submit(opts, reads))
+    outs = [srv.wait(i) for i in ids]
+    t_end = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    service, same = [], True
+    for (t_arr, opts, reads), o in zip(items, outs):
+        t1 = time.perf_counter()
+        p = galn_b200.aln(ix, opts, reads, galn_b200.GALN_ENGINE_PLAIN)
+        service.append(time.perf_counter() - t1)
+        same = same and p.sai_bytes() == o.sai_bytes()
+    t_free, lat = 0.0, []
+    for (t_arr, _, _), sv in zip(items, service):
+        start = max(t_arr, t_free)
+        t_free = start + sv
+        lat.append(t_free - t_arr)
+    lat = np.array(lat) * 1e3
+    return {"requests": len(items), "reads": total, "arrival_rate_hz": rate_hz,
+            "reads_per_s": total / max(t_end - t_sub[0], 1e-9), "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "steps": st["steps"], "device_busy_s": st["busy_ms"] / 1e3,
+            "plain_per_request": {"reads_per_s": total / sum(service), "p50_ms": float(np.percentile(lat, 50)),
+                                  "p99_ms": float(np.percentile(lat, 99)),
+                                  "latency": "FIFO queue of one-at-a-time launches with the same arrivals"},
+            "sai_identical_served_vs_plain": bool(same)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -167,6 +215,8 @@ def main():
     ap.add_argument("--trace", action="store_true", help="compute per-read trace hashes (verification mode)")
     ap.add_argument("--t0-cap", type=int, default=1024, help="first-tier stack entries per thread")
     ap.add_argument("--warp-arena", type=int, default=16384, help="warp-tier stack chunks (32 entries) per warp")
+    ap.add_argument("--serve-requests", type=int, default=40, help="requests in the serving run (0: none)")
+    ap.add_argument("--serve-rate", type=float, default=16.0, help="request arrival rate (per second)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -288,6 +338,10 @@ def main():
         plain = {"value": total_reads / max_over_ranks(statistics.mean(pdev)),
                  "e2e": total_reads / max_over_ranks(statistics.mean(pe2e)), "sai_md5_same": pmd5 == md5}
 
+    serving = None
+    if args.serve_requests > 0 and args.workload == "adna":
+        serving = serving_run(ix, ref, args.serve_requests, 1000 + rank, args.serve_rate, args.scale)
+
     cpu = None
     if rank == 0 and world == 1 and args.cpu_sample > 0:
         cpu, why = cpu_reference(prefix, reads, opts, args.cpu_sample, d)
@@ -325,6 +379,8 @@ def main():
     }
     if plain:
         line["plain_engine"] = plain
+    if serving:
+        line["serving"] = serving
     print(json.dumps(line))
     return 0
 

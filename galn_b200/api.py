@@ -81,6 +81,15 @@ def lib():
     L.galn_index_set_trace.argtypes = [vp, C.c_int]
     L.galn_index_set_warp_tier.argtypes = [vp, C.c_int, C.c_int]
     L.galn_last_warp_counters.argtypes = [vp, vp, C.c_int]
+    L.galn_server_start.restype = vp
+    L.galn_server_start.argtypes = [vp, C.c_size_t, C.POINTER(C.c_int)]
+    L.galn_server_stop.argtypes = [vp]
+    L.galn_server_configure.argtypes = [vp, C.c_int, C.c_int]
+    L.galn_aln_submit.restype = C.c_int64
+    L.galn_aln_submit.argtypes = [vp, C.POINTER(Options), C.POINTER(_Reads)]
+    L.galn_aln_wait.argtypes = [vp, C.c_int64, C.c_int, C.POINTER(_Results)]
+    L.galn_server_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     L.galn_version.restype = C.c_char_p
     _lib = L
     return L
@@ -294,3 +303,51 @@ def aln(index: Index, args: list[str] | Options, reads: Reads | str,
 
 def write_sai(path: str, res: Results) -> int:
     return res.write_sai(path)
+
+
+class Server:
+    """Continuous-batching request loop on a resident index (galn_server_*)."""
+
+    def __init__(self, index: Index, stack_bytes: int = 0, step_reads: int | None = None, max_active: int = 64):
+        err = C.c_int(0)
+        self.index = index
+        self.h = lib().galn_server_start(index.h, stack_bytes, C.byref(err))
+        if not self.h:
+            raise GalnError(f"cannot start the server ({err.value})")
+        if step_reads is not None:
+            lib().galn_server_configure(self.h, step_reads, max_active)
+        self._keep = {}
+
+    def submit(self, args: list[str] | Options, reads: Reads) -> int:
+        opts = args if isinstance(args, Options) else parse_options(list(args))
+        cr, keep = reads.c_struct()
+        rid = lib().galn_aln_submit(self.h, C.byref(opts), C.byref(cr))
+        if rid <= 0:
+            raise GalnError(f"submit failed ({rid})")
+        self._keep[rid] = opts
+        return rid
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> Results:
+        res = _Results()
+        rc = lib().galn_aln_wait(self.h, rid, timeout_ms, C.byref(res))
+        if rc != 0:
+            raise GalnError(f"request {rid} failed ({rc})")
+        out = Results(res, self._keep.pop(rid))
+        lib().galn_results_free(C.byref(res))
+        return out
+
+    def stats(self) -> dict:
+        p50, p99, busy = C.c_double(), C.c_double(), C.c_double()
+        nr, nreads, steps = C.c_int64(), C.c_int64(), C.c_int64()
+        lib().galn_server_stats(self.h, C.byref(p50), C.byref(p99), C.byref(nr), C.byref(nreads), C.byref(busy),
+                                C.byref(steps))
+        return dict(p50_ms=p50.value, p99_ms=p99.value, requests=nr.value, reads=nreads.value, busy_ms=busy.value,
+                    steps=steps.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().galn_server_stop(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

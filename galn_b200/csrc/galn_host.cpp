@@ -345,15 +345,6 @@ extern "C" int galn_index_info(const galn_index *ix, uint64_t *seq_len, uint64_t
 // ---------------------------------------------------------------------------------------------------
 // results and .sai
 
-namespace {
-struct ResultsPriv {
-    std::vector<int32_t> n_aln;
-    std::vector<int64_t> rec_off;
-    std::vector<galn_aln1> rec;
-    std::vector<uint64_t> pops, trace;
-};
-}  // namespace
-
 void galn::results_fill(galn_results *out, int n, const int32_t *n_aln, const int64_t *dev_off,
                         const uint64_t *rec_words, const uint64_t *pops, const uint64_t *trace)
 {

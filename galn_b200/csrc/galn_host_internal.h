@@ -87,6 +87,13 @@ struct galn_index {
 };
 
 namespace galn {
+// what galn_results._priv owns
+struct ResultsPriv {
+    std::vector<int32_t> n_aln;
+    std::vector<int64_t> rec_off;
+    std::vector<galn_aln1> rec;
+    std::vector<uint64_t> pops, trace;
+};
 void results_fill(galn_results *out, int n, const int32_t *n_aln, const int64_t *dev_off, const uint64_t *rec_words,
                   const uint64_t *pops, const uint64_t *trace);
 int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);

@@ -1,12 +1,20 @@
-// galn_serve.cpp -- the request loop around a resident index.
+// galn_serve.cpp -- continuous batching of alignment requests on a resident index.
 //
-// galn_aln_submit copies a request (its own options and bwa batch boundaries) into a queue; a worker thread
-// takes requests in arrival order and runs them on the index. galn_aln_wait blocks until a request's
-// results are ready. Each request's results are computed exactly as by galn_aln_run_batch of that request
-// alone (the per-batch options come only from the request's own reads), so they do not depend on what else
-// is queued.
+// Requests (each with its own options and its own bwa batch boundaries) are copied in by galn_aln_submit.
+// A scheduler thread runs steps back to back. Each step takes up to `step_reads` reads from the admitted
+// requests -- every request first gets an equal share, what is left goes to the oldest -- and searches them
+// together in one pass of the device tiers, so requests share the same kernels. A request that arrives
+// while a step runs joins the next step; a request leaves as soon as its last read has been searched.
+// Admission is bounded by the step size (the device workspace of one step) and by max_active requests in
+// flight; later requests wait in the queue.
+//
+// Results do not depend on what else is in a step: each read's options are its request's, and each bwa
+// batch's options come from the longest read of that batch in its own request (batch_max_len), whether the
+// request is searched in one step or spread over several.
+#include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -19,13 +27,24 @@
 
 namespace {
 
+double now_ms()
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 struct Request {
     int64_t id = 0;
     galn_opts opt;
     std::vector<char> seq;
     std::vector<int64_t> off;
-    std::vector<int32_t> batch;
-    std::vector<int32_t> bmax;
+    std::vector<int32_t> batch;        // own bwa batch of each read
+    std::vector<int32_t> bmax;         // longest read of each own batch
+    int n = 0, next = 0;
+    // results, in read order
+    std::vector<int32_t> n_aln;
+    std::vector<galn_aln1> rec;
+    std::vector<uint64_t> pops, trace;
+    double t_submit = 0, t_done = 0;
     int rc = 0;
     bool done = false;
     galn_results res;
@@ -37,54 +56,175 @@ struct galn_server {
     galn_index *ix = nullptr;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<Request *> queue;
+    std::deque<Request *> queue;       // submitted, not yet admitted
+    std::vector<Request *> active;     // admitted, not finished
     std::map<int64_t, Request *> all;
     int64_t next_id = 1;
     bool stop = false;
-    size_t max_queued = 4096;
+    size_t max_queued = 1 << 16;
+    int max_active = 64;
+    int step_reads = 1 << 18;
+    // statistics
+    std::vector<double> lat_ms;
+    int64_t reads_done = 0, steps = 0;
+    double busy_ms = 0;
     std::thread worker;
 };
 
+static void finish_request(Request *rq)
+{
+    auto *P = new galn::ResultsPriv();
+    P->n_aln.swap(rq->n_aln);
+    P->rec.swap(rq->rec);
+    P->pops.swap(rq->pops);
+    P->trace.swap(rq->trace);
+    P->rec_off.resize((size_t)rq->n + 1);
+    int64_t t = 0;
+    for (int r = 0; r < rq->n; ++r) {
+        P->rec_off[r] = t;
+        if (P->n_aln[r] > 0) t += P->n_aln[r];
+    }
+    P->rec_off[rq->n] = t;
+    if (P->rec.empty()) P->rec.resize(1);
+    if (P->n_aln.empty()) { P->n_aln.resize(1); P->pops.resize(1); P->trace.resize(1); }
+    rq->res.n_reads = rq->n;
+    rq->res.n_aln = P->n_aln.data();
+    rq->res.rec_offset = P->rec_off.data();
+    rq->res.rec = P->rec.data();
+    rq->res.n_pops = P->pops.data();
+    rq->res.trace = P->trace.data();
+    rq->res._priv = P;
+    std::vector<char>().swap(rq->seq);
+}
+
 static void serve_loop(galn_server *s)
 {
+    struct Piece { Request *rq; int r0, m; };
+    std::vector<char> seq;
+    std::vector<int64_t> off;
+    std::vector<int32_t> batch, bmax, bset;
+    std::vector<galn_opts> sets;
     for (;;) {
-        Request *rq = nullptr;
+        std::vector<Piece> pieces;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
-            if (s->queue.empty()) return;
-            rq = s->queue.front();
-            s->queue.pop_front();
+            s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty() || !s->active.empty(); });
+            if (s->stop && s->queue.empty() && s->active.empty()) return;
+            while (!s->queue.empty() && (int)s->active.size() < s->max_active) {
+                s->active.push_back(s->queue.front());
+                s->queue.pop_front();
+            }
+            // equal shares first, then the oldest requests take what is left
+            int budget = s->step_reads;
+            int na = (int)s->active.size();
+            int share = std::max(4096, s->step_reads / std::max(1, na));
+            std::vector<int> take(na, 0);
+            for (int a = 0; a < na && budget > 0; ++a) {
+                Request *rq = s->active[a];
+                int m = std::min({rq->n - rq->next, share, budget});
+                take[a] = m;
+                budget -= m;
+            }
+            for (int a = 0; a < na && budget > 0; ++a) {
+                Request *rq = s->active[a];
+                int m = std::min(rq->n - rq->next - take[a], budget);
+                take[a] += m;
+                budget -= m;
+            }
+            for (int a = 0; a < na; ++a)
+                if (take[a] > 0 || s->active[a]->n == 0) pieces.push_back({s->active[a], s->active[a]->next, take[a]});
+        }
+        // one combined job: every request is one option set, every (request, own batch) one batch
+        seq.clear(); off.clear(); batch.clear(); bmax.clear(); bset.clear(); sets.clear();
+        off.push_back(0);
+        for (size_t p = 0; p < pieces.size(); ++p) {
+            Request *rq = pieces[p].rq;
+            sets.push_back(rq->opt);
+            std::map<int, int> gb;   // own batch -> batch of the step
+            for (int r = pieces[p].r0; r < pieces[p].r0 + pieces[p].m; ++r) {
+                int own = rq->batch[r];
+                auto it = gb.find(own);
+                if (it == gb.end()) {
+                    it = gb.emplace(own, (int)bmax.size()).first;
+                    bmax.push_back(rq->bmax[own]);
+                    bset.push_back((int32_t)p);
+                }
+                seq.insert(seq.end(), rq->seq.begin() + rq->off[r], rq->seq.begin() + rq->off[r + 1]);
+                off.push_back((int64_t)seq.size());
+                batch.push_back(it->second);
+            }
         }
         galn_reads in;
         memset(&in, 0, sizeof(in));
-        in.n_reads = (int32_t)rq->off.size() - 1;
-        in.seq = rq->seq.data();
-        in.offset = rq->off.data();
-        in.batch = rq->batch.empty() ? nullptr : rq->batch.data();
-        in.batch_max_len = rq->bmax.empty() ? nullptr : rq->bmax.data();
-        in.n_batches = (int32_t)rq->bmax.size();
-        memset(&rq->res, 0, sizeof(rq->res));
-        int rc = galn_aln_run_batch(s->ix, &rq->opt, &in, GALN_ENGINE_PERSISTENT, &rq->res);
+        in.n_reads = (int32_t)batch.size();
+        in.seq = seq.empty() ? "" : seq.data();
+        in.offset = off.data();
+        in.batch = batch.data();
+        in.batch_max_len = bmax.data();
+        in.n_batches = (int32_t)bmax.size();
+        galn_results res;
+        memset(&res, 0, sizeof(res));
+        int rc = 0;
+        double t0 = now_ms();
+        if (in.n_reads > 0) {
+            std::lock_guard<std::mutex> lk(s->ix->mu);
+            rc = galn::run_job_multi(s->ix, sets.data(), (int)sets.size(), bset.data(), &in, GALN_ENGINE_PERSISTENT, &res);
+        }
+        double t1 = now_ms();
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            rq->rc = rc;
-            rq->done = true;
-            std::vector<char>().swap(rq->seq);
+            s->busy_ms += t1 - t0;
+            ++s->steps;
+            int j = 0;
+            for (auto &pc : pieces) {
+                Request *rq = pc.rq;
+                for (int t = 0; t < pc.m; ++t, ++j) {
+                    int na = rc ? rq->rc : res.n_aln[j];
+                    rq->n_aln.push_back(rc ? GALN_ERR_STACK : na);
+                    rq->pops.push_back(rc ? 0 : res.n_pops[j]);
+                    rq->trace.push_back(rc ? 0 : res.trace[j]);
+                    if (!rc && na > 0)
+                        rq->rec.insert(rq->rec.end(), res.rec + res.rec_offset[j], res.rec + res.rec_offset[j + 1]);
+                }
+                if (rc) rq->rc = rc;
+                rq->next += pc.m;
+                s->reads_done += pc.m;
+                if (rq->next >= rq->n || rc) {
+                    finish_request(rq);
+                    rq->t_done = now_ms();
+                    rq->done = true;
+                    s->lat_ms.push_back(rq->t_done - rq->t_submit);
+                    s->active.erase(std::find(s->active.begin(), s->active.end(), rq));
+                }
+            }
         }
+        if (in.n_reads > 0) galn_results_free(&res);
         s->cv_done.notify_all();
     }
 }
 
 extern "C" galn_server *galn_server_start(galn_index *ix, size_t stack_bytes, int *err)
 {
-    (void)stack_bytes;
     if (!ix) { if (err) *err = GALN_EINVAL; return nullptr; }
     auto *s = new galn_server();
     s->ix = ix;
+    if (stack_bytes) {
+        // a step's device workspace scales with its reads: about 100 KB per first-tier thread slot
+        size_t reads = stack_bytes / (100 * 1024);
+        s->step_reads = (int)std::max<size_t>(16384, std::min<size_t>(reads, 1 << 20));
+    }
     s->worker = std::thread(serve_loop, s);
     if (err) *err = 0;
     return s;
+}
+
+extern "C" int galn_server_configure(galn_server *s, int step_reads, int max_active)
+{
+    if (!s || step_reads < 1024 || max_active < 1) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->step_reads = step_reads;
+    s->max_active = max_active;
+    return 0;
 }
 
 extern "C" int galn_server_stop(galn_server *s)
@@ -97,7 +237,7 @@ extern "C" int galn_server_stop(galn_server *s)
     s->cv_work.notify_all();
     s->worker.join();
     for (auto &kv : s->all) {
-        if (kv.second->done && kv.second->rc == 0) galn_results_free(&kv.second->res);
+        if (kv.second->done) galn_results_free(&kv.second->res);
         delete kv.second;
     }
     delete s;
@@ -109,16 +249,33 @@ extern "C" int64_t galn_aln_submit(galn_server *s, const galn_opts *o, const gal
     if (!s || !o || !in || in->n_reads < 0 || (in->n_reads > 0 && (!in->seq || !in->offset))) return GALN_EINVAL;
     auto *rq = new Request();
     rq->opt = *o;
-    int n = in->n_reads;
+    const int n = in->n_reads;
+    rq->n = n;
     int64_t base = n ? in->offset[0] : 0, total = n ? in->offset[n] - base : 0;
     rq->seq.assign(in->seq + base, in->seq + base + total);
     rq->off.resize((size_t)n + 1);
+    int nb = 0;
+    rq->batch.resize((size_t)n);
     for (int r = 0; r <= n; ++r) rq->off[r] = in->offset[r] - base;
-    if (in->batch) rq->batch.assign(in->batch, in->batch + n);
-    if (in->batch_max_len) rq->bmax.assign(in->batch_max_len, in->batch_max_len + in->n_batches);
+    for (int r = 0; r < n; ++r) {
+        int64_t len = rq->off[r + 1] - rq->off[r];
+        int b = in->batch ? in->batch[r] : r / galn::kBatchReads;
+        if (len < 0 || len > 65535 || b < 0) { delete rq; return GALN_EINVAL; }
+        rq->batch[r] = b;
+        nb = std::max(nb, b + 1);
+    }
+    if (in->batch_max_len) nb = std::max(nb, (int)in->n_batches);
+    rq->bmax.assign((size_t)std::max(nb, 1), 0);
+    for (int r = 0; r < n; ++r) rq->bmax[rq->batch[r]] = std::max(rq->bmax[rq->batch[r]], (int32_t)(rq->off[r + 1] - rq->off[r]));
+    if (in->batch_max_len)
+        for (int b = 0; b < in->n_batches; ++b) rq->bmax[b] = std::max(rq->bmax[b], in->batch_max_len[b]);
+    rq->n_aln.reserve((size_t)n);
+    rq->pops.reserve((size_t)n);
+    rq->trace.reserve((size_t)n);
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->queue.size() >= s->max_queued) { delete rq; return GALN_EBUSY; }
     rq->id = s->next_id++;
+    rq->t_submit = now_ms();
     s->all[rq->id] = rq;
     s->queue.push_back(rq);
     s->cv_work.notify_one();
@@ -136,8 +293,25 @@ extern "C" int galn_aln_wait(galn_server *s, int64_t id, int timeout_ms, galn_re
     if (timeout_ms < 0) s->cv_done.wait(lk, ready);
     else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return GALN_ETIMEOUT;
     int rc = rq->rc;
-    if (rc == 0) *out = rq->res;
+    *out = rq->res;              // the caller owns the results now (galn_results_free)
     s->all.erase(it);
     delete rq;
     return rc;
+}
+
+extern "C" int galn_server_stats(galn_server *s, double *p50_ms, double *p99_ms, int64_t *n_requests, int64_t *n_reads,
+                                 double *busy_ms, int64_t *steps)
+{
+    if (!s) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    std::vector<double> v = s->lat_ms;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double q) { return v.empty() ? 0.0 : v[(size_t)std::min<double>(v.size() - 1, floor(q * (v.size() - 1) + 0.5))]; };
+    if (p50_ms) *p50_ms = pct(0.50);
+    if (p99_ms) *p99_ms = pct(0.99);
+    if (n_requests) *n_requests = (int64_t)v.size();
+    if (n_reads) *n_reads = s->reads_done;
+    if (busy_ms) *busy_ms = s->busy_ms;
+    if (steps) *steps = s->steps;
+    return 0;
 }

@@ -141,9 +141,12 @@ int galn_aln_run_batch(galn_index *ix, const galn_opts *o, const galn_reads *in,
 int galn_sai_write(const char *path, const galn_opts *o, const galn_results *res);
 
 /* ---- serving ---------------------------------------------------------------------------------------------- */
-/* A resident index serves requests with their own options and batch boundaries. Requests that arrive
- * while others run are admitted as device memory for their stacks frees up and share the device with
- * them; each request's results are the same bytes as a galn_aln_run_batch of it alone. */
+/* A resident index serves requests with their own options and batch boundaries (continuous batching):
+ * steps of up to step_reads reads are taken from all admitted requests (equal shares, then oldest first)
+ * and searched together; a request that arrives while a step runs joins the next one, and leaves when its
+ * last read is done. stack_bytes (0: default) bounds a step's device workspace. Each request's results
+ * are the same bytes as a galn_aln_run_batch of it alone. The reference's equivalent is its per-batch
+ * scheduling of one input file (src/galn.cu:605-635, 835-905). */
 typedef struct galn_server galn_server;
 galn_server *galn_server_start(galn_index *ix, size_t stack_bytes, int *err);
 int galn_server_stop(galn_server *s);
@@ -151,6 +154,13 @@ int galn_server_stop(galn_server *s);
 int64_t galn_aln_submit(galn_server *s, const galn_opts *o, const galn_reads *in);
 /* waits up to timeout_ms (-1: forever) for a request; on success moves its results into *out */
 int galn_aln_wait(galn_server *s, int64_t id, int timeout_ms, galn_results *out);
+/* reads per step (the device workspace of one step) and requests in flight at once (no reference
+ * counterpart; defaults 262144 and 64) */
+int galn_server_configure(galn_server *s, int step_reads, int max_active);
+/* submit-to-result latency percentiles of the finished requests, requests and reads finished, device
+ * busy milliseconds and steps run (no reference counterpart) */
+int galn_server_stats(galn_server *s, double *p50_ms, double *p99_ms, int64_t *n_requests, int64_t *n_reads,
+                      double *busy_ms, int64_t *steps);
 
 /* ---- search without device allocation --------------------------------------------------------------
  * No counterpart in the reference. For callers that may not allocate or free device memory while they
