@@ -48,23 +48,23 @@ static double now_ms()
 
 static inline int score_of(int m, int o, int e, const galn_opts *p) { return m * p->s_mm + o * p->s_gapo + e * p->s_gape; }
 
-int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine, galn_results *out)
+int run_job(galn_index *ix, ExecCtx &ctx, const galn_opts *o, const galn_reads *in, int engine, galn_results *out)
 {
-    return run_job_multi(ix, o, 1, nullptr, in, engine, out);
+    return run_job_multi(ix, ctx, o, 1, nullptr, in, engine, out);
 }
 
 // sets[batch_set[b]] are the options of bwa batch b (all sets[0] when batch_set is NULL)
-int run_job_multi(galn_index *ix, const galn_opts *sets, int n_sets, const int32_t *batch_set, const galn_reads *in,
-                  int engine, galn_results *out)
+int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_sets, const int32_t *batch_set,
+                  const galn_reads *in, int engine, galn_results *out)
 {
     double t_start = now_ms();
     if (!sets || n_sets < 1) return GALN_EINVAL;
     const int n = in->n_reads;
     if (n < 0 || (n > 0 && (!in->seq || !in->offset))) return GALN_EINVAL;
-    JobBufs &B = ix->ws;
-    RunStats &S = ix->last;
+    JobBufs &B = ctx.ws;
+    RunStats &S = ctx.last;
     S = RunStats();
-    cudaStream_t st = ix->stream;
+    cudaStream_t st = ctx.stream;
     ECK(cudaSetDevice(ix->dev.device));
 
     // ---- per-read lengths, batches, options ----
@@ -208,6 +208,7 @@ int run_job_multi(galn_index *ix, const galn_opts *sets, int n_sets, const int32
     size_t free_b = 0, total_b = 0;
     ECK(cudaMemGetInfo(&free_b, &total_b));
     size_t budget = (size_t)((double)(free_b + B.ws.n) * ix->mem_fraction);
+    budget = std::min(budget, (size_t)((double)total_b * ix->mem_fraction * ctx.mem_share));
 
     cudaEvent_t e0, e1;
     ECK(cudaEventCreate(&e0));
@@ -256,7 +257,8 @@ int run_job_multi(galn_index *ix, const galn_opts *sets, int n_sets, const int32
     int n_ovf = 0;
     TierCfg t0;
     t0.tier = 0;
-    t0.freelist = false; t0.cap = ix->t0_cap; t0.aln_cap = ix->t0_aln; t0.block = ix->t0_block;
+    t0.freelist = false; t0.aln_cap = ix->t0_aln; t0.block = ix->t0_block;
+    t0.cap = engine == GALN_ENGINE_PLAIN ? ix->plain_t0_cap : ix->t0_cap;
     if (engine == GALN_ENGINE_PERSISTENT) {
         t0.persistent = true;
         RCK(run_tier(t0, cur, n, nxt, &n_ovf));
@@ -286,7 +288,7 @@ int run_job_multi(galn_index *ix, const galn_opts *sets, int n_sets, const int32
     std::swap(cur, nxt);
 
     // ---- W: the warp tier for the reads that overflowed T0 (those it can take) ----
-    const bool warp_ok = ix->use_warp && !wide;
+    const bool warp_ok = ix->use_warp && !wide && engine != GALN_ENGINE_PLAIN;
     if (warp_ok && n_ovf > 0) {
         std::vector<int32_t> ov((size_t)n_ovf), elig, rest;
         ECK(cudaMemcpyAsync(ov.data(), cur, (size_t)n_ovf * 4, cudaMemcpyDeviceToHost, st));
@@ -450,7 +452,7 @@ extern "C" int galn_aln_run_batch(galn_index *ix, const galn_opts *o, const galn
     if (engine != GALN_ENGINE_PLAIN && engine != GALN_ENGINE_PERSISTENT) return GALN_EINVAL;
     memset(out, 0, sizeof(*out));
     std::lock_guard<std::mutex> lk(ix->mu);
-    return galn::run_job(ix, o, in, engine, out);
+    return galn::run_job(ix, ix->main, o, in, engine, out);
 }
 
 extern "C" int galn_last_run_stats(galn_index *ix, double *ms_total, double *ms_kernels, int *tiers,
@@ -458,11 +460,11 @@ extern "C" int galn_last_run_stats(galn_index *ix, double *ms_total, double *ms_
 {
     if (!ix) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
-    if (ms_total) *ms_total = ix->last.ms_total;
-    if (ms_kernels) *ms_kernels = ix->last.ms_kernels;
-    if (tiers) *tiers = ix->last.tiers;
-    if (launches) *launches = ix->last.kernel_launches;
-    if (overflow) memcpy(overflow, ix->last.overflow_reads, sizeof(ix->last.overflow_reads));
+    if (ms_total) *ms_total = ix->main.last.ms_total;
+    if (ms_kernels) *ms_kernels = ix->main.last.ms_kernels;
+    if (tiers) *tiers = ix->main.last.tiers;
+    if (launches) *launches = ix->main.last.kernel_launches;
+    if (overflow) memcpy(overflow, ix->main.last.overflow_reads, sizeof(ix->main.last.overflow_reads));
     return 0;
 }
 
@@ -471,14 +473,14 @@ extern "C" int galn_last_run_profile(galn_index *ix, double *ms_device, double *
 {
     if (!ix) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
-    if (ms_device) *ms_device = ix->last.ms_device;
-    if (ms_tier) memcpy(ms_tier, ix->last.ms_tier, sizeof(ix->last.ms_tier));
-    if (tier_reads) memcpy(tier_reads, ix->last.tier_reads, sizeof(ix->last.tier_reads));
-    if (tier_threads) memcpy(tier_threads, ix->last.tier_threads, sizeof(ix->last.tier_threads));
+    if (ms_device) *ms_device = ix->main.last.ms_device;
+    if (ms_tier) memcpy(ms_tier, ix->main.last.ms_tier, sizeof(ix->main.last.ms_tier));
+    if (tier_reads) memcpy(tier_reads, ix->main.last.tier_reads, sizeof(ix->main.last.tier_reads));
+    if (tier_threads) memcpy(tier_threads, ix->main.last.tier_threads, sizeof(ix->main.last.tier_threads));
     if (fetch || tier) {
-        if ((size_t)n > ix->last.fetch.size()) return GALN_EINVAL;
-        if (fetch) memcpy(fetch, ix->last.fetch.data(), (size_t)n * 4);
-        if (tier) memcpy(tier, ix->last.tier_of.data(), (size_t)n);
+        if ((size_t)n > ix->main.last.fetch.size()) return GALN_EINVAL;
+        if (fetch) memcpy(fetch, ix->main.last.fetch.data(), (size_t)n * 4);
+        if (tier) memcpy(tier, ix->main.last.tier_of.data(), (size_t)n);
     }
     return 0;
 }
@@ -487,7 +489,7 @@ extern "C" int galn_last_warp_counters(galn_index *ix, uint64_t *counters, int n
 {
     if (!ix || !counters || n < 1) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
-    for (int q = 0; q < n && q < galn::kWarpDbg; ++q) counters[q] = ix->last.warp_dbg[q];
+    for (int q = 0; q < n && q < galn::kWarpDbg; ++q) counters[q] = ix->main.last.warp_dbg[q];
     return 0;
 }
 

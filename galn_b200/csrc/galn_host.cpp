@@ -275,6 +275,7 @@ static galn_index *index_from_words(const uint64_t hdr[5], const uint32_t *body,
         if (err) *err = GALN_ECUDA;
         return nullptr;
     }
+    ix->main.stream = ix->stream;
     int rc = dev_index_build(d, body, n_words, ix->stream);
     if (rc) {
         dev_index_free(d);
@@ -326,7 +327,7 @@ extern "C" int galn_index_close(galn_index *ix)
 {
     if (!ix) return GALN_EINVAL;
     cudaSetDevice(ix->dev.device);
-    ix->ws.release();
+    ix->main.ws.release();
     dev_index_free(ix->dev);
     if (ix->stream) cudaStreamDestroy(ix->stream);
     delete ix;

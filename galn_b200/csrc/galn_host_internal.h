@@ -67,17 +67,25 @@ struct RunStats {
     std::vector<int8_t> tier_of;     // per read, of the last run
 };
 
+// what one search job runs on: a stream, its device buffers and the statistics of its last run
+struct ExecCtx {
+    cudaStream_t stream = nullptr;
+    JobBufs ws;
+    RunStats last;
+    double mem_share = 1.0;            // of the budget this context's workspace may take
+};
+
 }  // namespace galn
 
 struct galn_index {
     galn::DevIndex dev;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     // the main context's stream
     int sms = 0;
-    std::mutex mu;
-    galn::JobBufs ws;
-    galn::RunStats last;
+    std::mutex mu;                     // serialises galn_aln_run_batch calls on the main context
+    galn::ExecCtx main;
     // tuning knobs (galn_tune.cpp sets them; defaults otherwise)
     int t0_cap = 1024, t0_aln = 32, t0_block = 128;
+    int plain_t0_cap = 4096;            // the plain engine's first tier (the reference's light_cap)
     int t1_cap = 65536, t1_aln = 1024;
     double mem_fraction = 0.6;          // of free device memory a job's workspace may take
     bool keep_stats = false;            // keep per-read fetch counts and tiers of the last run
@@ -96,7 +104,7 @@ struct ResultsPriv {
 };
 void results_fill(galn_results *out, int n, const int32_t *n_aln, const int64_t *dev_off, const uint64_t *rec_words,
                   const uint64_t *pops, const uint64_t *trace);
-int run_job(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);
-int run_job_multi(galn_index *ix, const galn_opts *sets, int n_sets, const int32_t *batch_set, const galn_reads *in,
-                  int engine, galn_results *out);
+int run_job(galn_index *ix, ExecCtx &ctx, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);
+int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_sets, const int32_t *batch_set,
+                  const galn_reads *in, int engine, galn_results *out);
 }  // namespace galn

@@ -6,7 +6,8 @@
 // together in one pass of the device tiers, so requests share the same kernels. A request that arrives
 // while a step runs joins the next step; a request leaves as soon as its last read has been searched.
 // Admission is bounded by the step size (the device workspace of one step) and by max_active requests in
-// flight; later requests wait in the queue.
+// flight; later requests wait in the queue. Several steps run at once (n_workers, each with its own stream
+// and device buffers), so the last heavy reads of one step overlap the next step's work on the device.
 //
 // Results do not depend on what else is in a step: each read's options are its request's, and each bwa
 // batch's options come from the longest read of that batch in its own request (batch_max_len), whether the
@@ -32,6 +33,13 @@ double now_ms()
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+struct Chunk {                         // results of reads [r0, r0 + m) of a request
+    int r0 = 0, m = 0;
+    std::vector<int32_t> n_aln;
+    std::vector<galn_aln1> rec;
+    std::vector<uint64_t> pops, trace;
+};
+
 struct Request {
     int64_t id = 0;
     galn_opts opt;
@@ -39,8 +47,9 @@ struct Request {
     std::vector<int64_t> off;
     std::vector<int32_t> batch;        // own bwa batch of each read
     std::vector<int32_t> bmax;         // longest read of each own batch
-    int n = 0, next = 0;
-    // results, in read order
+    int n = 0, next = 0, done_reads = 0;
+    std::vector<Chunk> chunks;         // finished pieces, in any order
+    // results, in read order (assembled when the last piece is done)
     std::vector<int32_t> n_aln;
     std::vector<galn_aln1> rec;
     std::vector<uint64_t> pops, trace;
@@ -64,15 +73,25 @@ struct galn_server {
     size_t max_queued = 1 << 16;
     int max_active = 64;
     int step_reads = 1 << 18;
+    int n_workers = 2;
+    std::vector<galn::ExecCtx *> ctxs;
+    std::vector<std::thread> workers;
     // statistics
     std::vector<double> lat_ms;
     int64_t reads_done = 0, steps = 0;
     double busy_ms = 0;
-    std::thread worker;
 };
 
 static void finish_request(Request *rq)
 {
+    std::sort(rq->chunks.begin(), rq->chunks.end(), [](const Chunk &a, const Chunk &b) { return a.r0 < b.r0; });
+    for (auto &c : rq->chunks) {
+        rq->n_aln.insert(rq->n_aln.end(), c.n_aln.begin(), c.n_aln.end());
+        rq->rec.insert(rq->rec.end(), c.rec.begin(), c.rec.end());
+        rq->pops.insert(rq->pops.end(), c.pops.begin(), c.pops.end());
+        rq->trace.insert(rq->trace.end(), c.trace.begin(), c.trace.end());
+    }
+    std::vector<Chunk>().swap(rq->chunks);
     auto *P = new galn::ResultsPriv();
     P->n_aln.swap(rq->n_aln);
     P->rec.swap(rq->rec);
@@ -97,7 +116,7 @@ static void finish_request(Request *rq)
     std::vector<char>().swap(rq->seq);
 }
 
-static void serve_loop(galn_server *s)
+static void serve_loop(galn_server *s, galn::ExecCtx *ctx)
 {
     struct Piece { Request *rq; int r0, m; };
     std::vector<char> seq;
@@ -108,8 +127,15 @@ static void serve_loop(galn_server *s)
         std::vector<Piece> pieces;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty() || !s->active.empty(); });
-            if (s->stop && s->queue.empty() && s->active.empty()) return;
+            // wait for reads nobody has taken yet (a request may be active with all its reads in flight)
+            auto has_work = [&] {
+                if (!s->queue.empty() && (int)s->active.size() < s->max_active) return true;
+                for (Request *rq : s->active)
+                    if (rq->next < rq->n || (rq->n == 0 && rq->next == 0)) return true;
+                return false;
+            };
+            s->cv_work.wait(lk, [&] { return s->stop || has_work(); });
+            if (s->stop && !has_work()) return;
             while (!s->queue.empty() && (int)s->active.size() < s->max_active) {
                 s->active.push_back(s->queue.front());
                 s->queue.pop_front();
@@ -121,19 +147,26 @@ static void serve_loop(galn_server *s)
             std::vector<int> take(na, 0);
             for (int a = 0; a < na && budget > 0; ++a) {
                 Request *rq = s->active[a];
-                int m = std::min({rq->n - rq->next, share, budget});
+                int m = std::min({std::max(0, rq->n - rq->next), share, budget});
                 take[a] = m;
                 budget -= m;
             }
             for (int a = 0; a < na && budget > 0; ++a) {
                 Request *rq = s->active[a];
-                int m = std::min(rq->n - rq->next - take[a], budget);
+                int m = std::min(std::max(0, rq->n - rq->next - take[a]), budget);
                 take[a] += m;
                 budget -= m;
             }
-            for (int a = 0; a < na; ++a)
-                if (take[a] > 0 || s->active[a]->n == 0) pieces.push_back({s->active[a], s->active[a]->next, take[a]});
+            for (int a = 0; a < na; ++a) {
+                Request *rq = s->active[a];
+                if (take[a] > 0 || (rq->n == 0 && rq->next == 0)) {
+                    pieces.push_back({rq, rq->next, take[a]});
+                    rq->next += take[a];
+                    if (rq->n == 0) rq->next = 1;   // an empty request is taken once
+                }
+            }
         }
+        if (pieces.empty()) continue;
         // one combined job: every request is one option set, every (request, own batch) one batch
         seq.clear(); off.clear(); batch.clear(); bmax.clear(); bset.clear(); sets.clear();
         off.push_back(0);
@@ -167,8 +200,8 @@ static void serve_loop(galn_server *s)
         int rc = 0;
         double t0 = now_ms();
         if (in.n_reads > 0) {
-            std::lock_guard<std::mutex> lk(s->ix->mu);
-            rc = galn::run_job_multi(s->ix, sets.data(), (int)sets.size(), bset.data(), &in, GALN_ENGINE_PERSISTENT, &res);
+            rc = galn::run_job_multi(s->ix, *ctx, sets.data(), (int)sets.size(), bset.data(), &in, GALN_ENGINE_PERSISTENT,
+                                     &res);
         }
         double t1 = now_ms();
         {
@@ -178,18 +211,21 @@ static void serve_loop(galn_server *s)
             int j = 0;
             for (auto &pc : pieces) {
                 Request *rq = pc.rq;
+                Chunk ch;
+                ch.r0 = pc.r0; ch.m = pc.m;
                 for (int t = 0; t < pc.m; ++t, ++j) {
-                    int na = rc ? rq->rc : res.n_aln[j];
-                    rq->n_aln.push_back(rc ? GALN_ERR_STACK : na);
-                    rq->pops.push_back(rc ? 0 : res.n_pops[j]);
-                    rq->trace.push_back(rc ? 0 : res.trace[j]);
+                    int na = rc ? GALN_ERR_STACK : res.n_aln[j];
+                    ch.n_aln.push_back(na);
+                    ch.pops.push_back(rc ? 0 : res.n_pops[j]);
+                    ch.trace.push_back(rc ? 0 : res.trace[j]);
                     if (!rc && na > 0)
-                        rq->rec.insert(rq->rec.end(), res.rec + res.rec_offset[j], res.rec + res.rec_offset[j + 1]);
+                        ch.rec.insert(ch.rec.end(), res.rec + res.rec_offset[j], res.rec + res.rec_offset[j + 1]);
                 }
+                rq->chunks.push_back(std::move(ch));
                 if (rc) rq->rc = rc;
-                rq->next += pc.m;
+                rq->done_reads += pc.m;
                 s->reads_done += pc.m;
-                if (rq->next >= rq->n || rc) {
+                if (rq->done_reads >= rq->n) {
                     finish_request(rq);
                     rq->t_done = now_ms();
                     rq->done = true;
@@ -198,8 +234,9 @@ static void serve_loop(galn_server *s)
                 }
             }
         }
-        if (in.n_reads > 0) galn_results_free(&res);
+        if (in.n_reads > 0 && rc == 0) galn_results_free(&res);
         s->cv_done.notify_all();
+        s->cv_work.notify_all();
     }
 }
 
@@ -213,7 +250,20 @@ extern "C" galn_server *galn_server_start(galn_index *ix, size_t stack_bytes, in
         size_t reads = stack_bytes / (100 * 1024);
         s->step_reads = (int)std::max<size_t>(16384, std::min<size_t>(reads, 1 << 20));
     }
-    s->worker = std::thread(serve_loop, s);
+    if (cudaSetDevice(ix->dev.device) != cudaSuccess) { delete s; if (err) *err = GALN_ECUDA; return nullptr; }
+    for (int w = 0; w < s->n_workers; ++w) {
+        auto *c = new galn::ExecCtx();
+        c->mem_share = 1.0 / s->n_workers;
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            if (err) *err = GALN_ECUDA;
+            for (auto *q : s->ctxs) { cudaStreamDestroy(q->stream); delete q; }
+            delete c;
+            delete s;
+            return nullptr;
+        }
+        s->ctxs.push_back(c);
+    }
+    for (auto *c : s->ctxs) s->workers.emplace_back(serve_loop, s, c);
     if (err) *err = 0;
     return s;
 }
@@ -235,7 +285,13 @@ extern "C" int galn_server_stop(galn_server *s)
         s->stop = true;
     }
     s->cv_work.notify_all();
-    s->worker.join();
+    for (auto &t : s->workers) t.join();
+    cudaSetDevice(s->ix->dev.device);
+    for (auto *c : s->ctxs) {
+        c->ws.release();
+        cudaStreamDestroy(c->stream);
+        delete c;
+    }
     for (auto &kv : s->all) {
         if (kv.second->done) galn_results_free(&kv.second->res);
         delete kv.second;
