@@ -57,15 +57,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def prepare(workload: str, scale: float, rank: int, device: int, data_dir: str | None):
+def prepare(workload: str, scale: float, rank: int, device: int, data_dir: str | None, reads_scale=None):
     """Reference + BWA index (built on this GPU) + this rank's reads, cached on disk."""
     from galn_b200 import index_build, synth
     d = data_dir or os.path.join(tempfile.gettempdir(), f"galn_bench_{workload}_{scale}_r{rank}")
     os.makedirs(d, exist_ok=True)
     t = time.time()
-    ref, reads, opts = synth.workload(workload, scale, seed=1)
+    ref, reads, opts = synth.workload(workload, scale, seed=1, reads_scale=reads_scale)
     if rank:
-        _, reads, _ = synth.workload(workload, scale, seed=1 + 7919 * rank)
+        _, reads, _ = synth.workload(workload, scale, seed=1 + 7919 * rank, reads_scale=reads_scale)
     prefix = os.path.join(d, "ref")
     if not os.path.exists(prefix + ".bwt"):
         index_build.build_from_reference(ref, prefix, device=f"cuda:{device}")
@@ -208,6 +208,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="adna", choices=sorted(WORKLOAD_DESC))
     ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--reads-scale", type=float, default=None, help="reads at this fraction of the workload's")
     ap.add_argument("--engine", default="persistent", choices=["persistent", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-engine comparison")
     ap.add_argument("--cpu-sample", type=int, default=200_000)
@@ -226,7 +227,7 @@ def main():
         if rank != 0:
             return 0
         import torch  # noqa: F401  (index build)
-        d, prefix, ref, reads, opts = prepare(args.workload, args.scale, 0, local, args.data_dir)
+        d, prefix, ref, reads, opts = prepare(args.workload, args.scale, 0, local, args.data_dir, args.reads_scale)
         cb, why = cpu_reference(prefix, reads, opts, args.cpu_sample, d, steps=args.steps, warmup=args.warmup)
         if cb is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
@@ -250,7 +251,7 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    d, prefix, ref, reads, opts = prepare(args.workload, args.scale, rank, local, args.data_dir)
+    d, prefix, ref, reads, opts = prepare(args.workload, args.scale, rank, local, args.data_dir, args.reads_scale)
     n = len(reads)
     # pinned host inputs
     seq_h = torch.empty(len(reads.seq), dtype=torch.uint8, pin_memory=True)
@@ -359,7 +360,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": 1e3 * e2e_s, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int64",
         "data": "synthetic: seeded reference and reads with the workload's shapes (no public dataset here)",
-        "config": {"workload": WORKLOAD_DESC[args.workload], "scale": args.scale, "reads_per_gpu": n,
+        "config": {"workload": WORKLOAD_DESC[args.workload], "scale": args.scale, "reads_scale": args.reads_scale,
+                   "reads_per_gpu": n,
                    "options": " ".join(opts), "engine": args.engine, "trace_hashes": bool(args.trace),
                    "l2": "flushed before every step (512 MB device write, outside the timed region)",
                    "parallelism": f"{world} independent GPU shards (reads split, index replicated)"},

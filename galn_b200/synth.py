@@ -301,26 +301,28 @@ def write_fastq(path: str, reads: Reads) -> None:
 # ---------------------------------------------------------------------------------------------
 # the named workloads
 
-def workload(name: str, scale: float = 1.0, seed: int = 1):
-    """(reference, reads, options) for a named workload at `scale` of its full size."""
+def workload(name: str, scale: float = 1.0, seed: int = 1, reads_scale: float | None = None):
+    """(reference, reads, options) for a named workload at `scale` of its full size (the reads at
+    `reads_scale` of theirs when given)."""
+    rs = scale if reads_scale is None else reads_scale
     if name == "plain_small":
         ref = reference_uniform(max(10_000, int(1_000_000 * scale)), seed)
-        reads = simulate_reads(ref, max(1, int(20_000 * scale)), seed + 1, 100, sub_rate=0.01,
+        reads = simulate_reads(ref, max(1, int(20_000 * rs)), seed + 1, 100, sub_rate=0.01,
                                indel_rate=0.001, random_frac=0.02, prefix="ps")
         return ref, reads, list(DEFAULT_OPTS)
     if name == "adna":
         ref = reference_adna(max(20_000, int(100_000_000 * scale)), seed)
-        reads = simulate_reads(ref, max(1, int(2_000_000 * scale)), seed + 1, adna_lengths, sub_rate=0.005,
+        reads = simulate_reads(ref, max(1, int(2_000_000 * rs)), seed + 1, adna_lengths, sub_rate=0.005,
                                random_frac=0.03, deaminate=0.3, prefix="ad")
         return ref, reads, list(ADNA_OPTS)
     if name == "divergent":
         ref = reference_adna(max(20_000, int(100_000_000 * scale)), seed)
-        reads = simulate_reads(ref, max(1, int(1_000_000 * scale)), seed + 2, 100, sub_rate=0.04,
+        reads = simulate_reads(ref, max(1, int(1_000_000 * rs)), seed + 2, 100, sub_rate=0.04,
                                indel_rate=0.005, prefix="dv")
         return ref, reads, list(DIVERGENT_OPTS)
     if name == "genome":
         ref = reference_genome(max(200_000, int(3_100_000_000 * scale)), seed)
-        reads = simulate_reads(ref, max(1, int(10_000_000 * scale)), seed + 3, 150,
+        reads = simulate_reads(ref, max(1, int(10_000_000 * rs)), seed + 3, 150,
                                sub_rate=lambda x: 0.001 + 0.014 * x, indel_rate=0.0005, prefix="gn")
         return ref, reads, list(DEFAULT_OPTS)
     raise KeyError(name)
