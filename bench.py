@@ -217,6 +217,8 @@ def main():
     ap.add_argument("--t0-cap", type=int, default=1024, help="first-tier stack entries per thread")
     ap.add_argument("--warp-arena", type=int, default=16384, help="warp-tier stack chunks (32 entries) per warp")
     ap.add_argument("--serve-requests", type=int, default=40, help="requests in the serving run (0: none)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false")
+    ap.add_argument("--autotune-sample", type=int, default=262144)
     ap.add_argument("--serve-rate", type=float, default=16.0, help="request arrival rate (per second)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -289,7 +291,11 @@ def main():
                 md5.add(hashlib.md5(res.sai_bytes()).hexdigest())
         return e2e, dev, tier0, launches, md5, res
 
-    # warm-up, then the timed steps bracketed by barriers and synchronisation
+    # the autotuner picks the thread/warp split for these options on a sample (untimed), then warm-up
+    tune = None
+    if args.autotune and engine == galn_b200.GALN_ENGINE_PERSISTENT:
+        tune = ix.autotune(opts, R, max_sample=args.autotune_sample)
+        log(f"[bench] autotuner: {tune}")
     for _ in range(args.warmup):
         galn_b200.aln(ix, opts, R, engine)
     barrier()
@@ -314,7 +320,10 @@ def main():
     total_reads = n * world
 
     # roofline of the dominant kernel: algorithmic block fetches of the reads the first tier finished
-    ix.set_tuning(t0_cap=args.t0_cap, keep_stats=True)
+    if tune:
+        ix.set_tuning(t0_cap=tune["t0_cap"], t0_block=tune["block"], keep_stats=True)
+    else:
+        ix.set_tuning(t0_cap=args.t0_cap, keep_stats=True)
     galn_b200.aln(ix, opts, R, engine)
     prof = ix.last_profile(n)
     tiers_info = {"ms": [round(x, 3) for x in prof["ms_tier"]], "reads": prof["tier_reads"],
@@ -363,6 +372,7 @@ def main():
         "config": {"workload": WORKLOAD_DESC[args.workload], "scale": args.scale, "reads_scale": args.reads_scale,
                    "reads_per_gpu": n,
                    "options": " ".join(opts), "engine": args.engine, "trace_hashes": bool(args.trace),
+                   "autotuned": tune,
                    "l2": "flushed before every step (512 MB device write, outside the timed region)",
                    "parallelism": f"{world} independent GPU shards (reads split, index replicated)"},
         "e2e": {"value": total_reads / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

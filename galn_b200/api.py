@@ -90,6 +90,10 @@ def lib():
     L.galn_aln_wait.argtypes = [vp, C.c_int64, C.c_int, C.POINTER(_Results)]
     L.galn_server_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                     C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    L.galn_autotune.argtypes = [vp, C.POINTER(Options), C.POINTER(_Reads), C.c_int, C.POINTER(C.c_int),
+                                C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.galn_autotune_clear.argtypes = [vp]
+    L.galn_last_graph_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     L.galn_version.restype = C.c_char_p
     _lib = L
     return L
@@ -155,6 +159,16 @@ class Index:
                  "cyc_commit", "cyc_load", "chain_pops"]
         return {k: int(x) for k, x in zip(names, v)}
 
+    def autotune(self, args, reads: "Reads", max_sample: int = 131072) -> dict:
+        """Pick the first-tier stack depth and block size for these options on a sample of `reads`."""
+        opts = args if isinstance(args, Options) else parse_options(list(args))
+        cr, keep = reads.c_struct()
+        cap, blk, ms = C.c_int(), C.c_int(), C.c_double()
+        rc = lib().galn_autotune(self.h, C.byref(opts), C.byref(cr), max_sample, C.byref(cap), C.byref(blk), C.byref(ms))
+        if rc:
+            raise GalnError(f"autotune failed ({rc})")
+        return dict(t0_cap=cap.value, block=blk.value, ms=ms.value)
+
     def set_trace(self, on: bool):
         lib().galn_index_set_trace(self.h, int(on))
 
@@ -182,7 +196,10 @@ class Index:
         t, k, tiers, la = C.c_double(), C.c_double(), C.c_int(), C.c_int64()
         ovf = (C.c_int64 * 8)()
         lib().galn_last_run_stats(self.h, C.byref(t), C.byref(k), C.byref(tiers), C.byref(la), ovf)
-        return dict(ms_total=t.value, ms_kernels=k.value, tiers=tiers.value, launches=la.value, overflow=list(ovf))
+        g = C.c_int64()
+        lib().galn_last_graph_launches(self.h, C.byref(g))
+        return dict(ms_total=t.value, ms_kernels=k.value, tiers=tiers.value, launches=la.value, overflow=list(ovf),
+                    graph_launches=g.value)
 
 
 @dataclass

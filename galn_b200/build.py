@@ -28,7 +28,7 @@ CXXFLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall", "-I" + o
             "-I" + os.path.join(ROOT, "include")]
 
 CU_SOURCES = ["galn_kernels.cu", "galn_noalloc.cu"]
-CPP_SOURCES = ["galn_host.cpp", "galn_engine.cpp", "galn_serve.cpp"]
+CPP_SOURCES = ["galn_host.cpp", "galn_engine.cpp", "galn_serve.cpp", "galn_tune.cpp"]
 
 
 def _headers():

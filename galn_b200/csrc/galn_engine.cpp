@@ -237,12 +237,41 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
         RCK(B.ws.ensure(ws_bytes(cfg, job)));
         S.tier_threads[cfg.tier] = std::max<int64_t>(S.tier_threads[cfg.tier], cfg.threads);
         S.tier_reads[cfg.tier] += m;
-        ECK(cudaMemsetAsync(job.counters, 0, 8, st));
-        ECK(cudaEventRecord(e0, st));
-        RCK(dev_search(ix->dev, job, cfg, list, m, ovf, B.ws.p, st));
-        ECK(cudaEventRecord(e1, st));
-        ECK(cudaMemcpyAsync(h_cnt, job.counters, 8, cudaMemcpyDeviceToHost, st));
-        ECK(cudaStreamSynchronize(st));
+        if (cfg.persistent && cfg.tier == 0 && ix->use_graph) {
+            // the persistent first-tier launch as a CUDA graph: counter reset, timing events, the kernel and the
+            // read-back of the overflow count are captured once and re-instantiated only when the captured
+            // graph cannot update the executable one (e.g. a different kernel instantiation)
+            cudaGraph_t g = nullptr;
+            ECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            cudaMemsetAsync(job.counters, 0, 8, st);
+            cudaEventRecord(e0, st);
+            int lrc = dev_search(ix->dev, job, cfg, list, m, ovf, B.ws.p, st);
+            cudaEventRecord(e1, st);
+            cudaMemcpyAsync(h_cnt, job.counters, 8, cudaMemcpyDeviceToHost, st);
+            cudaError_t ce = cudaStreamEndCapture(st, &g);
+            if (lrc || ce != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return lrc ? lrc : GALN_ECUDA; }
+            bool updated = false;
+            if (ctx.graph_exec) {
+                cudaGraphExecUpdateResultInfo info;
+                updated = cudaGraphExecUpdate(ctx.graph_exec, g, &info) == cudaSuccess;
+                if (!updated) { cudaGetLastError(); cudaGraphExecDestroy(ctx.graph_exec); ctx.graph_exec = nullptr; }
+            }
+            if (!updated) {
+                cudaError_t ie = cudaGraphInstantiate(&ctx.graph_exec, g, 0);
+                if (ie != cudaSuccess) { cudaGraphDestroy(g); ctx.graph_exec = nullptr; return GALN_ECUDA; }
+            }
+            cudaGraphDestroy(g);
+            ECK(cudaGraphLaunch(ctx.graph_exec, st));
+            ECK(cudaStreamSynchronize(st));
+            S.graph_launches += 1;
+        } else {
+            ECK(cudaMemsetAsync(job.counters, 0, 8, st));
+            ECK(cudaEventRecord(e0, st));
+            RCK(dev_search(ix->dev, job, cfg, list, m, ovf, B.ws.p, st));
+            ECK(cudaEventRecord(e1, st));
+            ECK(cudaMemcpyAsync(h_cnt, job.counters, 8, cudaMemcpyDeviceToHost, st));
+            ECK(cudaStreamSynchronize(st));
+        }
         float ms = 0;
         ECK(cudaEventElapsedTime(&ms, e0, e1));
         k_ms += ms;
@@ -259,6 +288,11 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     t0.tier = 0;
     t0.freelist = false; t0.aln_cap = ix->t0_aln; t0.block = ix->t0_block;
     t0.cap = engine == GALN_ENGINE_PLAIN ? ix->plain_t0_cap : ix->t0_cap;
+    if (engine != GALN_ENGINE_PLAIN && !ix->tune_active && !ix->tuned.empty()) {
+        // the autotuner's choice for this option set (single-set jobs; mixed jobs use the first set's)
+        auto it = ix->tuned.find(opts_key(&sets[0]));
+        if (it != ix->tuned.end()) { t0.cap = it->second.first; t0.block = it->second.second; }
+    }
     if (engine == GALN_ENGINE_PERSISTENT) {
         t0.persistent = true;
         RCK(run_tier(t0, cur, n, nxt, &n_ovf));
@@ -482,6 +516,14 @@ extern "C" int galn_last_run_profile(galn_index *ix, double *ms_device, double *
         if (fetch) memcpy(fetch, ix->main.last.fetch.data(), (size_t)n * 4);
         if (tier) memcpy(tier, ix->main.last.tier_of.data(), (size_t)n);
     }
+    return 0;
+}
+
+extern "C" int galn_last_graph_launches(galn_index *ix, int64_t *graph_launches)
+{
+    if (!ix || !graph_launches) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    *graph_launches = ix->main.last.graph_launches;
     return 0;
 }
 

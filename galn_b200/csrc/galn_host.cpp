@@ -327,7 +327,7 @@ extern "C" int galn_index_close(galn_index *ix)
 {
     if (!ix) return GALN_EINVAL;
     cudaSetDevice(ix->dev.device);
-    ix->main.ws.release();
+    ix->main.release();
     dev_index_free(ix->dev);
     if (ix->stream) cudaStreamDestroy(ix->stream);
     delete ix;

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "../../include/galn_aln.h"
@@ -73,6 +75,12 @@ struct ExecCtx {
     JobBufs ws;
     RunStats last;
     double mem_share = 1.0;            // of the budget this context's workspace may take
+    cudaGraphExec_t graph_exec = nullptr;   // the persistent first-tier launch, captured
+    void release()
+    {
+        if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+        ws.release();
+    }
 };
 
 }  // namespace galn
@@ -91,10 +99,14 @@ struct galn_index {
     bool keep_stats = false;            // keep per-read fetch counts and tiers of the last run
     bool trace = true;                  // compute the per-read trace hash (the reference's --verify data)
     bool use_warp = true;               // the warp tier for reads that overflow T0
+    std::map<uint64_t, std::pair<int, int>> tuned;   // option-set key -> (first-tier depth, block), autotuner
+    bool tune_active = false;           // the autotuner is timing a candidate: ignore the table
+    bool use_graph = true;              // launch the persistent first tier through a CUDA graph
     int warp_arena = 1 << 14;           // 32-entry chunks per warp
 };
 
 namespace galn {
+uint64_t opts_key(const galn_opts *o);
 // what galn_results._priv owns
 struct ResultsPriv {
     std::vector<int32_t> n_aln;

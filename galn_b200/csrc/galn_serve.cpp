@@ -288,7 +288,7 @@ extern "C" int galn_server_stop(galn_server *s)
     for (auto &t : s->workers) t.join();
     cudaSetDevice(s->ix->dev.device);
     for (auto *c : s->ctxs) {
-        c->ws.release();
+        c->release();
         cudaStreamDestroy(c->stream);
         delete c;
     }

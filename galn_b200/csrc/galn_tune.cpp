@@ -1,0 +1,79 @@
+// galn_tune.cpp -- the autotuner: per option set, the first tier's stack depth and block size.
+//
+// The first tier's stack depth decides the split between the thread-per-read and the warp-per-read tiers:
+// a read whose search needs more stack than that leaves the thread tier and is searched by a warp. The
+// best depth depends on the options (how many reads backtrack deeply) and on the index (how long
+// exact-match chains run), so it is measured: a sample of the job's reads is searched once per candidate
+// (depth x block size) and the fastest device time wins. Results never depend on the choice; only speed
+// does. The table is keyed by the option block, so every parameter set has its own entry.
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "galn_host_internal.h"
+
+namespace galn {
+
+uint64_t opts_key(const galn_opts *o)
+{
+    // FNV-1a over the option block (n_threads is only a header value and does not change the search)
+    galn_opts c = *o;
+    c.n_threads = 0;
+    const unsigned char *p = (const unsigned char *)&c;
+    uint64_t h = 1469598103934665603ULL;
+    for (size_t i = 0; i < sizeof(c); ++i) h = (h ^ p[i]) * 1099511628211ULL;
+    return h;
+}
+
+}  // namespace galn
+
+using namespace galn;
+
+extern "C" int galn_autotune(galn_index *ix, const galn_opts *o, const galn_reads *in, int max_sample, int *best_cap,
+                             int *best_block, double *best_ms)
+{
+    if (!ix || !o || !in || in->n_reads < 0) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    galn_reads s = *in;
+    if (max_sample > 0 && s.n_reads > max_sample) s.n_reads = max_sample;
+    static const int caps[] = {256, 512, 1024, 2048, 4096};
+    static const int blocks[] = {128, 256};
+    const int saved_cap = ix->t0_cap, saved_block = ix->t0_block;
+    const bool saved_stats = ix->keep_stats;
+    ix->keep_stats = false;
+    int bc = saved_cap, bb = saved_block;
+    double bms = 1e300;
+    int rc = 0;
+    for (int cap : caps)
+        for (int blk : blocks) {
+            ix->t0_cap = cap;
+            ix->t0_block = blk;
+            ix->tune_active = true;
+            galn_results res;
+            memset(&res, 0, sizeof(res));
+            rc = run_job(ix, ix->main, o, &s, GALN_ENGINE_PERSISTENT, &res);
+            ix->tune_active = false;
+            if (rc) break;
+            galn_results_free(&res);
+            double ms = ix->main.last.ms_device;
+            if (ms < bms) { bms = ms; bc = cap; bb = blk; }
+        }
+    ix->t0_cap = saved_cap;
+    ix->t0_block = saved_block;
+    ix->keep_stats = saved_stats;
+    if (rc) return rc;
+    ix->tuned[opts_key(o)] = std::make_pair(bc, bb);
+    if (best_cap) *best_cap = bc;
+    if (best_block) *best_block = bb;
+    if (best_ms) *best_ms = bms;
+    return 0;
+}
+
+extern "C" int galn_autotune_clear(galn_index *ix)
+{
+    if (!ix) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    ix->tuned.clear();
+    return 0;
+}

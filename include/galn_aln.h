@@ -196,6 +196,17 @@ int galn_last_run_stats(galn_index *ix, double *ms_total, double *ms_kernels, in
 int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, int64_t *tier_reads, int64_t *tier_threads,
                           uint32_t *fetch, int8_t *tier, int32_t n);
 
+/* The autotuner (no reference counterpart): times the first max_sample reads (0: all) once per candidate
+ * first-tier stack depth (256..4096 entries: the split between thread-per-read and warp-per-read) and block
+ * size, and keeps the fastest for this option set; later searches with the same options use it. Returns
+ * the choice and its device milliseconds. galn_autotune_clear forgets all choices. */
+int galn_autotune(galn_index *ix, const galn_opts *o, const galn_reads *in, int max_sample, int *best_cap,
+                  int *best_block, double *best_ms);
+int galn_autotune_clear(galn_index *ix);
+
+/* How many of the last run's kernel launches went through a CUDA graph (no reference counterpart). */
+int galn_last_graph_launches(galn_index *ix, int64_t *graph_launches);
+
 /* Counters of the warp tier in the last keep_stats run (no reference counterpart): reads, waves, lanes
  * given entries, lanes replayed, pops, chains continued, hits, SM cycles in chains / replay / commit /
  * wave loads (summed over warps), pops run speculatively. */

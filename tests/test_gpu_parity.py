@@ -171,3 +171,17 @@ def test_empty_and_single_read():
     assert len(res) == 0
     res = galn_b200.aln(ix, [], galn_b200.Reads.from_strings(["ACGTTGCA"]))
     assert len(res) == 1
+
+
+def test_autotune_and_graph_keep_bytes():
+    """The autotuner's choice and the CUDA-graph launch of the first tier change speed only."""
+    ix = galn_b200.Index(os.path.join(GOLDEN, "small", "ref"))
+    meta = CASES["adna"]
+    p = case_paths("adna", meta)
+    reads = galn_b200.read_fastq(p["fq"])
+    tune = ix.autotune(meta["opts"], reads)
+    assert tune["t0_cap"] in (256, 512, 1024, 2048, 4096) and tune["block"] in (128, 256)
+    for _ in range(2):   # the second run updates the instantiated graph
+        res = galn_b200.aln(ix, meta["opts"], reads)
+        assert res.sai_bytes() == open(p["sai"], "rb").read()
+        assert ix.last_stats()["graph_launches"] >= 1
