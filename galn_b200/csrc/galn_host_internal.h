@@ -64,6 +64,7 @@ struct RunStats {
     int64_t tier_threads[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t tier_reads[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t kernel_launches = 0;
+    int64_t graph_launches = 0;      // of those, launched through a CUDA graph
     uint64_t warp_dbg[16] = {};      // warp-tier counters (keep_stats runs)
     std::vector<uint32_t> fetch;     // per read, of the last run
     std::vector<int8_t> tier_of;     // per read, of the last run
