@@ -127,6 +127,8 @@ def lib():
         L.orc_cal_maxdiff.argtypes = [C.c_int, C.c_double, C.c_double]
         L.orc_aln.restype = vp
         L.orc_aln.argtypes = [vp, C.c_char_p, vp, vp, vp, vp, C.c_int, C.c_int]
+        L.orc_aln_bmax.restype = vp
+        L.orc_aln_bmax.argtypes = [vp, C.c_char_p, vp, vp, vp, vp, C.c_int, C.c_int, vp, C.c_int]
         L.orc_result_total.restype = C.c_int64
         L.orc_result_total.argtypes = [vp]
         L.orc_result_dump.argtypes = [vp] + [vp] * 10
@@ -221,7 +223,7 @@ class Result:
             self.h = None
 
 
-def aln(index: Index, opt: bytes, query, off, length, batch, n_threads: int = 0) -> Result:
+def aln(index: Index, opt: bytes, query, off, length, batch, n_threads: int = 0, batch_max_len=None) -> Result:
     n = len(length)
     q = np.ascontiguousarray(query, np.uint8)
     if q.size == 0:
@@ -230,7 +232,11 @@ def aln(index: Index, opt: bytes, query, off, length, batch, n_threads: int = 0)
     ln = np.ascontiguousarray(length, np.int32)
     bt = np.ascontiguousarray(batch, np.int32)
     nt = n_threads or max(1, os.cpu_count() or 1)
-    h = lib().orc_aln(index.h, opt, _ptr(q), _ptr(off), _ptr(ln), _ptr(bt), n, nt)
+    if batch_max_len is None:
+        h = lib().orc_aln(index.h, opt, _ptr(q), _ptr(off), _ptr(ln), _ptr(bt), n, nt)
+    else:
+        bm = np.ascontiguousarray(batch_max_len, np.int32)
+        h = lib().orc_aln_bmax(index.h, opt, _ptr(q), _ptr(off), _ptr(ln), _ptr(bt), n, nt, _ptr(bm), len(bm))
     return Result(h, n)
 
 

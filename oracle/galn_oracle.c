@@ -466,14 +466,16 @@ static void *worker(void *arg)
     return NULL;
 }
 
-void *orc_aln(const void *index, const orc_gap_opt_t *u, const uint8_t *query, const int64_t *off,
-              const int32_t *len, const int32_t *batch, int n, int n_threads)
+void *orc_aln_bmax(const void *index, const orc_gap_opt_t *u, const uint8_t *query, const int64_t *off,
+                   const int32_t *len, const int32_t *batch, int n, int n_threads, const int32_t *bmax, int n_bmax)
 {
     const oindex_t *x = (const oindex_t*)index;
     int nbatch = 0;
     for (int r = 0; r < n; ++r) if (batch[r] + 1 > nbatch) nbatch = batch[r] + 1;
+    if (bmax && n_bmax > nbatch) nbatch = n_bmax;
     int *maxlen = (int*)calloc(nbatch > 0 ? nbatch : 1, sizeof(int));
     for (int r = 0; r < n; ++r) if (len[r] > maxlen[batch[r]]) maxlen[batch[r]] = len[r];
+    if (bmax) for (int b = 0; b < n_bmax; ++b) if (bmax[b] > maxlen[b]) maxlen[b] = bmax[b];
     ropt_t *bopt = (ropt_t*)calloc(nbatch > 0 ? nbatch : 1, sizeof(ropt_t));
     int *bstacks = (int*)calloc(nbatch > 0 ? nbatch : 1, sizeof(int));
     for (int b = 0; b < nbatch; ++b) bstacks[b] = batch_opt(u, maxlen[b], &bopt[b]);
@@ -496,6 +498,12 @@ void *orc_aln(const void *index, const orc_gap_opt_t *u, const uint8_t *query, c
     for (int t = 0; t < n_threads; ++t) pthread_join(tid[t], NULL);
     free(tid); free(maxlen); free(bopt); free(bstacks);
     return R;
+}
+
+void *orc_aln(const void *index, const orc_gap_opt_t *u, const uint8_t *query, const int64_t *off,
+              const int32_t *len, const int32_t *batch, int n, int n_threads)
+{
+    return orc_aln_bmax(index, u, query, off, len, batch, n, n_threads, NULL, 0);
 }
 
 int64_t orc_result_total(const void *p)

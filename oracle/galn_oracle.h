@@ -47,6 +47,9 @@ int   orc_cal_maxdiff(int l, double err, double thres);
 
 void *orc_aln(const void *index, const orc_gap_opt_t *opt, const uint8_t *query, const int64_t *off,
               const int32_t *len, const int32_t *batch, int n_reads, int n_threads);
+/* the same with each batch's longest read given for the whole input (these reads may be a shard of it) */
+void *orc_aln_bmax(const void *index, const orc_gap_opt_t *opt, const uint8_t *query, const int64_t *off,
+                   const int32_t *len, const int32_t *batch, int n_reads, int n_threads, const int32_t *bmax, int n_bmax);
 int64_t orc_result_total(const void *res);
 int   orc_result_dump(const void *res, int32_t *n_aln, uint64_t *pops, uint64_t *trace, int32_t *peak,
                       uint64_t *fetch128, uint64_t *fetch64, int32_t *n_stacks, int32_t *max_diff,
