@@ -244,9 +244,9 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
             cudaGraph_t g = nullptr;
             ECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             cudaMemsetAsync(job.counters, 0, 8, st);
-            cudaEventRecord(e0, st);
+            cudaEventRecordWithFlags(e0, st, cudaEventRecordExternal);   // a timed event node, not a capture join
             int lrc = dev_search(ix->dev, job, cfg, list, m, ovf, B.ws.p, st);
-            cudaEventRecord(e1, st);
+            cudaEventRecordWithFlags(e1, st, cudaEventRecordExternal);
             cudaMemcpyAsync(h_cnt, job.counters, 8, cudaMemcpyDeviceToHost, st);
             cudaError_t ce = cudaStreamEndCapture(st, &g);
             if (lrc || ce != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return lrc ? lrc : GALN_ECUDA; }
