@@ -153,10 +153,10 @@ class Index:
             raise GalnError("bad warp tier setting")
 
     def warp_counters(self) -> dict:
-        v = np.zeros(12, np.uint64)
-        lib().galn_last_warp_counters(self.h, v.ctypes.data, 12)
+        v = np.zeros(14, np.uint64)
+        lib().galn_last_warp_counters(self.h, v.ctypes.data, 14)
         names = ["reads", "waves", "lanes", "consumed", "pops", "continued", "hits", "cyc_chain", "cyc_replay",
-                 "cyc_commit", "cyc_load", "chain_pops"]
+                 "cyc_commit", "cyc_load", "chain_pops", "cyc_read", "cyc_read_max"]
         return {k: int(x) for k, x in zip(names, v)}
 
     def autotune(self, args, reads: "Reads", max_sample: int = 131072) -> dict:

@@ -73,6 +73,34 @@ __device__ __forceinline__ void occ4_one(const IndexView &ix, uint64_t pos, uint
     o[3] = s[3] + cnt.w + __popcll(p0 & p1 & m);
 }
 
+// Occ(c, k1) and Occ(c, l) for all four bases, without a branch around the loads: both blocks are read (the
+// same address twice when k1 and l share a block, which the L1 merges), so threads of a warp that differ in
+// that respect still wait for one round trip together. `fetches` counts the distinct 32-byte blocks (the
+// roofline's unit of algorithmic traffic): one when both positions fall in one block.
+__device__ __forceinline__ void occ4_pair_u(const IndexView &ix, uint64_t k1, uint64_t l, uint64_t ok[4], uint64_t ol[4],
+                                            uint32_t &fetches)
+{
+    const bool kn = k1 == ~0ull, ln = l == ~0ull;   // Occ(., -1) = 0
+    const uint64_t pk = kn ? 0 : k1 - (k1 >= ix.primary);
+    const uint64_t pl = ln ? 0 : l - (l >= ix.primary);
+    const bool same = !kn && !ln && (pk >> 6) == (pl >> 6);
+    fetches += same ? 1u : (uint32_t)(!kn) + (uint32_t)(!ln);
+    const uint4 *bk = ix.blk + ((pk >> 6) << 1), *bl = ix.blk + ((pl >> 6) << 1);
+    const uint4 ck = __ldg(bk), xk = __ldg(bk + 1), cl = __ldg(bl), xl = __ldg(bl + 1);
+    const uint64_t p0k = (uint64_t)xk.x | ((uint64_t)xk.y << 32), p1k = (uint64_t)xk.z | ((uint64_t)xk.w << 32);
+    const uint64_t p0l = (uint64_t)xl.x | ((uint64_t)xl.y << 32), p1l = (uint64_t)xl.z | ((uint64_t)xl.w << 32);
+    const uint64_t mk = kn ? 0 : (2ull << (pk & 63)) - 1, ml = ln ? 0 : (2ull << (pl & 63)) - 1;
+    const uint64_t *sk = ix.sb[pk >> 32], *sl = ix.sb[pl >> 32];
+    ok[0] = kn ? 0 : sk[0] + ck.x + __popcll(~p0k & ~p1k & mk);
+    ok[1] = kn ? 0 : sk[1] + ck.y + __popcll(p0k & ~p1k & mk);
+    ok[2] = kn ? 0 : sk[2] + ck.z + __popcll(~p0k & p1k & mk);
+    ok[3] = kn ? 0 : sk[3] + ck.w + __popcll(p0k & p1k & mk);
+    ol[0] = ln ? 0 : sl[0] + cl.x + __popcll(~p0l & ~p1l & ml);
+    ol[1] = ln ? 0 : sl[1] + cl.y + __popcll(p0l & ~p1l & ml);
+    ol[2] = ln ? 0 : sl[2] + cl.z + __popcll(~p0l & p1l & ml);
+    ol[3] = ln ? 0 : sl[3] + cl.w + __popcll(p0l & p1l & ml);
+}
+
 // Occ(c, k1) and Occ(c, l) for all four bases, one fetch when both fall in one block. `fetches` counts the
 // 32-byte blocks read (the roofline's unit of algorithmic traffic).
 __device__ __forceinline__ void occ4_pair(const IndexView &ix, uint64_t k1, uint64_t l, uint64_t ok[4], uint64_t ol[4],

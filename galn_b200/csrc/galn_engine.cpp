@@ -334,23 +334,44 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
                 h.s_gape > 0) elig.push_back(r);
             else rest.push_back(r);
         }
-        // pass 1 with the tuned arena; pass 2 for its overflow with arenas that hold the max_entries cut-off
+        // longest expected searches first (max_diff, then length), so that the heaviest reads do not start
+        // last and run alone at the end of the launch; results do not depend on the order
+        std::stable_sort(elig.begin(), elig.end(), [&](int32_t x, int32_t y) {
+            if (maxdiff[x] != maxdiff[y]) return maxdiff[x] > maxdiff[y];
+            return in->offset[x + 1] - in->offset[x] > in->offset[y + 1] - in->offset[y];
+        });
+        // pass 1: the tuned arena per warp, plus up to kBigWarps warps whose arenas hold the max_entries
+        // cut-off and take over, in the same launch, the reads that outgrow the small ones; pass 2, only for
+        // reads still queued when pass 1 ended, with big arenas for every warp
         const int aln_cap_w = 4096;
+        const int kBigWarps = 128;
+        const int64_t full = (max_entries_all + 16 + 3 * 32 * 128 + kWarpMaxStacks * 32) / 32 + kWarpMaxStacks + 1;
+        const int big_chunks = (int)std::min<int64_t>(std::max<int64_t>(full, ix->warp_arena), 1 << 22);
         for (int pass = 0; pass < 2 && !elig.empty(); ++pass) {
             int ne = (int)elig.size();
             int res_w = warp_resident(ix->dev.device);
             if (res_w <= 0) return GALN_ECUDA;
-            int nw = std::min(ne, res_w);
-            int arena = ix->warp_arena;
-            if (pass == 1) {
-                nw = std::min(nw, 256);   // few reads get here; keep the big arenas' footprint bounded
-                int64_t full = (max_entries_all + 16 + kWarpMaxStacks * 32) / 32 + 1;
-                arena = (int)std::min<int64_t>(std::max<int64_t>(full, arena), 1 << 22);
+            WarpCfg wc;
+            wc.aln_cap = aln_cap_w;
+            wc.n_warps = std::min(ne, res_w);
+            wc.arena_chunks = ix->warp_arena;
+            wc.big_chunks = big_chunks;
+            if (pass == 0) {
+                wc.n_big = std::min(kBigWarps, wc.n_warps / 8);
+                if (big_chunks <= wc.arena_chunks) wc.n_big = 0;
+                while (wc.n_big > 0 && warp_ws_bytes(wc, ne) > budget) wc.n_big /= 2;
+                while (wc.arena_chunks > 1024 && warp_ws_bytes(wc, ne) > budget) wc.arena_chunks /= 2;
+                while (wc.n_warps > 1 && warp_ws_bytes(wc, ne) > budget) {
+                    wc.n_warps /= 2;
+                    wc.n_big = std::min(wc.n_big, wc.n_warps / 8);
+                }
+            } else {
+                wc.n_warps = std::min(wc.n_warps, 256);   // few reads get here; keep the big arenas' footprint bounded
+                wc.arena_chunks = big_chunks;
+                wc.n_big = 0;
+                while (wc.n_warps > 1 && warp_ws_bytes(wc, ne) > budget) wc.n_warps /= 2;
             }
-            while (nw > 1 && warp_ws_bytes(nw, arena, aln_cap_w) > budget) nw /= 2;
-            if (pass == 0)
-                while (arena > 1024 && warp_ws_bytes(nw, arena, aln_cap_w) > budget) arena /= 2;
-            RCK(B.ws.ensure(warp_ws_bytes(nw, arena, aln_cap_w)));
+            RCK(B.ws.ensure(warp_ws_bytes(wc, ne)));
             ECK(cudaMemcpyAsync(cur, elig.data(), (size_t)ne * 4, cudaMemcpyHostToDevice, st));
             ECK(cudaMemsetAsync(job.counters, 0, 8, st));
             unsigned long long *dbg = nullptr;
@@ -360,30 +381,40 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
                 ECK(cudaMemsetAsync(dbg, 0, kWarpDbg * 8, st));
             }
             ECK(cudaEventRecord(e0, st));
-            RCK(dev_search_warp(ix->dev, job, nw, arena, aln_cap_w, 1, cur, ne, nxt, B.ws.p, st, dbg));
+            RCK(dev_search_warp(ix->dev, job, wc, 1, cur, ne, nxt, B.ws.p, st, dbg));
             ECK(cudaEventRecord(e1, st));
+            int32_t *q_slots = nullptr;
+            int32_t *q_ctl = warp_queue(wc, ne, B.ws.p, &q_slots);
             ECK(cudaMemcpyAsync(h_cnt, job.counters, 8, cudaMemcpyDeviceToHost, st));
+            ECK(cudaMemcpyAsync(h_cnt + 4, q_ctl, 16, cudaMemcpyDeviceToHost, st));
             if (dbg) {
                 unsigned long long hd[kWarpDbg];
                 ECK(cudaMemcpyAsync(hd, dbg, sizeof(hd), cudaMemcpyDeviceToHost, st));
                 ECK(cudaStreamSynchronize(st));
-                for (int q = 0; q < kWarpDbg; ++q) S.warp_dbg[q] += hd[q];
+                for (int q = 0; q < kWarpDbg; ++q)
+                    S.warp_dbg[q] = q == kWarpDbg - 1 ? std::max<uint64_t>(S.warp_dbg[q], hd[q]) : S.warp_dbg[q] + hd[q];
             }
             ECK(cudaStreamSynchronize(st));
             float ms = 0;
             ECK(cudaEventElapsedTime(&ms, e0, e1));
             k_ms += ms;
             S.ms_tier[1] += ms;
-            S.tier_threads[1] = std::max<int64_t>(S.tier_threads[1], (int64_t)nw * 32);
+            S.tier_threads[1] = std::max<int64_t>(S.tier_threads[1], (int64_t)wc.n_warps * 32);
             S.tier_reads[1] += ne;
             S.kernel_launches += 1;
-            int got = h_cnt[1];
-            std::vector<int32_t> wov((size_t)got);
-            if (got) {
-                ECK(cudaMemcpyAsync(wov.data(), nxt, (size_t)got * 4, cudaMemcpyDeviceToHost, st));
-                ECK(cudaStreamSynchronize(st));
-            }
-            if (pass == 1) S.overflow_reads[1] = got;
+            // the reads pass 1 could not finish: its overflow list, then the reads still queued for a big
+            // warp (all queued reads if a queue slot was lost)
+            const int got = h_cnt[1];
+            const int q_head = h_cnt[4], q_tail = h_cnt[5], q_lost = h_cnt[7];
+            const int q_from = q_lost ? 0 : std::min(q_head, q_tail);
+            const int n_q = wc.n_big > 0 ? std::max(0, q_tail - q_from) : 0;
+            std::vector<int32_t> wov((size_t)got + n_q);
+            if (got) ECK(cudaMemcpyAsync(wov.data(), nxt, (size_t)got * 4, cudaMemcpyDeviceToHost, st));
+            if (n_q) ECK(cudaMemcpyAsync(wov.data() + got, q_slots + q_from, (size_t)n_q * 4, cudaMemcpyDeviceToHost, st));
+            if (got || n_q) ECK(cudaStreamSynchronize(st));
+            for (int32_t r : wov)
+                if (r < 0 || r >= n) return GALN_ECUDA;   // a slot written by no warp
+            if (pass == 1) S.overflow_reads[1] = (int64_t)wov.size();
             elig.swap(wov);
         }
         rest.insert(rest.end(), elig.begin(), elig.end());

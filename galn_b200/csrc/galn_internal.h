@@ -85,14 +85,22 @@ int dev_search(const DevIndex &ix, DevJob &job, const TierCfg &cfg, const int32_
 // Occupancy: resident threads per SM for a tier's kernel at the given block size
 int dev_resident_threads(const TierCfg &cfg, bool wide, int device);
 
-// The warp tier: one warp per read over list[0..n), each warp with an arena of arena_chunks 32-entry chunks
-// and aln_cap records; reads it cannot finish go to ovf[]. ws_mem holds warp_ws_bytes(...) bytes.
+// The warp tier: one warp per read over list[0..n). Warps 0..n_big-1 have arenas of big_chunks 32-entry
+// chunks, the others arena_chunks; a read that outgrows a small arena is handed to a big warp in the same
+// launch through a queue in ws_mem. Every warp holds aln_cap records. Reads the launch cannot finish go to
+// ovf[]; reads still queued when it ends are read back through warp_queue(). ws_mem holds
+// warp_ws_bytes(cfg, n) bytes.
 constexpr int kWarpMaxLen = 256, kWarpMaxStacks = 256;
+struct WarpCfg {
+    int n_warps = 0, arena_chunks = 0, aln_cap = 0, n_big = 0, big_chunks = 0;
+};
 size_t warp_smem_bytes();
 int warp_resident(int device);
-size_t warp_ws_bytes(int n_warps, int arena_chunks, int aln_cap);
-constexpr int kWarpDbg = 12;   // counters of the warp tier when profiling is on
-int dev_search_warp(const DevIndex &ix, DevJob &job, int n_warps, int arena_chunks, int aln_cap, int tier,
-                    const int32_t *list, int n, int32_t *ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg);
+size_t warp_ws_bytes(const WarpCfg &c, int n);
+constexpr int kWarpDbg = 14;   // counters of the warp tier when profiling is on
+int dev_search_warp(const DevIndex &ix, DevJob &job, const WarpCfg &c, int tier, const int32_t *list, int n,
+                    int32_t *ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg);
+// the queue in ws_mem: control words (0 head, 1 tail, 2 small warps finished, 3 a slot was lost) and slots
+int32_t *warp_queue(const WarpCfg &c, int n, void *ws_mem, int32_t **slots);
 
 }  // namespace galn

@@ -5,6 +5,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
+
 #include "galn_internal.h"
 #include "galn_search.cuh"
 #include "galn_warp.cuh"
@@ -328,40 +330,69 @@ int warp_resident(int device)
     return bps * sms;
 }
 
-size_t warp_ws_bytes(int n_warps, int arena_chunks, int aln_cap)
+// workspace layout of the warp tier, in order
+struct WarpLayout {
+    size_t chunks, chunk_prev, free_ids, aln, stage, prec, side, q_ctl, ovq, total;
+};
+
+static WarpLayout warp_layout(const WarpCfg &c, int n)
 {
-    size_t w = (size_t)n_warps;
-    return align256(w * arena_chunks * kWCH * 16) + 2 * align256(w * arena_chunks * 4) + align256(w * aln_cap * 24)
-         + align256(w * 3 * 32 * kWL * 16) + align256(w * 32 * kWR * 16);
+    const size_t w = (size_t)c.n_warps;
+    const size_t tot = (size_t)c.n_big * c.big_chunks + (w - (size_t)c.n_big) * c.arena_chunks;
+    WarpLayout L;
+    size_t o = 0;
+    L.chunks = o;     o += align256(tot * kWCH * 16);
+    L.chunk_prev = o; o += align256(tot * 4);
+    L.free_ids = o;   o += align256(tot * 4);
+    L.aln = o;        o += align256(w * c.aln_cap * 24);
+    L.stage = o;      o += align256(w * 3 * 32 * kWL * 16);
+    L.prec = o;       o += align256(w * 32 * kWP * 16);
+    L.side = o;       o += align256(w * sizeof(WSide));
+    L.q_ctl = o;      o += align256(16);
+    L.ovq = o;        o += align256((size_t)std::max(n, 1) * 4);
+    L.total = o;
+    return L;
 }
 
-int dev_search_warp(const DevIndex &ix, DevJob &job, int n_warps, int arena_chunks, int aln_cap, int tier,
-                    const int32_t *list, int n, int32_t *ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg)
+size_t warp_ws_bytes(const WarpCfg &c, int n) { return warp_layout(c, n).total; }
+
+int32_t *warp_queue(const WarpCfg &c, int n, void *ws_mem, int32_t **slots)
+{
+    const WarpLayout L = warp_layout(c, n);
+    *slots = (int32_t *)((char *)ws_mem + L.ovq);
+    return (int32_t *)((char *)ws_mem + L.q_ctl);
+}
+
+int dev_search_warp(const DevIndex &ix, DevJob &job, const WarpCfg &c, int tier, const int32_t *list, int n,
+                    int32_t *ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg)
 {
     if (n == 0) return 0;
+    if (c.n_big < 0 || c.n_big > c.n_warps || (c.n_big > 0 && c.big_chunks < 1) || c.arena_chunks < 1) return -20;   // GALN_EINVAL
     WArgs a;
     memset(&a, 0, sizeof(a));
     a.ix.blk = (const uint4 *)ix.blocks;
     a.ix.primary = ix.primary;
     a.ix.seq_len = ix.seq_len;
-    for (int c = 0; c < 4; ++c) a.ix.C[c] = ix.L2[c];
+    for (int q = 0; q < 4; ++q) a.ix.C[q] = ix.L2[q];
     memcpy(a.ix.sb, ix.sb, sizeof(a.ix.sb));
     a.query = job.query; a.off = job.off; a.bidx = job.bidx; a.maxdiff = job.maxdiff;
     a.bopt = (const BatchOpt *)job.bopt; a.seed_len = job.seed_len;
-    a.list = list; a.n = n; a.claim = job.counters; a.n_warps = n_warps;
-    size_t w = (size_t)n_warps;
+    a.list = list; a.n = n; a.claim = job.counters; a.n_warps = c.n_warps;
+    const WarpLayout L = warp_layout(c, n);
     char *base = (char *)ws_mem;
-    a.chunks = (uint4 *)base;
-    base += align256(w * arena_chunks * kWCH * 16);
-    a.chunk_prev = (int32_t *)base;
-    base += align256(w * arena_chunks * 4);
-    a.free_ids = (int32_t *)base;
-    base += align256(w * arena_chunks * 4);
-    a.aln = (uint64_t *)base;
-    base += align256(w * aln_cap * 24);
-    a.stage = (uint4 *)base;
-    base += align256(w * 3 * 32 * kWL * 16);
-    a.prec = (uint4 *)base;
+    a.chunks = (uint4 *)(base + L.chunks);
+    a.chunk_prev = (int32_t *)(base + L.chunk_prev);
+    a.free_ids = (int32_t *)(base + L.free_ids);
+    a.aln = (uint64_t *)(base + L.aln);
+    a.stage = (uint4 *)(base + L.stage);
+    a.prec = (uint4 *)(base + L.prec);
+    a.side = (WSide *)(base + L.side);
+    a.q_ctl = (int32_t *)(base + L.q_ctl);
+    a.ovq = (int32_t *)(base + L.ovq);
+    a.n_big = c.n_big; a.big_chunks = c.big_chunks;
+    GALN_CUDA(cudaMemsetAsync(a.q_ctl, 0, 16, st));
+    GALN_CUDA(cudaMemsetAsync(a.ovq, 0xff, (size_t)n * 4, st));
+    const int arena_chunks = c.arena_chunks, aln_cap = c.aln_cap, n_warps = c.n_warps;
     a.arena_chunks = arena_chunks; a.aln_cap = aln_cap;
     a.out_n = job.out_n; a.out_off = job.out_off; a.out_pops = job.out_pops; a.out_trace = job.out_trace;
     a.out_peak = job.out_peak; a.out_fetch = job.out_fetch; a.out_tier = job.out_tier; a.tier = tier;

@@ -1,4 +1,4 @@
-// galn_warp.cuh -- the heavy-read tier: one warp per read, up to 32 stack entries expanded at once.
+// galn_warp.cuh -- the heavy-read tier: one warp per read, many stack entries expanded at once.
 //
 // Why this is exact. With positive penalties (s_mm, s_gapo, s_gape > 0) every child of an entry popped from
 // score bucket b goes to a bucket above b, except the exact-match child, which has score b and is pushed
@@ -6,23 +6,30 @@
 // entry while it is being popped: its pops are the entries e_m, e_{m-1}, ..., e_1 (LIFO), each followed
 // by its chain of exact-match children. Between two hits the expansion of a chain depends only on its
 // first entry, the width arrays and max_diff, none of which change without a hit; so the chains of the
-// top W <= 32 entries of bucket b can be expanded at the same time, one per lane.
+// top entries of bucket b can be expanded at the same time, in any order and on any lane.
 //
-// One wave: lane j takes the j-th entry from the top of bucket b (lane 0 takes a pending exact child left
-// by the previous wave), runs its chain for up to kWR pops, staging the pushes of each pop (in the order
-// bwt_match_gap pushes them) in global memory, one list per distinct target bucket (b+s_mm, b+s_gapo,
-// b+s_gape), with 4 bytes of per-pop data in shared memory, and stopping at a hit (a "hazard"). Then the warp replays the
-// lanes in order exactly as the sequential search would pop them: the max_entries test before each pop,
-// n_entries after each pop and push, the pop count, the trace hash, the first hit (handled sequentially:
-// best_score, max_diff, -R, gapped-hit de-duplication, gap_shadow, the record). Replay stops at a hit or at a
-// lane whose chain is not finished; later lanes' speculation is discarded and their entries stay on the stack.
-// The pushes of the replayed pops are committed to their buckets in replay order (per bucket: lane order,
-// then pop order), so every bucket is the same LIFO as in the sequential search.
+// One wave takes up to kWE entries from the top of bucket b (entry 0 may be a pending exact child left by
+// the previous wave). The warp runs in steps: in each step every busy lane expands one pop of its chain,
+// and every idle lane takes the next entry not yet handed out (in entry order), so lanes stay busy however
+// uneven the chains are. A lane stages the pushes of each pop (in the order bwt_match_gap pushes them) in
+// global memory, one list per distinct target bucket (b+s_mm, b+s_gapo, b+s_gape), and 2 bytes of per-pop
+// data in shared memory; when a chain ends it writes the entry's record (its lane, pops, staged segments
+// and prefix sums). A chain that reaches a hit, a score past n_stacks, or the end of its lane's space
+// (a "stop") ends the hand-out after its entry; entries past it are dropped.
+//
+// Then the warp replays the entries in order exactly as the sequential search would pop them: the
+// max_entries test before each pop, n_entries after each pop and push, the pop count, the trace hash, the
+// first hit (handled sequentially: best_score, max_diff, -R, gapped-hit de-duplication, gap_shadow, the
+// record). Without the trace hash the entries before the first stop are replayed at once from prefix
+// sums; that entry (and, in trace mode, every entry) one pop at a time. The pushes of the replayed entries
+// are committed to their buckets in replay order (per bucket: entry order, then pop order), so every
+// bucket is the same LIFO as in the sequential search.
 //
 // Storage: each bucket is a chain of 32-entry chunks in the warp's arena (global memory), with its top
-// chunk, fill and entry count in shared memory. Widths, the query and the per-pop data are in shared
-// memory; staged pushes (and, in trace mode, popped entries) in a per-warp global staging area. Reads the tier cannot take (length > 256, n_stacks > 256, a penalty <= 0, 32-byte entries) or
-// that outgrow the arena or the record buffer go to the thread tiers (the host routes them).
+// chunk, fill and entry count in shared memory. Widths, the query, the wave's entries and records and the
+// per-pop data are in shared memory; staged pushes (and, in trace mode, popped entries) in a per-warp
+// global staging area. Reads the tier cannot take (length > 256, n_stacks > 256, a penalty <= 0, 32-byte
+// entries) or that outgrow the arena or the record buffer go to the thread tiers (the host routes them).
 #pragma once
 
 #include "galn_search.cuh"
@@ -31,10 +38,14 @@ namespace galn {
 
 constexpr int kWMaxB = 256;      // buckets
 constexpr int kWMaxLen = 256;    // read length
-constexpr int kWR = 32;          // pops per lane per wave
+constexpr int kWE = 128;         // entries per wave
+constexpr int kWP = 48;          // pops per lane per wave
 constexpr int kWL = 128;         // staged pushes per lane and target list per wave
 constexpr int kWCH = 32;         // entries per chunk
 constexpr int kWNewC = (kWCH + 32 * kWL) / kWCH + 2;   // chunks one commit may allocate
+constexpr int kWGrabPops = 6;    // an idle lane takes an entry only with room for this many pops
+
+constexpr int kWDbgN = 14;       // optional counters per read (the kDbg* list below)
 
 struct WarpSmem {
     int32_t top_chunk[kWMaxB];
@@ -44,16 +55,27 @@ struct WarpSmem {
     uint64_t W[kWMaxLen + 1];
     uint64_t SW[kWMaxLen + 1];
     uint8_t q[kWMaxLen];
-    // per pop of each lane: pushes (bits 0-7, the fused exact child not counted), has an exact child
-    // (bit 8), index blocks read (bits 16-31)
-    uint32_t meta[32][kWR + 1];       // one word of padding per row: lanes writing the same pop hit distinct banks
-    uint4 hz[32];                     // hazard entry of each lane
-    uint64_t hk[32], hl[32];          // its interval after the exact tail
-    int32_t lane_np[32], lane_end[32];
-    uint32_t lane_nl[32][3];          // staged pushes of each lane per target list
-    uint4 lane_x[32];                 // pending exact child of a lane that stopped mid-chain
+    uint4 ent[kWE];                   // the wave's entries, in pop order
+    uint32_t e_info[kWE];             // per entry: lane (bits 0-7), first pop (8-15), pops (16-23), end code (24-31)
+    uint32_t e_seg[3][kWE];           // per entry and list: first staged push (bits 0-15), count (16-31)
+    uint32_t e_a[kWE];                // per entry: net change of n_entries (signed, bits 0-15), its highest value before a pop (16-31)
+    uint32_t e_b[kWE];                // per entry: highest value after a pop (bits 0-15), index blocks read (16-31)
     int32_t newc[kWNewC];             // chunks allocated for one commit
-    int32_t incl[32];                 // inclusive scan of the lanes' counts in one commit
+    int32_t wch[kWE / kWCH + 2];      // chunks of bucket b holding the wave's entries, top first
+    BatchOpt O;                       // the read's batch options (read from here, not held in registers)
+    unsigned long long dv[kWDbgN];    // optional counters of this read (profiling runs)
+    long long t_mark, t_read;
+};
+
+// Per-warp data that is written often but read rarely (at hits, pending children and the one entry a wave
+// replays pop by pop), kept in global memory to leave shared memory for more resident warps.
+struct WSide {
+    uint4 hz[32];                     // hazard entry of each lane
+    uint4 lane_x[32];                 // pending exact child of a lane that stopped mid-chain
+    uint64_t hk[32], hl[32];          // the hazard's interval after the exact tail
+    // per pop of each lane: pushes (bits 0-3, the fused exact child not counted), has an exact child
+    // (bit 4), index blocks read (bits 5-15)
+    uint16_t meta[32][kWP];
 };
 
 struct WArgs {
@@ -75,7 +97,8 @@ struct WArgs {
     uint64_t *aln;            // n_warps * aln_cap * 3
     int aln_cap;
     uint4 *stage;             // n_warps * 3 lists * 32 lanes * kWL staged pushes
-    uint4 *prec;              // n_warps * 32 lanes * kWR popped entries (trace mode)
+    uint4 *prec;              // n_warps * 32 lanes * kWP popped entries (trace mode)
+    WSide *side;              // n_warps
     int32_t *out_n;
     int64_t *out_off;
     uint64_t *out_pops, *out_trace;
@@ -88,12 +111,24 @@ struct WArgs {
     int64_t rec_cap;
     int32_t *ovf;
     int32_t *ovf_n;
+    // Warps 0..n_big-1 have arenas of big_chunks chunks (room for the max_entries cut-off); the others
+    // arena_chunks. A read that outgrows a small arena is queued in ovq (its tail at q_ctl[1]) for the big
+    // warps, which take queued reads before new ones (q_ctl: 0 head, 1 tail, 2 small warps finished,
+    // 3 set when a big warp gave up waiting; the host then re-runs every queued read).
+    int n_big, big_chunks;
+    int32_t *ovq;
+    int32_t *q_ctl;
     unsigned long long *dbg;  // optional counters (kWDbg entries), or NULL
 };
 
 // optional counters of the warp tier (per launch, summed over warps)
 enum { kDbgReads, kDbgWaves, kDbgLanes, kDbgConsumed, kDbgPops, kDbgCont, kDbgHazard, kDbgCycChain,
-       kDbgCycReplay, kDbgCycCommit, kDbgCycLoad, kDbgChainPops, kWDbg };
+       kDbgCycReplay, kDbgCycCommit, kDbgCycLoad, kDbgChainPops, kDbgCycRead, kDbgCycReadMax, kWDbg };
+static_assert(kWDbg == kWDbgN, "counter list");
+
+// profiling helpers: lane 0 keeps the read's counters in shared memory
+#define WDBG_ADD(K, V) do { if (dbg && lane == 0) S->dv[K] += (unsigned long long)(V); } while (0)
+#define WDBG_LAP(K) do { if (dbg && lane == 0) { long long t_ = clock64(); S->dv[K] += (unsigned long long)(t_ - S->t_mark); S->t_mark = t_; } } while (0)
 
 // an entry in registers (the score is the bucket of the wave)
 struct WEnt {
@@ -140,61 +175,86 @@ struct WCtx {
     bool gape, nonstop;
 };
 
-// one lane's chain: end code 0 = finished, 1 = hazard (a hit) at its last pop, 2 = stopped with x pending,
-// 3 = its last pop pushes a score >= n_stacks (bwt_match_gap returns BWTGAP_ERR_SCORE there).
-// st: this lane's three staging lists (kWL apart, 32 * kWL between lists); tl: list of each push kind
-// (mismatch, gap open, gap extension); pr: this lane's popped-entry records (trace mode)
+// The exact walk of a pop with no difference left (bwt_match_exact_alt, src/bwtgap_hd.h:195-211), kept
+// across steps: one LF step per warp step, so that it shares the step's single index fetch with the other
+// lanes' pops instead of stalling the warp for its whole length.
+struct WWalk {
+    uint64_t k, l;
+    int i;                 // bases left to match (positions i-1 .. 0)
+    uint32_t f;            // index blocks read by the walk so far
+    bool on;
+};
+
+// One step of a lane's chain: a pop, or one LF step of a pop's exact walk. Returns the chain's end code:
+// -2 = the pop's exact walk goes on (no pop finished), -1 = the pop finished and the chain continues with
+// its exact child (now in x), 0 = the chain is finished, 1 = hazard (a hit) at this pop, 2 = stopped with
+// the exact child pending (no room left in this wave; the child is in D->lane_x), 3 = this pop pushes a
+// score >= n_stacks (bwt_match_gap returns BWTGAP_ERR_SCORE there). A finished pop's data goes to
+// D->meta[lane][lp] (and to mt); its pushes are appended to this lane's staging lists (st: list L at
+// st + L * 32 * kWL; tl: list of each push kind, mismatch, gap open, gap extension); in trace mode the popped
+// entry goes to pr[lp].
 template <bool TRACE>
-__device__ __forceinline__ void lane_chain(const IndexView &ix, const BatchOpt &O, const WCtx &c, WarpSmem *S, int lane,
-                                           WEnt x, int b, uint32_t &fetches, uint4 *st, const int tl[3], uint4 *pr)
+__device__ __forceinline__ int lane_step(const IndexView &ix, const BatchOpt &O, const WCtx &c, WarpSmem *S, WSide *D,
+                                         int lane, WEnt &x, WWalk &wk, int b, uint32_t &fetches, uint4 *st, const int tl[3],
+                                         uint4 *pr, int &lp, int &nl0, int &nl1, int &nl2, uint32_t &mt)
 {
-    int np = 0, endc = 0;
-    int nl0 = 0, nl1 = 0, nl2 = 0;
     const size_t lstride = (size_t)32 * kWL;
-    // a push of the given kind (0 mismatch, 1 gap open, 2 gap extension); a score at or past n_stacks ends
-    // the read
-#define WPUSH(KIND, BKT, ...)                                                           \
-    do {                                                                                \
-        int bk_ = (BKT);                                                                \
-        if (bk_ >= O.n_stacks) { err = true; break; }                                   \
-        int L_ = tl[KIND];                                                              \
-        int &n_ = L_ == 0 ? nl0 : (L_ == 1 ? nl1 : nl2);                                \
-        st[L_ * lstride + n_] = wpack_child(__VA_ARGS__);                               \
-        ++n_;                                                                           \
-        ++npu;                                                                          \
-    } while (0)
-    for (;;) {
-        bool err = false;
-        const uint32_t f_pop = fetches;
-        if (TRACE) pr[np] = wpack(x);
-        int diffs = x.n_mm + x.n_gapo + (c.gape ? x.n_gape : 0);
-        int m = c.max_diff - diffs;
-        int i = x.i;
-        uint32_t npu = 0, hx = 0;
+    bool err = false;
+    uint32_t npu = 0;
+    int endc = -2;
+    bool load = false;           // this step reads Occ at (k1, l1)
+    uint64_t k1 = 0, l1 = 0;
+    int diffs = 0, m = 0, i = x.i;
+    // ---- before the fetch: the tests that need no index data ----
+    if (wk.on) {
+        if (S->q[wk.i - 1] > 3) { wk.on = false; mt = wk.f << 5; endc = 0; }
+        else { load = true; k1 = wk.k - 1; l1 = wk.l; }
+    } else {
+        if (TRACE) pr[lp] = wpack(x);
+        diffs = x.n_mm + x.n_gapo + (c.gape ? x.n_gape : 0);
+        m = c.max_diff - diffs;
         if (m < 0 || (i > 0 && m < (int)(S->W[i - 1] >> 48))) {
-            S->meta[lane][np] = 0; ++np; endc = 0; break;
+            mt = 0; endc = 0;
+        } else if (i == 0) {
+            D->hz[lane] = wpack(x); D->hk[lane] = x.k; D->hl[lane] = x.l;
+            mt = 0; endc = 1;
+        } else if (m == 0 && (x.state == kStM || c.gape || x.n_gape == O.max_gape)) {
+            // bwt_match_exact_alt over positions i-1 .. 0
+            if (S->q[i - 1] > 3) { mt = 0; endc = 0; }
+            else { wk.on = true; wk.k = x.k; wk.l = x.l; wk.i = i; wk.f = 0; load = true; k1 = x.k - 1; l1 = x.l; }
+        } else {
+            load = true; k1 = x.k - 1; l1 = x.l;
         }
-        if (i == 0) {
-            S->hz[lane] = wpack(x); S->hk[lane] = x.k; S->hl[lane] = x.l;
-            S->meta[lane][np] = 0; ++np; endc = 1; break;
-        }
-        if (m == 0 && (x.state == kStM || c.gape || x.n_gape == O.max_gape)) {
-            uint64_t k = x.k, l = x.l;
-            if (match_exact_alt(ix, i, S->q, k, l, fetches)) {
-                S->hz[lane] = wpack(x); S->hk[lane] = k; S->hl[lane] = l; endc = 1;
-            } else endc = 0;
-            S->meta[lane][np] = (fetches - f_pop) << 16;
-            ++np;
-            break;
-        }
+    }
+    // ---- the step's one fetch ----
+    uint64_t ck[4], cl[4];
+    uint32_t df = 0;
+    if (load) {
+        const uint32_t f0 = fetches;
+        occ4_pair_u(ix, k1, l1, ck, cl, fetches);
+        df = fetches - f0;
+    }
+    if (load && wk.on) {
+        // one LF step of the exact walk
+        const int cc = S->q[wk.i - 1];
+        const uint64_t kk = ix.C[cc] + sel4(cc, ck[0], ck[1], ck[2], ck[3]) + 1;
+        const uint64_t ll = ix.C[cc] + sel4(cc, cl[0], cl[1], cl[2], cl[3]);
+        wk.f += df;
+        if (kk > ll) { wk.on = false; mt = wk.f << 5; endc = 0; }
+        else if (--wk.i == 0) {
+            wk.on = false;
+            D->hz[lane] = wpack(x); D->hk[lane] = kk; D->hl[lane] = ll;
+            mt = wk.f << 5; endc = 1;
+        } else { wk.k = kk; wk.l = ll; }
+    } else if (load) {
+        // the expansion of the pop (src/bwtgap_hd.h:396-470) as nine predicated push slots in the order
+        // bwt_match_gap pushes them: the gap child that keeps the interval (insertion open or extension), the
+        // four deletion children (open or extension), the mismatches; then the exact child
         --i;
-        uint64_t ck[4], cl[4];
-        occ4_pair(ix, x.k - 1, x.l, ck, cl, fetches);
-        const uint64_t kk0 = ix.C[0] + ck[0] + 1, ll0 = ix.C[0] + cl[0];
-        const uint64_t kk1 = ix.C[1] + ck[1] + 1, ll1 = ix.C[1] + cl[1];
-        const uint64_t kk2 = ix.C[2] + ck[2] + 1, ll2 = ix.C[2] + cl[2];
-        const uint64_t kk3 = ix.C[3] + ck[3] + 1, ll3 = ix.C[3] + cl[3];
-        uint64_t occ = x.l - x.k + 1;
+        uint64_t kk[4], ll[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { kk[q] = ix.C[q] + ck[q] + 1; ll[q] = ix.C[q] + cl[q]; }
+        const uint64_t occ = x.l - x.k + 1;
         int allow_diff = 1, allow_M = 1;
         if (i > 0) {
             uint64_t wa = S->W[i - 1], wb = S->W[i];
@@ -210,70 +270,86 @@ __device__ __forceinline__ void lane_chain(const IndexView &ix, const BatchOpt &
                 else if (sba == m_seed - 1 && sbb == m_seed - 1 && (sa & kW48) == (sb & kW48)) allow_M = 0;
             }
         }
-        int gaps = x.n_gapo + x.n_gape;
-        int tmp = (O.mode & kModeLoggap) ? (gaps ? (31 - __clz(gaps)) : 0) / 2 + 1 : gaps;
-        if (allow_diff && i >= O.indel_end_skip + tmp && c.len - i >= O.indel_end_skip + tmp) {
-            if (x.state == kStM) {
-                if (x.n_gapo < O.max_gapo) {
-                    WPUSH(1, b + O.s_gapo, x.k, x.l, i, x.n_mm, x.n_gapo + 1, x.n_gape, x.n_ins + 1, kStI, 1);
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        uint64_t kk = sel4(cc, kk0, kk1, kk2, kk3), ll = sel4(cc, ll0, ll1, ll2, ll3);
-                        if (!err && kk <= ll)
-                            WPUSH(1, b + O.s_gapo, kk, ll, i + 1, x.n_mm, x.n_gapo + 1, x.n_gape, x.n_ins, kStD, 1);
-                    }
-                }
-            } else if (x.state == kStI) {
-                if (x.n_gape < O.max_gape)
-                    WPUSH(2, b + O.s_gape, x.k, x.l, i, x.n_mm, x.n_gapo, x.n_gape + 1, x.n_ins + 1, kStI, 1);
-            } else if (x.state == kStD) {
-                if (x.n_gape < O.max_gape && (gaps < c.max_diff || occ < (uint64_t)(int64_t)O.max_del_occ)) {
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        uint64_t kk = sel4(cc, kk0, kk1, kk2, kk3), ll = sel4(cc, ll0, ll1, ll2, ll3);
-                        if (!err && kk <= ll)
-                            WPUSH(2, b + O.s_gape, kk, ll, i + 1, x.n_mm, x.n_gapo, x.n_gape + 1, x.n_ins, kStD, 1);
-                    }
-                }
-            }
-        }
+        const int gaps = x.n_gapo + x.n_gape;
+        const int tmp = (O.mode & kModeLoggap) ? (gaps ? (31 - __clz(gaps)) : 0) / 2 + 1 : gaps;
+        const bool indel = allow_diff && i >= O.indel_end_skip + tmp && c.len - i >= O.indel_end_skip + tmp;
+        const bool st_m = x.state == kStM, st_i = x.state == kStI;
+        const bool open_ok = indel && st_m && x.n_gapo < O.max_gapo;
+        const bool ext_i = indel && st_i && x.n_gape < O.max_gape;
+        const bool ext_d = indel && x.state == kStD && x.n_gape < O.max_gape
+                           && (gaps < c.max_diff || occ < (uint64_t)(int64_t)O.max_del_occ);
+        const bool self_ok = open_ok || ext_i;          // insertion: open from M, extension from I
+        const bool del_ok = open_ok || ext_d;           // deletions: open from M, extension from D
+        const bool mm_ok = allow_diff && allow_M;
+        // list and bucket of each slot kind (a gap open from M, an extension otherwise)
+        const int g_list = st_m ? tl[1] : tl[2];
+        const int g_bkt = b + (st_m ? O.s_gapo : O.s_gape);
+        const int m_bkt = b + O.s_mm;
+        // the packed words of each slot kind, but for k and l
+        const uint64_t gap1 = st_m ? (1ull << 38) : (1ull << 45);    // n_gapo + 1 or n_gape + 1
+        const uint64_t w1b = ((uint64_t)(x.n_gapo & 127) << 38) | ((uint64_t)(x.n_gape & 127) << 45)
+                           | ((uint64_t)(x.n_ins & 255) << 52);
+        const uint64_t w0b = ((uint64_t)(x.n_mm & 127) << 54) | (1ull << 63);
+        const uint64_t h0_self = w0b | ((uint64_t)(uint32_t)i << 38) | ((uint64_t)kStI << 61);
+        const uint64_t h1_self = w1b + gap1 + (1ull << 52);
+        const uint64_t h0_del = w0b | ((uint64_t)(uint32_t)(i + 1) << 38) | ((uint64_t)kStD << 61);
+        const uint64_t h1_del = w1b + gap1;
+        const uint64_t h0_mm = (w0b + (1ull << 54)) | ((uint64_t)(uint32_t)i << 38) | ((uint64_t)kStM << 61);
         const int base = S->q[i];
-        bool exact = false;
-        uint64_t ek = 0, el = 0;
-        if (err) {
-        } else if (allow_diff && allow_M) {
+        // which slots push: bit 0 the kept-interval gap child, bits 1-4 deletions by base, bits 5-8 mismatches
+        uint32_t slots = self_ok ? 1u : 0u;
 #pragma unroll
-            for (int j = 1; j <= 4; ++j) {
-                int cc = (base + j) & 3;
-                int mm = j != 4 || base > 3;
-                uint64_t kk = sel4(cc, kk0, kk1, kk2, kk3), ll = sel4(cc, ll0, ll1, ll2, ll3);
-                if (!err && kk <= ll) {
-                    if (!mm) { exact = true; ek = kk; el = ll; }
-                    else WPUSH(0, b + O.s_mm, kk, ll, i, x.n_mm + 1, x.n_gapo, x.n_gape, x.n_ins, kStM, 1);
+        for (int q = 0; q < 4; ++q) if (del_ok && kk[q] <= ll[q]) slots |= 2u << q;
+#pragma unroll
+        for (int j = 1; j <= 4; ++j) {
+            const int q = (base + j) & 3;
+            const bool mm = j != 4 || base > 3;
+            if (mm_ok && mm && sel4(q, kk[0], kk[1], kk[2], kk[3]) <= sel4(q, ll[0], ll[1], ll[2], ll[3])) slots |= 32u << (j - 1);
+        }
+        // a push at or past n_stacks ends the read (BWTGAP_ERR_SCORE); nothing else of this pop matters then
+        err = ((slots & 0x1fu) && g_bkt >= O.n_stacks) || ((slots & 0x1e0u) && m_bkt >= O.n_stacks);
+        if (!err) {
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                if (!(slots & (1u << t))) continue;
+                uint64_t w0, w1;
+                int L;
+                if (t == 0) { w0 = (x.k & kK38) | h0_self; w1 = (x.l & kK38) | h1_self; L = g_list; }
+                else if (t <= 4) {
+                    w0 = (kk[t - 1] & kK38) | h0_del; w1 = (ll[t - 1] & kK38) | h1_del; L = g_list;
+                } else {
+                    const int q = (base + t - 4) & 3;
+                    w0 = (sel4(q, kk[0], kk[1], kk[2], kk[3]) & kK38) | h0_mm;
+                    w1 = (sel4(q, ll[0], ll[1], ll[2], ll[3]) & kK38) | w1b;
+                    L = tl[0];
                 }
+                const int n_ = L == 0 ? nl0 : (L == 1 ? nl1 : nl2);
+                st[L * lstride + n_] = make_uint4((uint32_t)w0, (uint32_t)(w0 >> 32), (uint32_t)w1, (uint32_t)(w1 >> 32));
+                nl0 += L == 0; nl1 += L == 1; nl2 += L == 2;
+                ++npu;
             }
-        } else if (base < 4) {
-            uint64_t kk = sel4(base, kk0, kk1, kk2, kk3), ll = sel4(base, ll0, ll1, ll2, ll3);
-            if (kk <= ll) { exact = true; ek = kk; el = ll; }
         }
-        const uint32_t fpop = (fetches - f_pop) << 16;
+        const bool exact = !err && base < 4 && sel4(base, kk[0], kk[1], kk[2], kk[3]) <= sel4(base, ll[0], ll[1], ll[2], ll[3]);
         if (err) {   // the read ends at this pop with BWTGAP_ERR_SCORE
-            S->meta[lane][np] = fpop; ++np; endc = 3; break;
+            mt = df << 5; endc = 3;
+        } else {
+            mt = npu | (exact ? 16u : 0u) | df << 5;
+            endc = exact ? -1 : 0;
+            if (exact) {
+                x.k = sel4(base, kk[0], kk[1], kk[2], kk[3]); x.l = sel4(base, ll[0], ll[1], ll[2], ll[3]);
+                x.i = i; x.isdiff = 0; x.state = kStM;
+            }
         }
-        if (exact) hx = 1;
-        S->meta[lane][np] = npu | (hx << 8) | fpop;
-        ++np;
-        if (!exact) { endc = 0; break; }
-        x.k = ek; x.l = el; x.i = i; x.isdiff = 0; x.state = kStM;
-        // room for one more pop: at most 9 pushes, all possibly in one list
-        if (np == kWR || nl0 + 9 > kWL || nl1 + 9 > kWL || nl2 + 9 > kWL) { endc = 2; S->lane_x[lane] = wpack(x); break; }
     }
-#undef WPUSH
-    S->lane_np[lane] = np;
-    S->lane_end[lane] = endc;
-    S->lane_nl[lane][0] = (uint32_t)nl0;
-    S->lane_nl[lane][1] = (uint32_t)nl1;
-    S->lane_nl[lane][2] = (uint32_t)nl2;
+    if (endc == -2) return endc;
+    D->meta[lane][lp] = (uint16_t)mt;
+    ++lp;
+    // room for one more pop: at most 9 pushes, all possibly in one list
+    if (endc == -1 && (lp == kWP || nl0 + 9 > kWL || nl1 + 9 > kWL || nl2 + 9 > kWL)) {
+        endc = 2;
+        D->lane_x[lane] = wpack(x);
+    }
+    return endc;
 }
 
 // the warp's chunk allocator (warp-uniform state; every lane holds the same copy)
@@ -307,13 +383,30 @@ struct WAlloc {
 };
 
 template <bool TRACE>
-__device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lane)
+__device__ __forceinline__ uint64_t trace_pop(uint64_t h, uint32_t binfo, const WEnt &y, int n_entries)
+{
+    h = trace_mix(h, binfo | (uint32_t)y.i);
+    h = trace_mix(h, y.k);
+    h = trace_mix(h, y.l);
+    h = trace_mix(h, (uint64_t)((uint32_t)y.n_mm | (uint32_t)y.n_gapo << 8 | (uint32_t)y.n_gape << 16
+                                | (uint32_t)y.state << 24));
+    int n_del = y.n_gapo + y.n_gape - y.n_ins;
+    h = trace_mix(h, (uint64_t)(y.n_ins & 0xffff) | (uint64_t)(n_del & 0xffff) << 16);
+    h = trace_mix(h, (uint64_t)(uint32_t)(y.isdiff ? y.i : 0));
+    h = trace_mix(h, (uint64_t)(uint32_t)n_entries);
+    return h;
+}
+
+template <bool TRACE>
+__device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
 {
     const unsigned FULL = 0xffffffffu;
-    const int r = a.list[pos];
+    const unsigned lt_mask = (1u << lane) - 1u;
     const int64_t s0 = a.off[r];
     const int len = (int)(a.off[r + 1] - s0);
-    const BatchOpt O = a.bopt[a.bidx[r]];
+    if (lane == 0) S->O = a.bopt[a.bidx[r]];
+    __syncwarp();
+    const BatchOpt &O = S->O;
     const int max_diff0 = a.maxdiff[r];
     const IndexView &ix = a.ix;
     for (int t = lane; t < len; t += 32) S->q[t] = a.query[s0 + t];
@@ -330,10 +423,17 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
     uint32_t f_alg = __shfl_sync(FULL, fetches, 0);   // algorithmic count: widths, then replayed chains
     uint4 *chunks = a.chunks;
     WAlloc A;
-    A.free_ids = a.free_ids + (size_t)wid * a.arena_chunks;
-    A.base = wid * a.arena_chunks; A.cap = a.arena_chunks; A.bump = 0; A.free_top = 0;
-    uint4 *stage_lane = a.stage + (size_t)wid * 3 * 32 * kWL + (size_t)lane * kWL;   // list L at + L * 32 * kWL
-    uint4 *prec_w = a.prec + (size_t)wid * 32 * kWR;
+    {
+        const bool big = wid < a.n_big;
+        const int64_t base = big ? (int64_t)wid * a.big_chunks
+                                 : (int64_t)a.n_big * a.big_chunks + (int64_t)(wid - a.n_big) * a.arena_chunks;
+        A.free_ids = a.free_ids + base;
+        A.base = (int)base; A.cap = big ? a.big_chunks : a.arena_chunks; A.bump = 0; A.free_top = 0;
+    }
+    uint4 *stage_w = a.stage + (size_t)wid * 3 * 32 * kWL;          // list L of lane j at + L * 32 * kWL + j * kWL
+    uint4 *stage_lane = stage_w + (size_t)lane * kWL;
+    uint4 *prec_w = a.prec + (size_t)wid * 32 * kWP;                 // pop t of lane j at + j * kWP + t
+    WSide *D = a.side + wid;
     // the staging list of each push kind: kinds whose target buckets coincide share a list, so the
     // bucket keeps the push order
     int tl[3];
@@ -351,9 +451,11 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
     int best_score = (max_diff0 + 1) * O.s_mm + (O.max_gapo + 1) * O.s_gapo + (O.max_gape + 1) * O.s_gape;
     int best_cnt = 0, n_aln = 0, ret = 0, n_entries = 0, peak = 0;
     uint64_t pops = 0, trace = kTraceInit;
-    unsigned long long d_waves = 0, d_lanes = 0, d_cons = 0, d_cont = 0, d_hz = 0, d_chainpops = 0;
-    long long c_chain = 0, c_replay = 0, c_commit = 0, c_load = 0, t_mark = 0;
     const bool dbg = a.dbg != nullptr;
+    if (dbg && lane == 0) {
+        for (int q = 0; q < kWDbgN; ++q) S->dv[q] = 0;
+        S->t_read = clock64();
+    }
 
     int n_amb = 0;
     for (int j = 0; j < len; ++j) n_amb += S->q[j] > 3;
@@ -381,128 +483,204 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
             }
             if (b >= kWMaxB || (!pend && S->n_in[b] <= 0)) { ret = kErrStack; break; }   // inconsistent: re-run elsewhere
             const uint32_t binfo = (uint32_t)b << 21;
-            if (dbg) t_mark = clock64();
-            const int navail = (pend ? 1 : 0) + S->n_in[b];
-            const int Wn = navail < 32 ? navail : 32;
-            // load the wave's entries: lane 0 the pending child (if any), then the bucket from the top
-            WEnt x;
-            x.k = 0; x.l = 0; x.i = 0; x.isdiff = 0; x.n_mm = x.n_gapo = x.n_gape = x.n_ins = 0; x.state = 0;
-            if (lane < Wn) {
-                if (pend && lane == 0) x = px;
-                else {
-                    int d = lane - (pend ? 1 : 0);
-                    int tc = S->top_chunk[b], cnt = S->top_cnt[b];
-                    uint4 v = make_uint4(0, 0, 0, 0);
-                    if (tc >= 0 && d < cnt) v = chunks[(size_t)tc * kWCH + (cnt - 1 - d)];
-                    else if (tc >= 0) {
-                        int pc = a.chunk_prev[tc];
-                        if (pc >= 0 && d - cnt < kWCH) v = chunks[(size_t)pc * kWCH + (kWCH - 1 - (d - cnt))];
-                    }
-                    x = wunpack(v);
-                }
-            }
+            const int pend_i = pend ? 1 : 0;
             // early stop (the same for the whole bucket until a hit): the sequential search pops one entry
-            if (!c.nonstop && (binfo >> 21) > (uint32_t)(best_score + O.s_mm)) {
+            if (!c.nonstop && b > best_score + O.s_mm) {
                 --n_entries;
                 ++pops;
                 if (TRACE) {
-                    WEnt y;
-                    y.k = __shfl_sync(FULL, x.k, 0); y.l = __shfl_sync(FULL, x.l, 0);
-                    y.i = __shfl_sync(FULL, x.i, 0); y.isdiff = __shfl_sync(FULL, x.isdiff, 0);
-                    y.n_mm = __shfl_sync(FULL, x.n_mm, 0); y.n_gapo = __shfl_sync(FULL, x.n_gapo, 0);
-                    y.n_gape = __shfl_sync(FULL, x.n_gape, 0); y.n_ins = __shfl_sync(FULL, x.n_ins, 0);
-                    y.state = __shfl_sync(FULL, x.state, 0);
-                    uint64_t h = trace;
-                    h = trace_mix(h, binfo | (uint32_t)y.i);
-                    h = trace_mix(h, y.k);
-                    h = trace_mix(h, y.l);
-                    h = trace_mix(h, (uint64_t)((uint32_t)y.n_mm | (uint32_t)y.n_gapo << 8 | (uint32_t)y.n_gape << 16
-                                                | (uint32_t)y.state << 24));
-                    int n_del = y.n_gapo + y.n_gape - y.n_ins;
-                    h = trace_mix(h, (uint64_t)(y.n_ins & 0xffff) | (uint64_t)(n_del & 0xffff) << 16);
-                    h = trace_mix(h, (uint64_t)(uint32_t)(y.isdiff ? y.i : 0));
-                    h = trace_mix(h, (uint64_t)(uint32_t)n_entries);
-                    trace = h;
+                    WEnt y = pend ? px : wunpack(chunks[(size_t)S->top_chunk[b] * kWCH + S->top_cnt[b] - 1]);
+                    trace = trace_pop<TRACE>(trace, binfo, y, n_entries);
                 }
                 break;
             }
-            // speculative chains
-            if (dbg) { long long t = clock64(); c_load += t - t_mark; t_mark = t; }
-            if (lane < Wn) lane_chain<TRACE>(ix, O, c, S, lane, x, b, fetches, stage_lane, tl, prec_w + (size_t)lane * kWR);
+            if (dbg && lane == 0) S->t_mark = clock64();
+            // the wave's entries, in pop order: the pending child (if any), then bucket b from the top
+            const int navail = pend_i + S->n_in[b];
+            const int Wcap = navail < kWE ? navail : kWE;
+            int walk_ok = 1;
+            if (lane == 0) {
+                int ch = S->top_chunk[b], k = 0, cov = 0;
+                const int need = Wcap - pend_i;
+                while (cov < need) {
+                    if (ch < 0 || k >= kWE / kWCH + 2) { walk_ok = 0; break; }
+                    S->wch[k] = ch;
+                    cov += k == 0 ? S->top_cnt[b] : kWCH;
+                    ++k;
+                    if (cov < need) ch = a.chunk_prev[ch];
+                }
+            }
+            walk_ok = __shfl_sync(FULL, walk_ok, 0);
+            if (!walk_ok) { ret = kErrStack; break; }
+            __syncwarp();
+            {
+                const int cnt = S->top_cnt[b];
+                for (int e = lane; e < Wcap; e += 32) {
+                    uint4 v;
+                    if (e < pend_i) v = wpack(px);
+                    else {
+                        const int d = e - pend_i;
+                        int ci, p;
+                        if (d < cnt) { ci = 0; p = cnt - 1 - d; }
+                        else { const int d2 = d - cnt; ci = 1 + d2 / kWCH; p = kWCH - 1 - d2 % kWCH; }
+                        v = chunks[(size_t)S->wch[ci] * kWCH + p];
+                    }
+                    S->ent[e] = v;
+                }
+            }
+            __syncwarp();
+            WDBG_LAP(kDbgCycLoad);
+
+            // ---- speculative chains: idle lanes take the next entry, busy lanes pop ----
+            int e_next = 0, limit = Wcap;
+            int ce = -1;                                   // this lane's entry
+            int lp = 0, nl0 = 0, nl1 = 0, nl2 = 0;        // this lane's pops and staged pushes in the wave
+            int e_p0 = 0, e_np = 0, e_pre = 0, e_mpre = 0, e_pmax = 0, e_s0 = 0, e_s1 = 0, e_s2 = 0;
+            uint32_t e_fs = 0;
+            WEnt x;
+            x.k = 0; x.l = 0; x.i = 0; x.isdiff = 0; x.n_mm = x.n_gapo = x.n_gape = x.n_ins = 0; x.state = 0;
+            WWalk wk;
+            wk.k = 0; wk.l = 0; wk.i = 0; wk.f = 0; wk.on = false;
+            for (;;) {
+                const int nlm = max(nl0, max(nl1, nl2));
+                const bool want = ce < 0 && lp + kWGrabPops <= kWP && nlm + 9 * kWGrabPops <= kWL;
+                const unsigned wb = __ballot_sync(FULL, want);
+                if (wb && e_next < limit) {
+                    const int e = e_next + __popc(wb & lt_mask);
+                    if (want && e < limit) {
+                        ce = e;
+                        x = wunpack(S->ent[e]);
+                        e_p0 = lp; e_np = 0; e_pre = 0; e_mpre = 0; e_pmax = 0; e_fs = 0;
+                        e_s0 = nl0; e_s1 = nl1; e_s2 = nl2;
+                    }
+                    e_next = min(limit, e_next + __popc(wb));
+                }
+                if (!__any_sync(FULL, ce >= 0)) break;
+                int stop_e = 0x7fffffff;
+                if (ce >= 0) {
+                    uint32_t mt = 0;
+                    const int endc = lane_step<TRACE>(ix, O, c, S, D, lane, x, wk, b, fetches, stage_lane, tl,
+                                                      prec_w + (size_t)lane * kWP, lp, nl0, nl1, nl2, mt);
+                    if (endc == -2) goto next_step;          // an exact walk goes on
+                    ++e_np;
+                    if (e_pre > e_mpre) e_mpre = e_pre;     // n_entries before this pop, relative to the chain start
+                    e_pre += (int)(mt & 15u) + (int)((mt >> 4) & 1u) - 1;
+                    if (e_pre > e_pmax) e_pmax = e_pre;
+                    e_fs += mt >> 5;
+                    if (endc >= 0) {
+                        S->e_info[ce] = (uint32_t)lane | (uint32_t)e_p0 << 8 | (uint32_t)e_np << 16 | (uint32_t)endc << 24;
+                        S->e_seg[0][ce] = (uint32_t)e_s0 | (uint32_t)(nl0 - e_s0) << 16;
+                        S->e_seg[1][ce] = (uint32_t)e_s1 | (uint32_t)(nl1 - e_s1) << 16;
+                        S->e_seg[2][ce] = (uint32_t)e_s2 | (uint32_t)(nl2 - e_s2) << 16;
+                        S->e_a[ce] = ((uint32_t)e_pre & 0xffffu) | (uint32_t)e_mpre << 16;
+                        S->e_b[ce] = (uint32_t)e_pmax | e_fs << 16;
+                        if (endc > 0) stop_e = ce;
+                        ce = -1;
+                    }
+                }
+            next_step:
+                // a stop ends the hand-out after its entry; chains past it are dropped
+                const int ms = __reduce_min_sync(FULL, stop_e);
+                if (ms != 0x7fffffff && ms + 1 < limit) limit = ms + 1;
+                if (ce >= limit) { ce = -1; wk.on = false; }
+            }
+            const int E = min(e_next, limit);
             __syncwarp();
             if (dbg) {
-                long long t = clock64(); c_chain += t - t_mark; t_mark = t;
-                ++d_waves; d_lanes += Wn;
-                for (int j = 0; j < Wn; ++j) d_chainpops += S->lane_np[j];
+                const unsigned cp = __reduce_add_sync(FULL, (unsigned)lp);
+                WDBG_LAP(kDbgCycChain);
+                WDBG_ADD(kDbgWaves, 1);
+                WDBG_ADD(kDbgLanes, E);
+                WDBG_ADD(kDbgChainPops, cp);
             }
-            // replay in sequential order. Without the trace hash, the lanes before the first lane that
+
+            // ---- replay in sequential order. Without the trace hash, the entries before the first one that
             // stops the replay (a hit, an error, an unfinished chain, or the max_entries cut-off inside its
-            // chain) are replayed at once from prefix sums; that lane, and in trace mode every lane, one pop
-            // at a time.
-            int consumed = 0;          // lanes whose entries are consumed
+            // chain) are replayed at once from prefix sums; that entry, and in trace mode every entry, one pop
+            // at a time. Lane j holds entries 4j..4j+3.
+            static_assert(kWE == 4 * 32, "replay layout");
+            int consumed = 0;
             bool stop = false, search_end = false, new_pend = false;
             int j_first = 0;
             if (!TRACE) {
-                const int npl = lane < Wn ? S->lane_np[lane] : 0;
-                const int endl = lane < Wn ? S->lane_end[lane] : 0;
-                int pre = 0, mpre = 0, pmax = 0;
-                uint32_t fsum = 0;
-                for (int t = 0; t < npl; ++t) {
-                    const uint32_t meta = S->meta[lane][t];
-                    if (pre > mpre) mpre = pre;          // n_entries before pop t, relative to the chain start
-                    pre += (int)(meta & 0xff) + (int)((meta >> 8) & 1) - 1;
-                    if (pre > pmax) pmax = pre;
-                    fsum += meta >> 16;
+                int pre_k[4], mpre_k[4], pmax_k[4], np_k[4];
+                uint32_t fs_k[4];
+                bool hard_k[4];
+                int lsum = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int e = 4 * lane + k;
+                    pre_k[k] = mpre_k[k] = pmax_k[k] = np_k[k] = 0; fs_k[k] = 0; hard_k[k] = false;
+                    if (e < E) {
+                        const uint32_t inf = S->e_info[e], ea = S->e_a[e], eb = S->e_b[e];
+                        pre_k[k] = (int)(int16_t)(ea & 0xffffu);
+                        mpre_k[k] = (int)(ea >> 16);
+                        pmax_k[k] = (int)(eb & 0xffffu);
+                        fs_k[k] = eb >> 16;
+                        np_k[k] = (int)((inf >> 16) & 0xffu);
+                        hard_k[k] = (inf >> 24) != 0;
+                    }
+                    lsum += pre_k[k];
                 }
-                int incl = pre;
+                int incl = lsum;
+#pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
-                    int v = __shfl_up_sync(FULL, incl, o);
+                    const int v = __shfl_up_sync(FULL, incl, o);
                     if (lane >= o) incl += v;
                 }
-                const int nstart = n_entries + incl - pre;
-                const bool cross = lane < Wn && nstart + mpre > O.max_entries;
-                const unsigned bal = __ballot_sync(FULL, lane < Wn && (cross || endl != 0));
-                const int sstar = bal ? __ffs(bal) - 1 : Wn;
-                const bool take = lane < sstar;
-                pops += (uint64_t)__reduce_add_sync(FULL, take ? (unsigned)npl : 0u);
-                n_entries += (int)__reduce_add_sync(FULL, take ? (unsigned)pre : 0u);
-                f_alg += __reduce_add_sync(FULL, take ? fsum : 0u);
-                const int pk = (int)__reduce_max_sync(FULL, take ? (unsigned)(nstart + pmax) : 0u);
-                if (pk > peak) peak = pk;
+                int run = n_entries + incl - lsum;         // n_entries before this lane's first entry
+                int first = 0x7fffffff;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int e = 4 * lane + k;
+                    if (e < E && first == 0x7fffffff && (hard_k[k] || run + mpre_k[k] > O.max_entries)) first = e;
+                    run += pre_k[k];
+                }
+                const int sstar = min(__reduce_min_sync(FULL, first), E);
+                run = n_entries + incl - lsum;
+                int t_np = 0, t_pre = 0, pk = 0;
+                uint32_t t_fs = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int e = 4 * lane + k;
+                    if (e < sstar) {
+                        t_np += np_k[k]; t_pre += pre_k[k]; t_fs += fs_k[k];
+                        pk = max(pk, run + pmax_k[k]);
+                    }
+                    run += pre_k[k];
+                }
+                pops += (uint64_t)__reduce_add_sync(FULL, (unsigned)t_np);
+                n_entries += (int)__reduce_add_sync(FULL, (unsigned)t_pre);
+                f_alg += __reduce_add_sync(FULL, t_fs);
+                const int pkm = (int)__reduce_max_sync(FULL, (unsigned)pk);
+                if (pkm > peak) peak = pkm;
                 consumed = sstar;
                 j_first = sstar;
             }
-            for (int j = j_first; j < Wn && !stop && (TRACE || j == j_first); ++j) {
-                const int np = S->lane_np[j], endc = S->lane_end[j];
+            for (int e = j_first; e < E && !stop && (TRACE || e == j_first); ++e) {
+                const uint32_t inf = S->e_info[e];
+                const int ln = (int)(inf & 0xffu), p0 = (int)((inf >> 8) & 0xffu), np = (int)((inf >> 16) & 0xffu);
+                const int endc = (int)(inf >> 24);
+                // the entry's per-pop data, np <= kWP <= 64 words, one load per lane
+                static_assert(kWP <= 64, "replay prefetch");
+                const uint16_t *mrow = D->meta[ln] + p0;
+                const uint32_t m_lo = lane < np ? mrow[lane] : 0u, m_hi = lane + 32 < np ? mrow[lane + 32] : 0u;
                 for (int t = 0; t < np; ++t) {
                     if (n_entries > O.max_entries) { search_end = true; stop = true; break; }
                     --n_entries;
                     ++pops;
-                    const uint32_t meta = S->meta[j][t];
-                    f_alg += meta >> 16;
-                    if (TRACE) {
-                        WEnt y = wunpack(prec_w[(size_t)j * kWR + t]);
-                        uint64_t h = trace;
-                        h = trace_mix(h, binfo | (uint32_t)y.i);
-                        h = trace_mix(h, y.k);
-                        h = trace_mix(h, y.l);
-                        h = trace_mix(h, (uint64_t)((uint32_t)y.n_mm | (uint32_t)y.n_gapo << 8
-                                                    | (uint32_t)y.n_gape << 16 | (uint32_t)y.state << 24));
-                        int n_del = y.n_gapo + y.n_gape - y.n_ins;
-                        h = trace_mix(h, (uint64_t)(y.n_ins & 0xffff) | (uint64_t)(n_del & 0xffff) << 16);
-                        h = trace_mix(h, (uint64_t)(uint32_t)(y.isdiff ? y.i : 0));
-                        h = trace_mix(h, (uint64_t)(uint32_t)n_entries);
-                        trace = h;
-                    }
+                    const uint32_t meta = __shfl_sync(FULL, t < 32 ? m_lo : m_hi, t & 31);
+                    f_alg += meta >> 5;
+                    if (TRACE) trace = trace_pop<TRACE>(trace, binfo, wunpack(prec_w[(size_t)ln * kWP + p0 + t]), n_entries);
                     if (t == np - 1 && endc == 3) { ret = kErrScore; search_end = true; stop = true; break; }
                     if (t == np - 1 && endc == 1) {
                         // the hit, as bwt_match_gap handles it
-                        consumed = j + 1;
+                        consumed = e + 1;
                         stop = true;
-                        WEnt e = wunpack(S->hz[j]);
-                        uint64_t k = S->hk[j], l = S->hl[j];
-                        int sc = e.n_mm * O.s_mm + e.n_gapo * O.s_gapo + e.n_gape * O.s_gape;
-                        int diffs = e.n_mm + e.n_gapo + (c.gape ? e.n_gape : 0);
+                        WEnt h = wunpack(D->hz[ln]);
+                        uint64_t k = D->hk[ln], l = D->hl[ln];
+                        int sc = h.n_mm * O.s_mm + h.n_gapo * O.s_gapo + h.n_gape * O.s_gape;
+                        int diffs = h.n_mm + h.n_gapo + (c.gape ? h.n_gape : 0);
                         if (n_aln == 0) {
                             best_score = sc;
                             if (!c.nonstop) c.max_diff = diffs + 1 > max_diff0 ? max_diff0 : diffs + 1;
@@ -510,11 +688,11 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                         if (sc == best_score) best_cnt = (int)(uint32_t)((uint64_t)(int64_t)best_cnt + (l - k + 1));
                         else if (best_cnt > O.max_top2) { search_end = true; break; }
                         bool add = true;
-                        if (e.n_gapo)
+                        if (h.n_gapo)
                             for (int q = 0; q < n_aln; ++q)
                                 if (aln[3 * q + 1] == k && aln[3 * q + 2] == l) { add = false; break; }
                         if (add) {
-                            int ldp = e.isdiff ? e.i : 0;
+                            int ldp = h.isdiff ? h.i : 0;
                             uint64_t xx = (uint64_t)(int64_t)(int)(l - k + 1);
                             int jb = 0;
                             for (int t0 = 0; t0 < ldp; t0 += 32) {
@@ -522,7 +700,7 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                                 uint64_t v = tt < ldp ? S->W[tt] : 0, wv = v & kW48;
                                 bool eq = tt < ldp && wv == xx, gt = tt < ldp && wv > xx;
                                 unsigned bal = __ballot_sync(FULL, eq);
-                                int rank = __popc(bal & ((1u << lane) - 1));
+                                int rank = __popc(bal & lt_mask);
                                 if (gt) S->W[tt] = (v & ~kW48) | (wv - xx);
                                 if (eq) S->W[tt] = (1ull << 48) | ((ix.seq_len - (uint64_t)(jb + rank + 1)) & kW48);
                                 jb += __popc(bal);
@@ -530,10 +708,10 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                             __syncwarp();
                             if (n_aln == a.aln_cap) { ret = kErrAln; search_end = true; break; }
                             if (lane == 0) {
-                                int n_del = e.n_gapo + e.n_gape - e.n_ins;
-                                aln[3 * n_aln] = (uint64_t)(e.n_mm & 0xff) | (uint64_t)(e.n_gapo & 0xff) << 8
-                                               | (uint64_t)(e.n_gape & 0xff) << 16 | (uint64_t)(sc & 0xfffff) << 24
-                                               | (uint64_t)(e.n_ins & 0x3ff) << 44 | (uint64_t)(n_del & 0x3ff) << 54;
+                                int n_del = h.n_gapo + h.n_gape - h.n_ins;
+                                aln[3 * n_aln] = (uint64_t)(h.n_mm & 0xff) | (uint64_t)(h.n_gapo & 0xff) << 8
+                                               | (uint64_t)(h.n_gape & 0xff) << 16 | (uint64_t)(sc & 0xfffff) << 24
+                                               | (uint64_t)(h.n_ins & 0x3ff) << 44 | (uint64_t)(n_del & 0x3ff) << 54;
                                 aln[3 * n_aln + 1] = k;
                                 aln[3 * n_aln + 2] = l;
                             }
@@ -542,38 +720,36 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                         }
                         break;
                     }
-                    n_entries += (int)(meta & 0xff) + (int)((meta >> 8) & 1);
+                    n_entries += (int)(meta & 15u) + (int)((meta >> 4) & 1u);
                     if (n_entries > peak) peak = n_entries;
                 }
                 if (stop) break;
-                consumed = j + 1;
+                consumed = e + 1;
                 if (endc == 2) { new_pend = true; stop = true; }
             }
             if (dbg) {
-                long long t = clock64(); c_replay += t - t_mark; t_mark = t;
-                d_cons += consumed; d_cont += new_pend ? 1 : 0;
-                if (consumed > 0 && S->lane_end[consumed - 1] == 1) ++d_hz;
+                WDBG_LAP(kDbgCycReplay);
+                WDBG_ADD(kDbgConsumed, consumed);
+                WDBG_ADD(kDbgCont, new_pend ? 1 : 0);
+                WDBG_ADD(kDbgHazard, consumed > 0 && (S->e_info[consumed - 1] >> 24) == 1 ? 1 : 0);
             }
             if (search_end) break;
-            // take the consumed entries off bucket b (lane 0 of the wave may have been the pending child)
-            int C = consumed - (pend ? 1 : 0);
+            // take the consumed entries off bucket b (entry 0 may have been the pending child)
+            const int C = consumed - pend_i;
             if (C > 0) {
-                int tc = S->top_chunk[b], cnt = S->top_cnt[b];
-                if (tc < 0) { ret = kErrStack; break; }
+                int tc = S->top_chunk[b], cnt = S->top_cnt[b], left = C;
                 __syncwarp();
-                if (C < cnt) {
-                    if (lane == 0) S->top_cnt[b] = (uint16_t)(cnt - C);
-                } else {
-                    int pc = a.chunk_prev[tc];
+                while (tc >= 0 && left >= cnt) {
+                    left -= cnt;
+                    const int pc = a.chunk_prev[tc];
                     A.release(tc, lane);
-                    int rest = C - cnt;    // entries taken from the previous chunk
-                    if (pc >= 0 && rest == kWCH) { int pp = a.chunk_prev[pc]; A.release(pc, lane); pc = pp; rest = 0; }
-                    if (lane == 0) {
-                        S->top_chunk[b] = pc;
-                        S->top_cnt[b] = (uint16_t)(pc >= 0 ? kWCH - rest : 0);
-                    }
+                    tc = pc;
+                    cnt = kWCH;
                 }
+                if (tc < 0 && left > 0) { ret = kErrStack; break; }
                 if (lane == 0) {
+                    S->top_chunk[b] = tc;
+                    S->top_cnt[b] = (uint16_t)(tc >= 0 ? cnt - left : 0);
                     S->n_in[b] -= C;
                     if (S->n_in[b] == 0) S->mask[b >> 5] &= ~(1u << (b & 31));
                 }
@@ -583,18 +759,25 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
             if (new_pend) {
                 pend = true;
                 pend_b = b;
-                px = wunpack(S->lane_x[consumed - 1]);
+                px = wunpack(D->lane_x[S->e_info[consumed - 1] & 0xffu]);
             }
-            // commit the pushes of the consumed lanes, list by list (one list per target bucket), in replay
-            // order: lane order, then the order the lane staged them
+            // commit the pushes of the consumed entries, list by list (one list per target bucket), in replay
+            // order: entry order, then the order the entry's lane staged them
             bool fail = false;
             for (int L = 0; L < 3 && !fail; ++L) {
                 if (lst_pen[L] < 0) continue;
                 const int X = b + lst_pen[L];
-                int cntX = lane < consumed ? (int)S->lane_nl[lane][L] : 0;
-                int incl = cntX;
+                int cnt_k[4], lsum = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int e = 4 * lane + k;
+                    cnt_k[k] = e < consumed ? (int)(S->e_seg[L][e] >> 16) : 0;
+                    lsum += cnt_k[k];
+                }
+                int incl = lsum;
+#pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
-                    int v = __shfl_up_sync(FULL, incl, o);
+                    const int v = __shfl_up_sync(FULL, incl, o);
                     if (lane >= o) incl += v;
                 }
                 const int T = __shfl_sync(FULL, incl, 31);
@@ -605,29 +788,40 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                 if (need > kWNewC || !A.alloc_n(need, S->newc, lane)) { ret = kErrStack; fail = true; break; }
                 // chain the new chunks on top of c0
                 for (int t = lane; t < need; t += 32) a.chunk_prev[S->newc[t]] = t == 0 ? c0 : S->newc[t - 1];
-                // copy: output position p (0..T) comes from the lane j with incl[j-1] <= p < incl[j]
-                S->incl[lane] = incl;
+                // inclusive counts per entry (e_a is free after the replay)
+                {
+                    int run = incl - lsum;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int e = 4 * lane + k;
+                        run += cnt_k[k];
+                        if (e < consumed) S->e_a[e] = (uint32_t)run;
+                    }
+                }
                 __syncwarp();
-                const uint4 *stw = a.stage + (size_t)wid * 3 * 32 * kWL + (size_t)L * 32 * kWL;
+                // copy: output position p (0..T) comes from the entry e with incl[e-1] <= p < incl[e]
+                const uint4 *stl = stage_w + (size_t)L * 32 * kWL;
                 for (int p0 = 0; p0 < T; p0 += 32) {
                     const int p = p0 + lane;
                     if (p < T) {
-                        int lo = 0, hi = 31;          // first lane whose inclusive count exceeds p
+                        int lo = 0, hi = consumed - 1;
                         while (lo < hi) {
-                            int mid = (lo + hi) >> 1;
-                            if (S->incl[mid] > p) hi = mid; else lo = mid + 1;
+                            const int mid = (lo + hi) >> 1;
+                            if ((int)S->e_a[mid] > p) hi = mid; else lo = mid + 1;
                         }
-                        const int before = lo ? S->incl[lo - 1] : 0;
+                        const int before = lo ? (int)S->e_a[lo - 1] : 0;
+                        const int ln = (int)(S->e_info[lo] & 0xffu);
+                        const int st0 = (int)(S->e_seg[L][lo] & 0xffffu);
                         const int g = cnt0 + p;
                         const int ci = g / kWCH;
                         const int chunk = c0 >= 0 ? (ci == 0 ? c0 : S->newc[ci - 1]) : S->newc[ci];
-                        chunks[(size_t)chunk * kWCH + (g % kWCH)] = stw[(size_t)lo * kWL + (p - before)];
+                        chunks[(size_t)chunk * kWCH + (g % kWCH)] = stl[(size_t)ln * kWL + st0 + (p - before)];
                     }
                 }
                 __syncwarp();
                 if (lane == 0) {
-                    int last = cnt0 + T - 1;
-                    int ci = last / kWCH;
+                    const int last = cnt0 + T - 1;
+                    const int ci = last / kWCH;
                     S->top_chunk[X] = c0 >= 0 ? (ci == 0 ? c0 : S->newc[ci - 1]) : S->newc[ci];
                     S->top_cnt[X] = (uint16_t)(last % kWCH + 1);
                     S->n_in[X] += T;
@@ -635,7 +829,7 @@ __device__ void warp_read(const WArgs &a, int pos, int wid, WarpSmem *S, int lan
                 }
                 __syncwarp();
             }
-            if (dbg) { long long t = clock64(); c_commit += t - t_mark; }
+            WDBG_LAP(kDbgCycCommit);
             if (fail) break;
         }
         if (ret == 0) ret = n_aln;
@@ -652,45 +846,102 @@ publish:
         }
     }
     if (dbg && lane == 0) {
-        atomicAdd(a.dbg + kDbgReads, 1ull);
-        atomicAdd(a.dbg + kDbgWaves, d_waves);
-        atomicAdd(a.dbg + kDbgLanes, d_lanes);
-        atomicAdd(a.dbg + kDbgConsumed, d_cons);
-        atomicAdd(a.dbg + kDbgPops, (unsigned long long)pops);
-        atomicAdd(a.dbg + kDbgCont, d_cont);
-        atomicAdd(a.dbg + kDbgHazard, d_hz);
-        atomicAdd(a.dbg + kDbgCycChain, (unsigned long long)c_chain);
-        atomicAdd(a.dbg + kDbgCycReplay, (unsigned long long)c_replay);
-        atomicAdd(a.dbg + kDbgCycCommit, (unsigned long long)c_commit);
-        atomicAdd(a.dbg + kDbgCycLoad, (unsigned long long)c_load);
-        atomicAdd(a.dbg + kDbgChainPops, d_chainpops);
+        S->dv[kDbgReads] = 1;
+        S->dv[kDbgPops] = pops;
+        const unsigned long long cyc = (unsigned long long)(clock64() - S->t_read);
+        S->dv[kDbgCycRead] = cyc;
+        for (int q = 0; q < kWDbgN; ++q)
+            if (q != kDbgCycReadMax) atomicAdd(a.dbg + q, S->dv[q]);
+        atomicMax(a.dbg + kDbgCycReadMax, cyc);
     }
     if (lane == 0) {
-        if (ret == kErrStack || ret == kErrAln) a.ovf[atomicAdd(a.ovf_n, 1)] = r;
         a.out_n[r] = ret;
         a.out_pops[r] = pops;
         a.out_trace[r] = TRACE ? trace : 0;
         a.out_peak[r] = peak;
         a.out_fetch[r] = f_alg;
         a.out_tier[r] = (int8_t)a.tier;
+        if (ret == kErrStack && wid >= a.n_big && a.n_big > 0) {
+            // to a big warp (its results overwrite these)
+            __threadfence();
+            const int slot = atomicAdd(a.q_ctl + 1, 1);
+            atomicExch(a.ovq + slot, r);
+        } else if (ret == kErrStack || ret == kErrAln) a.ovf[atomicAdd(a.ovf_n, 1)] = r;
     }
     __syncwarp();
 }
 
+__device__ __forceinline__ uint64_t gtimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// A big warp's next read (lane 0): a queued one first, else one from the list; -1 when the list is done, every
+// small warp has finished and the queue is empty, or after kQWaitNs of waiting (the reads still queued then
+// go to the next pass; if the wait was for a claimed slot, q_ctl[3] is set and the host re-runs every queued
+// read).
+constexpr uint64_t kQWaitNs = 2000000000ull;
+__device__ __noinline__ int big_next(const WArgs &a)
+{
+    volatile int32_t *qc = a.q_ctl;
+    const int n_small = a.n_warps - a.n_big;
+    const uint64_t t0 = gtimer_ns();
+    for (;;) {
+        if (gtimer_ns() - t0 > kQWaitNs) return -1;    // the reads left in the queue go to the next pass
+        const int h = qc[0], t = qc[1];
+        if (h < t) {
+            if (atomicCAS(a.q_ctl, h, h + 1) == h) {
+                // the producer has taken slot h; its read id follows its atomicAdd at once
+                for (;;) {
+                    const int r = atomicAdd(a.ovq + h, 0);
+                    if (r >= 0) { __threadfence(); return r; }
+                    if (gtimer_ns() - t0 > kQWaitNs) { atomicExch(a.q_ctl + 3, 1); return -1; }
+                    __nanosleep(100);
+                }
+            }
+            continue;
+        }
+        if (*(volatile int32_t *)a.claim < a.n) {
+            const int p = atomicAdd(a.claim, 1);
+            if (p < a.n) return a.list[p];
+            continue;
+        }
+        if (qc[2] == n_small) {
+            __threadfence();
+            if (qc[0] >= qc[1]) return -1;
+            continue;
+        }
+        __nanosleep(2000);
+    }
+}
+
 template <bool TRACE>
-__global__ void __launch_bounds__(32) warp_kernel(const __grid_constant__ WArgs a)
+__global__ void __launch_bounds__(32, 16) warp_kernel(const __grid_constant__ WArgs a)
 {
     extern __shared__ __align__(16) unsigned char wsm_raw[];
     WarpSmem *S = (WarpSmem *)wsm_raw;
     const int lane = threadIdx.x & 31;
     const int wid = blockIdx.x;
     if (wid >= a.n_warps) return;
+    const bool big = wid < a.n_big;
     for (;;) {
-        int pos = 0;
-        if (lane == 0) pos = atomicAdd(a.claim, 1);
-        pos = __shfl_sync(0xffffffffu, pos, 0);
-        if (pos >= a.n) break;
-        warp_read<TRACE>(a, pos, wid, S, lane);
+        int r = -1;
+        if (lane == 0) {
+            if (big) r = big_next(a);
+            else {
+                const int p = atomicAdd(a.claim, 1);
+                r = p < a.n ? a.list[p] : -1;
+            }
+        }
+        r = __shfl_sync(0xffffffffu, r, 0);
+        if (r < 0) break;
+        warp_read<TRACE>(a, r, wid, S, lane);
+    }
+    if (!big && a.n_big > 0 && lane == 0) {
+        __threadfence();
+        atomicAdd(a.q_ctl + 2, 1);
     }
 }
 
