@@ -153,10 +153,10 @@ class Index:
             raise GalnError("bad warp tier setting")
 
     def warp_counters(self) -> dict:
-        v = np.zeros(14, np.uint64)
-        lib().galn_last_warp_counters(self.h, v.ctypes.data, 14)
+        v = np.zeros(15, np.uint64)
+        lib().galn_last_warp_counters(self.h, v.ctypes.data, 15)
         names = ["reads", "waves", "lanes", "consumed", "pops", "continued", "hits", "cyc_chain", "cyc_replay",
-                 "cyc_commit", "cyc_load", "chain_pops", "cyc_read", "cyc_read_max"]
+                 "cyc_commit", "cyc_load", "chain_pops", "cyc_read", "steps", "cyc_read_max"]
         return {k: int(x) for k, x in zip(names, v)}
 
     def autotune(self, args, reads: "Reads", max_sample: int = 131072) -> dict:
@@ -191,6 +191,12 @@ class Index:
             out["fetch"] = fetch[:n]
             out["tier"] = tier[:n]
         return out
+
+    def last_phases(self) -> dict:
+        """Host-side timeline of the last run, in ms from the call's start."""
+        v = (C.c_double * 5)()
+        lib().galn_last_run_phases(self.h, v, 5)
+        return dict(launch=v[0], device_done=v[1], results=v[2], total=v[3], device=v[4])
 
     def last_stats(self) -> dict:
         t, k, tiers, la = C.c_double(), C.c_double(), C.c_int(), C.c_int64()

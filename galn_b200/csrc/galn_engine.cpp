@@ -119,18 +119,23 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     }
     std::vector<int32_t> maxdiff((size_t)std::max(n, 1));
     {
-        std::unordered_map<uint64_t, int> cache;   // (fnr bits, length) -> max_diff
+        // bwa_cal_maxdiff by read length, one table per distinct -n fraction among the option sets
+        std::vector<float> fnrs;
+        std::vector<std::vector<int32_t>> tabs;
         for (int r = 0; r < n; ++r) {
-            int len = (int)(in->offset[r + 1] - in->offset[r]);
+            const int len = (int)(in->offset[r + 1] - in->offset[r]);
             const galn_opts *o = bset[bid[r]];
             int md;
             if (o->fnr > 0.0) {
-                uint32_t fb;
-                memcpy(&fb, &o->fnr, 4);
-                uint64_t key = ((uint64_t)fb << 32) | (uint32_t)len;
-                auto it = cache.find(key);
-                if (it == cache.end()) it = cache.emplace(key, galn_cal_maxdiff(len, 0.02, o->fnr)).first;
-                md = it->second;
+                size_t t = 0;
+                while (t < fnrs.size() && memcmp(&fnrs[t], &o->fnr, 4) != 0) ++t;
+                if (t == fnrs.size()) {
+                    fnrs.push_back(o->fnr);
+                    tabs.emplace_back((size_t)max_len + 1, -1);
+                }
+                int32_t &slot = tabs[t][(size_t)len];
+                if (slot < 0) slot = galn_cal_maxdiff(len, 0.02, o->fnr);
+                md = slot;
             } else md = bopt[bid[r]].max_diff;
             maxdiff[r] = md;
             if (md > 125) wide = true;
@@ -202,6 +207,7 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     ECK(cudaEventCreate(&span0));
     ECK(cudaEventCreate(&span1));
     ECK(cudaEventRecord(span0, st));
+    S.ms_phase[0] = now_ms() - t_start;
     RCK(dev_encode(job, st));
     if (n > 0) S.kernel_launches += 1;
 
@@ -335,11 +341,21 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
             else rest.push_back(r);
         }
         // longest expected searches first (max_diff, then length), so that the heaviest reads do not start
-        // last and run alone at the end of the launch; results do not depend on the order
-        std::stable_sort(elig.begin(), elig.end(), [&](int32_t x, int32_t y) {
-            if (maxdiff[x] != maxdiff[y]) return maxdiff[x] > maxdiff[y];
-            return in->offset[x + 1] - in->offset[x] > in->offset[y + 1] - in->offset[y];
-        });
+        // last and run alone at the end of the launch; results do not depend on the order. A counting sort:
+        // the eligible reads have max_diff <= 125 and length <= kWarpMaxLen.
+        {
+            const int kL = kWarpMaxLen + 1, nkey = 126 * kL;
+            std::vector<int32_t> cnt((size_t)nkey + 1, 0), sorted(elig.size());
+            auto key = [&](int32_t r) {
+                const int md = std::min(std::max(maxdiff[r], 0), 125);
+                const int len = (int)(in->offset[r + 1] - in->offset[r]);
+                return (125 - md) * kL + (kWarpMaxLen - len);   // ascending key = descending (max_diff, length)
+            };
+            for (int32_t r : elig) ++cnt[(size_t)key(r) + 1];
+            for (int k = 0; k < nkey; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];
+            for (int32_t r : elig) sorted[(size_t)cnt[(size_t)key(r)]++] = r;
+            elig.swap(sorted);
+        }
         // pass 1: the tuned arena per warp, plus up to kBigWarps warps whose arenas hold the max_entries
         // cut-off and take over, in the same launch, the reads that outgrow the small ones; pass 2, only for
         // reads still queued when pass 1 ended, with big arenas for every warp
@@ -480,30 +496,48 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     cudaEventDestroy(span1);
     if (n_ovf > 0) return GALN_ENOMEM;
 
-    // ---- results ----
-    unsigned long long top = 0;
-    ECK(cudaMemcpyAsync(&top, job.rec_top, 8, cudaMemcpyDeviceToHost, st));
-    RCK(B.h_n.ensure(nn * 4));
-    RCK(B.h_off.ensure((nn + 1) * 8));
-    RCK(B.h_pops.ensure(nn * 8));
-    RCK(B.h_trace.ensure(nn * 8));
-    ECK(cudaMemcpyAsync(B.h_n.p, job.out_n, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
-    ECK(cudaMemcpyAsync(B.h_off.p, job.out_off, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
-    ECK(cudaMemcpyAsync(B.h_pops.p, job.out_pops, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
-    ECK(cudaMemcpyAsync(B.h_trace.p, job.out_trace, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
-    if (ix->keep_stats) {
-        S.fetch.resize(nn);
-        S.tier_of.resize(nn);
-        ECK(cudaMemcpyAsync(S.fetch.data(), job.out_fetch, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
-        ECK(cudaMemcpyAsync(S.tier_of.data(), job.out_tier, (size_t)n, cudaMemcpyDeviceToHost, st));
+    // ---- results: put in read order on the device, then one copy of each array into the caller's results ----
+    S.ms_phase[1] = now_ms() - t_start;
+    RCK(B.rec_off.ensure((nn + 1) * 8));
+    RCK(B.rec_ord.ensure((size_t)std::max<int64_t>(job.rec_cap, 1) * 24));
+    RCK(B.tile.ensure(order_tile_bytes(n)));
+    RCK(dev_order_results(job, n, (int64_t *)B.rec_off.p, (uint64_t *)B.rec_ord.p, (int64_t *)B.tile.p, st));
+    int64_t *h_total = (int64_t *)B.h_misc.p + 4;
+    *h_total = 0;
+    if (n > 0) ECK(cudaMemcpyAsync(h_total, (int64_t *)B.rec_off.p + n, 8, cudaMemcpyDeviceToHost, st));
+    ECK(cudaStreamSynchronize(st));
+    const int64_t n_rec = *h_total;
+    if (n_rec < 0 || n_rec > job.rec_cap) return GALN_ECUDA;
+    auto *P = new ResultsPriv();
+    P->n_aln.resize(nn);
+    P->rec_off.resize(nn + 1);
+    P->rec.resize((size_t)std::max<int64_t>(n_rec, 1));
+    P->pops.resize(nn);
+    P->trace.resize(nn);
+    P->rec_off[0] = 0;
+    cudaError_t ce = cudaSuccess;
+    if (n > 0) {
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(P->n_aln.data(), job.out_n, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(P->rec_off.data(), B.rec_off.p, ((size_t)n + 1) * 8, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess && n_rec)
+            ce = cudaMemcpyAsync(P->rec.data(), B.rec_ord.p, (size_t)n_rec * 24, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(P->pops.data(), job.out_pops, (size_t)n * 8, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(P->trace.data(), job.out_trace, (size_t)n * 8, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess && ix->keep_stats) {
+            S.fetch.resize(nn);
+            S.tier_of.resize(nn);
+            ce = cudaMemcpyAsync(S.fetch.data(), job.out_fetch, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(S.tier_of.data(), job.out_tier, (size_t)n, cudaMemcpyDeviceToHost, st);
+        }
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
     }
-    ECK(cudaStreamSynchronize(st));
-    top = std::min<unsigned long long>(top, (unsigned long long)job.rec_cap);
-    RCK(B.h_rec.ensure((size_t)std::max<unsigned long long>(top, 1) * 24));
-    if (top) ECK(cudaMemcpyAsync(B.h_rec.p, job.out_rec, (size_t)top * 24, cudaMemcpyDeviceToHost, st));
-    ECK(cudaStreamSynchronize(st));
-    results_fill(out, n, (const int32_t *)B.h_n.p, (const int64_t *)B.h_off.p, (const uint64_t *)B.h_rec.p,
-                 (const uint64_t *)B.h_pops.p, (const uint64_t *)B.h_trace.p);
+    if (ce != cudaSuccess) {
+        delete P;
+        fprintf(stderr, "[galn] CUDA error %s copying results\n", cudaGetErrorString(ce));
+        return GALN_ECUDA;
+    }
+    P->publish(out, n);
+    S.ms_phase[2] = now_ms() - t_start;
     S.ms_kernels = k_ms;
     S.ms_total = now_ms() - t_start;
     return 0;
@@ -555,6 +589,16 @@ extern "C" int galn_last_graph_launches(galn_index *ix, int64_t *graph_launches)
     if (!ix || !graph_launches) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
     *graph_launches = ix->main.last.graph_launches;
+    return 0;
+}
+
+extern "C" int galn_last_run_phases(galn_index *ix, double *ms, int n)
+{
+    if (!ix || !ms || n < 0) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    const galn::RunStats &S = ix->main.last;
+    const double v[5] = {S.ms_phase[0], S.ms_phase[1], S.ms_phase[2], S.ms_total, S.ms_device};
+    for (int q = 0; q < n && q < 5; ++q) ms[q] = v[q];
     return 0;
 }
 

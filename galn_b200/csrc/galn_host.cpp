@@ -346,34 +346,6 @@ extern "C" int galn_index_info(const galn_index *ix, uint64_t *seq_len, uint64_t
 // ---------------------------------------------------------------------------------------------------
 // results and .sai
 
-void galn::results_fill(galn_results *out, int n, const int32_t *n_aln, const int64_t *dev_off,
-                        const uint64_t *rec_words, const uint64_t *pops, const uint64_t *trace)
-{
-    auto *P = new ResultsPriv();
-    P->n_aln.assign(n_aln, n_aln + n);
-    P->pops.assign(pops, pops + n);
-    P->trace.assign(trace, trace + n);
-    P->rec_off.resize((size_t)n + 1);
-    int64_t t = 0;
-    for (int r = 0; r < n; ++r) {
-        P->rec_off[r] = t;
-        if (n_aln[r] > 0) t += n_aln[r];
-    }
-    P->rec_off[n] = t;
-    P->rec.resize((size_t)std::max<int64_t>(t, 1));
-    for (int r = 0; r < n; ++r) {
-        if (n_aln[r] <= 0) continue;
-        memcpy(&P->rec[P->rec_off[r]], rec_words + 3 * dev_off[r], (size_t)n_aln[r] * sizeof(galn_aln1));
-    }
-    out->n_reads = n;
-    out->n_aln = P->n_aln.data();
-    out->rec_offset = P->rec_off.data();
-    out->rec = P->rec.data();
-    out->n_pops = P->pops.data();
-    out->trace = P->trace.data();
-    out->_priv = P;
-}
-
 extern "C" int galn_results_free(galn_results *res)
 {
     if (!res) return GALN_EINVAL;

@@ -40,7 +40,7 @@ struct Buf {
 // every buffer one search job uses, kept across calls on the same index (calls are serialised)
 struct JobBufs {
     Buf seq, query, off, bidx, maxdiff, bopt, out_n, out_off, out_pops, out_trace, out_peak, out_fetch, out_tier,
-        out_rec, rec_top, list_a, list_b, counters, ws, dbg;
+        out_rec, rec_top, list_a, list_b, counters, ws, dbg, rec_off, rec_ord, tile;
     Buf h_n, h_off, h_pops, h_trace, h_rec, h_list, h_misc;
     JobBufs()
     {
@@ -49,8 +49,8 @@ struct JobBufs {
     void release()
     {
         Buf *all[] = {&seq, &query, &off, &bidx, &maxdiff, &bopt, &out_n, &out_off, &out_pops, &out_trace, &out_peak,
-                      &out_fetch, &out_tier, &dbg, &out_rec, &rec_top, &list_a, &list_b, &counters, &ws, &h_n, &h_off, &h_pops, &h_trace, &h_rec,
-                      &h_list, &h_misc};
+                      &out_fetch, &out_tier, &dbg, &out_rec, &rec_top, &list_a, &list_b, &counters, &ws, &rec_off,
+                      &rec_ord, &tile, &h_n, &h_off, &h_pops, &h_trace, &h_rec, &h_list, &h_misc};
         for (Buf *b : all) b->release();
     }
 };
@@ -58,6 +58,7 @@ struct JobBufs {
 // statistics of the last run (for benchmarks and tests)
 struct RunStats {
     double ms_total = 0, ms_kernels = 0, ms_device = 0;
+    double ms_phase[4] = {0, 0, 0, 0};   // host time from the call's start to: the first launch, the device's end, results ready
     double ms_tier[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int tiers = 0;
     int64_t overflow_reads[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -109,14 +110,38 @@ struct galn_index {
 namespace galn {
 uint64_t opts_key(const galn_opts *o);
 // what galn_results._priv owns
-struct ResultsPriv {
-    std::vector<int32_t> n_aln;
-    std::vector<int64_t> rec_off;
-    std::vector<galn_aln1> rec;
-    std::vector<uint64_t> pops, trace;
+// A vector whose resize leaves new elements uninitialised (results are overwritten by a device copy at once).
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind { using other = NoInitAlloc<U>; };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U> &) {}
+    template <class U>
+    void construct(U *p) noexcept { ::new ((void *)p) U; }
+    template <class U, class... A>
+    void construct(U *p, A &&...a) { ::new ((void *)p) U(std::forward<A>(a)...); }
 };
-void results_fill(galn_results *out, int n, const int32_t *n_aln, const int64_t *dev_off, const uint64_t *rec_words,
-                  const uint64_t *pops, const uint64_t *trace);
+template <class T>
+using hvec = std::vector<T, NoInitAlloc<T>>;
+
+struct ResultsPriv {
+    hvec<int32_t> n_aln;
+    hvec<int64_t> rec_off;
+    hvec<galn_aln1> rec;
+    hvec<uint64_t> pops, trace;
+    void publish(galn_results *out, int n)
+    {
+        out->n_reads = n;
+        out->n_aln = n_aln.data();
+        out->rec_offset = rec_off.data();
+        out->rec = rec.data();
+        out->n_pops = pops.data();
+        out->trace = trace.data();
+        out->_priv = this;
+    }
+};
 int run_job(galn_index *ix, ExecCtx &ctx, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);
 int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_sets, const int32_t *batch_set,
                   const galn_reads *in, int engine, galn_results *out);

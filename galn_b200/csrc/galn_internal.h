@@ -97,9 +97,13 @@ struct WarpCfg {
 size_t warp_smem_bytes();
 int warp_resident(int device);
 size_t warp_ws_bytes(const WarpCfg &c, int n);
-constexpr int kWarpDbg = 14;   // counters of the warp tier when profiling is on
+constexpr int kWarpDbg = 15;   // counters of the warp tier when profiling is on
 int dev_search_warp(const DevIndex &ix, DevJob &job, const WarpCfg &c, int tier, const int32_t *list, int n,
                     int32_t *ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg);
+// Results in read order: rec_off[0..n] (exclusive scan of max(out_n, 0)) and the records gathered from
+// out_rec into rec_ord; tile_sum holds order_tile_bytes(n) bytes of scratch. Three kernels on st.
+int dev_order_results(const DevJob &job, int n, int64_t *rec_off, uint64_t *rec_ord, int64_t *tile_sum, cudaStream_t st);
+size_t order_tile_bytes(int n);
 // the queue in ws_mem: control words (0 head, 1 tail, 2 small warps finished, 3 a slot was lost) and slots
 int32_t *warp_queue(const WarpCfg &c, int n, void *ws_mem, int32_t **slots);
 

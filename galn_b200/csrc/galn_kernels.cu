@@ -330,6 +330,110 @@ int warp_resident(int device)
     return bps * sms;
 }
 
+// ---- results in read order ----
+// Records are appended to out_rec in the order reads finish (an atomic counter per record block); the caller
+// wants them in read order. An exclusive scan of max(n_aln, 0) gives each read's first record in read order;
+// the last kernel adds the block prefixes and gathers each read's records there.
+constexpr int kScanThreads = 1024, kScanItems = 4, kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t *sm, int64_t &total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int64_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sm[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int64_t s = lane < kScanThreads / 32 ? sm[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        sm[lane] = s;     // inclusive prefix of warp sums
+    }
+    __syncthreads();
+    total = sm[kScanThreads / 32 - 1];
+    const int64_t before = w ? sm[w - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+// per tile: local exclusive offsets into rec_off[], tile sums into tile_sum[]
+__global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const int32_t *n_aln, int n, int64_t *rec_off,
+                                                                  int64_t *tile_sum)
+{
+    __shared__ int64_t sm[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int64_t v[kScanItems], s = 0;
+#pragma unroll
+    for (int u = 0; u < kScanItems; ++u) {
+        const int64_t r = base + u;
+        v[u] = r < n ? (int64_t)max(n_aln[r], 0) : 0;
+        s += v[u];
+    }
+    int64_t total;
+    int64_t off = block_excl_scan(s, sm, total);
+#pragma unroll
+    for (int u = 0; u < kScanItems; ++u) {
+        const int64_t r = base + u;
+        if (r < n) rec_off[r] = off;
+        off += v[u];
+    }
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
+}
+
+// exclusive scan of the tile sums, in one block; the grand total goes to rec_off[n]
+__global__ void __launch_bounds__(kScanThreads) scan_sums_kernel(int64_t *tile_sum, int n_tiles, int64_t *rec_off, int n)
+{
+    __shared__ int64_t sm[32];
+    int64_t carry = 0;
+    for (int t0 = 0; t0 < n_tiles; t0 += kScanThreads) {
+        const int t = t0 + threadIdx.x;
+        const int64_t v = t < n_tiles ? tile_sum[t] : 0;
+        int64_t total;
+        const int64_t e = block_excl_scan(v, sm, total);
+        if (t < n_tiles) tile_sum[t] = carry + e;
+        carry += total;
+    }
+    if (threadIdx.x == 0) rec_off[n] = carry;
+}
+
+// add the tile prefix; copy each read's records (3 words each) to their place in read order
+__global__ void __launch_bounds__(kScanThreads) gather_records_kernel(const int32_t *n_aln, const int64_t *dev_off,
+                                                                      const uint64_t *rec, int n, int64_t *rec_off,
+                                                                      const int64_t *tile_sum, uint64_t *rec_ord)
+{
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    const int64_t add = tile_sum[blockIdx.x];
+#pragma unroll
+    for (int u = 0; u < kScanItems; ++u) {
+        const int64_t r = base + u;
+        if (r >= n) break;
+        const int64_t o = rec_off[r] + add;
+        rec_off[r] = o;
+        const int k = n_aln[r];
+        for (int j = 0; j < 3 * k; ++j) rec_ord[3 * o + j] = rec[3 * dev_off[r] + j];
+    }
+}
+
+int dev_order_results(const DevJob &job, int n, int64_t *rec_off, uint64_t *rec_ord, int64_t *tile_sum, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    const int tiles = (int)(((int64_t)n + kScanTile - 1) / kScanTile);
+    scan_tiles_kernel<<<tiles, kScanThreads, 0, st>>>(job.out_n, n, rec_off, tile_sum);
+    scan_sums_kernel<<<1, kScanThreads, 0, st>>>(tile_sum, tiles, rec_off, n);
+    gather_records_kernel<<<tiles, kScanThreads, 0, st>>>(job.out_n, job.out_off, job.out_rec, n, rec_off, tile_sum, rec_ord);
+    GALN_CUDA(cudaGetLastError());
+    return 0;
+}
+
+size_t order_tile_bytes(int n) { return ((size_t)std::max(n, 1) + kScanTile - 1) / kScanTile * 8 + 8; }
+
 // workspace layout of the warp tier, in order
 struct WarpLayout {
     size_t chunks, chunk_prev, free_ids, aln, stage, prec, side, q_ctl, ovq, total;

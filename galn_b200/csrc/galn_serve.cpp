@@ -50,9 +50,9 @@ struct Request {
     int n = 0, next = 0, done_reads = 0;
     std::vector<Chunk> chunks;         // finished pieces, in any order
     // results, in read order (assembled when the last piece is done)
-    std::vector<int32_t> n_aln;
-    std::vector<galn_aln1> rec;
-    std::vector<uint64_t> pops, trace;
+    galn::hvec<int32_t> n_aln;
+    galn::hvec<galn_aln1> rec;
+    galn::hvec<uint64_t> pops, trace;
     double t_submit = 0, t_done = 0;
     int rc = 0;
     bool done = false;

@@ -45,7 +45,7 @@ constexpr int kWCH = 32;         // entries per chunk
 constexpr int kWNewC = (kWCH + 32 * kWL) / kWCH + 2;   // chunks one commit may allocate
 constexpr int kWGrabPops = 6;    // an idle lane takes an entry only with room for this many pops
 
-constexpr int kWDbgN = 14;       // optional counters per read (the kDbg* list below)
+constexpr int kWDbgN = 15;       // optional counters per read (the kDbg* list below)
 
 struct WarpSmem {
     int32_t top_chunk[kWMaxB];
@@ -123,7 +123,7 @@ struct WArgs {
 
 // optional counters of the warp tier (per launch, summed over warps)
 enum { kDbgReads, kDbgWaves, kDbgLanes, kDbgConsumed, kDbgPops, kDbgCont, kDbgHazard, kDbgCycChain,
-       kDbgCycReplay, kDbgCycCommit, kDbgCycLoad, kDbgChainPops, kDbgCycRead, kDbgCycReadMax, kWDbg };
+       kDbgCycReplay, kDbgCycCommit, kDbgCycLoad, kDbgChainPops, kDbgCycRead, kDbgSteps, kDbgCycReadMax, kWDbg };
 static_assert(kWDbg == kWDbgN, "counter list");
 
 // profiling helpers: lane 0 keeps the read's counters in shared memory
@@ -556,6 +556,7 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
                     e_next = min(limit, e_next + __popc(wb));
                 }
                 if (!__any_sync(FULL, ce >= 0)) break;
+                WDBG_ADD(kDbgSteps, 1);
                 int stop_e = 0x7fffffff;
                 if (ce >= 0) {
                     uint32_t mt = 0;

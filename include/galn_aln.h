@@ -207,10 +207,16 @@ int galn_autotune_clear(galn_index *ix);
 /* How many of the last run's kernel launches went through a CUDA graph (no reference counterpart). */
 int galn_last_graph_launches(galn_index *ix, int64_t *graph_launches);
 
-/* Counters of the warp tier in the last keep_stats run (no reference counterpart): reads, waves, lanes
- * given entries, lanes replayed, pops, chains continued, hits, SM cycles in chains / replay / commit /
- * wave loads (summed over warps), pops run speculatively. */
+/* Counters of the warp tier in the last keep_stats run (no reference counterpart): reads searched (with
+ * re-runs), waves, entries expanded, entries replayed, pops, chains continued in the next wave, hits, SM
+ * cycles in chains / replay / commit / wave loads (summed over warps), pops run (with dropped
+ * speculation), SM cycles inside reads, chain steps, the longest read's SM cycles. */
 int galn_last_warp_counters(galn_index *ix, uint64_t *counters, int n);
+
+/* Host-side timeline of the last run (no reference counterpart), up to n of: ms from the call's start to
+ * the first kernel launch, to the end of the device work, to the results being ready; the call's total
+ * ms; the device span in ms. */
+int galn_last_run_phases(galn_index *ix, double *ms, int n);
 
 /* Tier capacities (no reference counterpart; set by the autotuner): entries and records per thread in the
  * first tier, its block size (64/128/256/512), live entries and records per thread in the second tier, and
