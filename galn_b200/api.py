@@ -152,6 +152,11 @@ class Index:
         if lib().galn_index_set_warp_tier(self.h, int(on), arena_chunks):
             raise GalnError("bad warp tier setting")
 
+    def set_l2_persist(self, on: bool):
+        """Keep the occurrence blocks in a persisting L2 window (on by default)."""
+        if lib().galn_index_set_l2_persist(self.h, int(on)):
+            raise GalnError("bad L2 setting")
+
     def warp_counters(self) -> dict:
         v = np.zeros(15, np.uint64)
         lib().galn_last_warp_counters(self.h, v.ctypes.data, 15)

@@ -610,6 +610,16 @@ extern "C" int galn_last_warp_counters(galn_index *ix, uint64_t *counters, int n
     return 0;
 }
 
+extern "C" int galn_index_set_l2_persist(galn_index *ix, int on)
+{
+    if (!ix) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    ix->l2_persist = on != 0;
+    if (ix->l2_persist) galn::index_l2_policy(ix, ix->stream);
+    else galn::index_l2_clear(ix, ix->stream);
+    return 0;
+}
+
 extern "C" int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks)
 {
     if (!ix || arena_chunks < 64) return GALN_EINVAL;

@@ -283,8 +283,41 @@ static galn_index *index_from_words(const uint64_t hdr[5], const uint32_t *body,
         if (err) *err = rc;
         return nullptr;
     }
+    galn::index_l2_policy(ix, ix->stream);
     if (err) *err = 0;
     return ix;
+}
+
+// Keep the occurrence blocks in L2: a persisting access-policy window over them on every stream that
+// searches (the set-aside is a limit of this process's context and ends with it). The search reads the
+// index at random on every step, while stack pushes and pops stream through; without the window the
+// stream evicts the index.
+void galn::index_l2_policy(galn_index *ix, cudaStream_t st)
+{
+    if (!ix->l2_persist || !ix->dev.blocks) return;
+    int maxw = 0, maxp = 0;
+    cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, ix->dev.device);
+    cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, ix->dev.device);
+    if (maxw <= 0 || maxp <= 0) return;
+    const size_t bytes = std::min<size_t>((size_t)ix->dev.n_blocks * 32, (size_t)maxw);
+    const size_t persist = std::min<size_t>(bytes, (size_t)maxp);
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist) != cudaSuccess) { cudaGetLastError(); return; }
+    cudaStreamAttrValue v;
+    memset(&v, 0, sizeof(v));
+    v.accessPolicyWindow.base_ptr = ix->dev.blocks;
+    v.accessPolicyWindow.num_bytes = bytes;
+    v.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)persist / (double)bytes);
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    if (cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &v) != cudaSuccess) cudaGetLastError();
+}
+
+void galn::index_l2_clear(galn_index *ix, cudaStream_t st)
+{
+    cudaStreamAttrValue v;
+    memset(&v, 0, sizeof(v));
+    v.accessPolicyWindow.num_bytes = 0;
+    if (cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &v) != cudaSuccess) cudaGetLastError();
 }
 
 extern "C" galn_index *galn_index_open(const char *prefix, int device, int *err)

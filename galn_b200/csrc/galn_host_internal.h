@@ -105,6 +105,7 @@ struct galn_index {
     bool tune_active = false;           // the autotuner is timing a candidate: ignore the table
     bool use_graph = true;              // launch the persistent first tier through a CUDA graph
     int warp_arena = 1 << 14;           // 32-entry chunks per warp
+    bool l2_persist = true;             // the occurrence blocks in a persisting L2 window
 };
 
 namespace galn {
@@ -142,6 +143,8 @@ struct ResultsPriv {
         out->_priv = this;
     }
 };
+void index_l2_policy(galn_index *ix, cudaStream_t st);
+void index_l2_clear(galn_index *ix, cudaStream_t st);
 int run_job(galn_index *ix, ExecCtx &ctx, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);
 int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_sets, const int32_t *batch_set,
                   const galn_reads *in, int engine, galn_results *out);

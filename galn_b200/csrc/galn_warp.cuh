@@ -44,6 +44,8 @@ constexpr int kWL = 128;         // staged pushes per lane and target list per w
 constexpr int kWCH = 32;         // entries per chunk
 constexpr int kWNewC = (kWCH + 32 * kWL) / kWCH + 2;   // chunks one commit may allocate
 constexpr int kWGrabPops = 6;    // an idle lane takes an entry only with room for this many pops
+constexpr int kWChain = kWE / kWCH + 2;   // chunks of the current bucket kept walked
+constexpr int kFC = 64;          // free chunk ids kept in shared memory
 
 constexpr int kWDbgN = 15;       // optional counters per read (the kDbg* list below)
 
@@ -61,7 +63,8 @@ struct WarpSmem {
     uint32_t e_a[kWE];                // per entry: net change of n_entries (signed, bits 0-15), its highest value before a pop (16-31)
     uint32_t e_b[kWE];                // per entry: highest value after a pop (bits 0-15), index blocks read (16-31)
     int32_t newc[kWNewC];             // chunks allocated for one commit
-    int32_t wch[kWE / kWCH + 2];      // chunks of bucket b holding the wave's entries, top first
+    int32_t wch[kWChain];             // the current bucket's chunks from its top, as far as walked
+    int32_t fcache[kFC];              // the top of the warp's free-chunk stack
     BatchOpt O;                       // the read's batch options (read from here, not held in registers)
     unsigned long long dv[kWDbgN];    // optional counters of this read (profiling runs)
     long long t_mark, t_read;
@@ -352,33 +355,43 @@ __device__ __forceinline__ int lane_step(const IndexView &ix, const BatchOpt &O,
     return endc;
 }
 
-// the warp's chunk allocator (warp-uniform state; every lane holds the same copy)
+// the warp's chunk allocator (warp-uniform state; every lane holds the same copy): a stack of free chunk
+// ids whose top kFC entries live in shared memory (fc), the rest in global memory, then fresh chunks
 struct WAlloc {
     int32_t *free_ids;
-    int base, cap, bump, free_top;
+    int32_t *fc;
+    int base, cap, bump, g_top, fc_n;
     // `need` chunk ids into out[0..need), lane-parallel; false if the arena is exhausted
     __device__ __forceinline__ bool alloc_n(int need, int32_t *out, int lane)
     {
-        bool ok = true;
-        for (int t0 = 0; t0 < need; t0 += 32) {
-            int t = t0 + lane;
-            if (t < need) {
-                int id;
-                if (t < free_top) id = free_ids[free_top - 1 - t];
-                else id = bump + (t - free_top) < cap ? base + bump + (t - free_top) : -1;
-                out[t] = id;
-            }
+        const int from_c = need < fc_n ? need : fc_n;
+        const int from_g = need - from_c < g_top ? need - from_c : g_top;
+        const int from_b = need - from_c - from_g;
+        if (bump + from_b > cap) return false;
+        for (int t = lane; t < need; t += 32) {
+            int id;
+            if (t < from_c) id = fc[fc_n - 1 - t];
+            else if (t < from_c + from_g) id = free_ids[g_top - 1 - (t - from_c)];
+            else id = base + bump + (t - from_c - from_g);
+            out[t] = id;
         }
-        int from_free = need < free_top ? need : free_top;
-        if (bump + (need - from_free) > cap) ok = false;
-        else { free_top -= from_free; bump += need - from_free; }
+        fc_n -= from_c; g_top -= from_g; bump += from_b;
         __syncwarp();
-        return ok;
+        return true;
     }
     __device__ __forceinline__ void release(int id, int lane)
     {
-        if (lane == 0) free_ids[free_top] = id;
-        ++free_top;
+        static_assert(kFC == 64, "spill layout");
+        if (fc_n == kFC) {   // the cache's lower half to the global stack
+            free_ids[g_top + lane] = fc[lane];
+            const int v = fc[lane + 32];
+            __syncwarp();
+            fc[lane] = v;
+            g_top += 32; fc_n -= 32;
+        }
+        if (lane == 0) fc[fc_n] = id;
+        ++fc_n;
+        __syncwarp();
     }
 };
 
@@ -428,7 +441,8 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
         const int64_t base = big ? (int64_t)wid * a.big_chunks
                                  : (int64_t)a.n_big * a.big_chunks + (int64_t)(wid - a.n_big) * a.arena_chunks;
         A.free_ids = a.free_ids + base;
-        A.base = (int)base; A.cap = big ? a.big_chunks : a.arena_chunks; A.bump = 0; A.free_top = 0;
+        A.fc = S->fcache;
+        A.base = (int)base; A.cap = big ? a.big_chunks : a.arena_chunks; A.bump = 0; A.g_top = 0; A.fc_n = 0;
     }
     uint4 *stage_w = a.stage + (size_t)wid * 3 * 32 * kWL;          // list L of lane j at + L * 32 * kWL + j * kWL
     uint4 *stage_lane = stage_w + (size_t)lane * kWL;
@@ -470,6 +484,7 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
         px.state = kStM;
         if (n_stacks <= 0) { ret = kErrScore; goto publish; }
         n_entries = 1; peak = 1;
+        int wch_b = -1, wch_n = 0;   // bucket whose chunk chain S->wch holds, and its length
         for (;;) {
             if (n_entries == 0) break;
             if (n_entries > O.max_entries) break;
@@ -498,19 +513,27 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
             // the wave's entries, in pop order: the pending child (if any), then bucket b from the top
             const int navail = pend_i + S->n_in[b];
             const int Wcap = navail < kWE ? navail : kWE;
-            int walk_ok = 1;
+            // the bucket's chunks down to the wave's last entry; bucket b gets no pushes while it is popped,
+            // so the chain walked for earlier waves of b is still valid below its top
+            if (b != wch_b) { wch_b = b; wch_n = 0; }
+            int walk_ok = 1, k = wch_n;
             if (lane == 0) {
-                int ch = S->top_chunk[b], k = 0, cov = 0;
                 const int need = Wcap - pend_i;
-                while (cov < need) {
-                    if (ch < 0 || k >= kWE / kWCH + 2) { walk_ok = 0; break; }
-                    S->wch[k] = ch;
-                    cov += k == 0 ? S->top_cnt[b] : kWCH;
-                    ++k;
-                    if (cov < need) ch = a.chunk_prev[ch];
+                if (k == 0 && need > 0) {
+                    if (S->top_chunk[b] < 0) walk_ok = 0;
+                    else { S->wch[0] = S->top_chunk[b]; k = 1; }
+                }
+                int cov = k ? S->top_cnt[b] + (k - 1) * kWCH : 0;
+                while (walk_ok && cov < need) {
+                    if (k >= kWChain) { walk_ok = 0; break; }
+                    const int nx = a.chunk_prev[S->wch[k - 1]];
+                    if (nx < 0) { walk_ok = 0; break; }
+                    S->wch[k++] = nx;
+                    cov += kWCH;
                 }
             }
             walk_ok = __shfl_sync(FULL, walk_ok, 0);
+            wch_n = __shfl_sync(FULL, k, 0);
             if (!walk_ok) { ret = kErrStack; break; }
             __syncwarp();
             {
@@ -738,16 +761,20 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
             // take the consumed entries off bucket b (entry 0 may have been the pending child)
             const int C = consumed - pend_i;
             if (C > 0) {
-                int tc = S->top_chunk[b], cnt = S->top_cnt[b], left = C;
-                __syncwarp();
-                while (tc >= 0 && left >= cnt) {
-                    left -= cnt;
-                    const int pc = a.chunk_prev[tc];
-                    A.release(tc, lane);
-                    tc = pc;
-                    cnt = kWCH;
-                }
+                // whole chunks emptied: wch[0..j); the new top is wch[j], or the chunk below the last walked one
+                int cnt = S->top_cnt[b], left = C, j = 0;
+                while (j < wch_n && left >= cnt) { left -= cnt; ++j; cnt = kWCH; }
+                const int tc = j < wch_n ? S->wch[j] : (j > 0 ? a.chunk_prev[S->wch[j - 1]] : S->top_chunk[b]);
                 if (tc < 0 && left > 0) { ret = kErrStack; break; }
+                for (int t = 0; t < j; ++t) A.release(S->wch[t], lane);
+                // drop them from the kept chain
+                const int keep = wch_n - j;
+                const int v = lane < keep ? S->wch[j + lane] : 0;
+                __syncwarp();
+                if (j > 0) {
+                    if (keep > 0) { if (lane < keep) S->wch[lane] = v; wch_n = keep; }
+                    else { if (lane == 0 && tc >= 0) S->wch[0] = tc; wch_n = tc >= 0 ? 1 : 0; }
+                }
                 if (lane == 0) {
                     S->top_chunk[b] = tc;
                     S->top_cnt[b] = (uint16_t)(tc >= 0 ? cnt - left : 0);

@@ -227,6 +227,10 @@ int galn_index_set_tuning(galn_index *ix, int t0_cap, int t0_aln, int t0_block, 
  * counterpart; on by default with 16384 chunks). Results never depend on it. */
 int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks);
 
+/* The occurrence blocks in a persisting L2 access-policy window on the index's streams (no reference
+ * counterpart; on by default; results never depend on it). */
+int galn_index_set_l2_persist(galn_index *ix, int on);
+
 /* Trace hashes on or off (on by default). The reference computes them only in its --verify mode
  * (gapw_kernel<TRACE>, src/gapw.cuh:716-795); off, the kernels skip the hash and results carry 0 in
  * trace[]. n_aln, records and n_pops are unaffected. */
