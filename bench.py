@@ -13,7 +13,8 @@ table. The L2 cache is flushed (a 512 MB write) before each step, outside the ti
   value   reads / device span (first to last search kernel, CUDA events on the library's stream): inputs
           already in HBM
   e2e     reads / wall time of the whole call (H2D + device + D2H + result assembly)
-  roofline  the dominant kernel (first search tier): 32 B x its algorithmic block fetches / its time
+  roofline  the dominant kernel (the tier with the most device time): 32 B x the algorithmic block fetches
+          of the reads it finished / its time; also against the device's random 32-B gather peak
   cpu_baseline  the reference's own `galn aln --cpu-only` on a sample of the same reads, all host cores
 
 --impl reference times only the reference's CPU path (rank 0; other ranks exit at once).
@@ -21,6 +22,7 @@ table. The L2 cache is flushed (a 512 MB write) before each step, outside the ti
 from __future__ import annotations
 
 import argparse
+import ctypes
 import datetime
 import hashlib
 import json
@@ -35,6 +37,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "reads/s, .sai md5-identical (served vs plain launch, same B200); p50/p99 latency"
+TIER_NAMES = {0: "search tier 0 (thread per read, persistent claim, CUDA graph)",
+              1: "warp tier (one warp per heavy read, entries of a score bucket spread over lanes)",
+              2: "thread tiers (free-list stacks up to the max_entries cut-off)"}
 WORKLOAD_DESC = {
     "adna": "aDNA batched: 100 Mbp reference (45% GC, 10 contigs, 5% repeats), 2,000,000 reads per GPU, "
             "log-normal 25-120 bp, deaminated, 3% random; -l 1024 -n 0.01 -o 2",
@@ -272,7 +277,9 @@ def main():
         if world > 1:
             dist.barrier()
 
-    def run_steps(eng, k, w):
+    tier_ms_steps = []
+
+    def run_steps(eng, k, w, keep_tiers=False):
         md5 = set()
         e2e, dev, tier0, launches = [], [], [], 0
         for i in range(w + k):
@@ -287,6 +294,8 @@ def main():
                 e2e.append(dt)
                 dev.append(prof["ms_device"] / 1e3)
                 tier0.append(prof["ms_tier"][0] / 1e3)
+                if keep_tiers:
+                    tier_ms_steps.append(list(prof["ms_tier"]))
                 launches += st["launches"]
                 md5.add(hashlib.md5(res.sai_bytes()).hexdigest())
         return e2e, dev, tier0, launches, md5, res
@@ -302,7 +311,7 @@ def main():
     torch.cuda.synchronize()
     cpath = os.path.join(d, f"clocks_{rank}.csv")
     proc, cf = clock_sampler_start(cpath, local)
-    e2e, dev, tier0, launches, md5, res = run_steps(engine, args.steps, 0)
+    e2e, dev, tier0, launches, md5, res = run_steps(engine, args.steps, 0, keep_tiers=True)
     torch.cuda.synchronize()
     barrier()
     clocks = clock_sampler_stop(proc, cf, cpath)
@@ -330,11 +339,22 @@ def main():
                   "threads": prof["tier_threads"],
                   "fetches_finished": [int(prof["fetch"][prof["tier"] == t].astype(np.int64).sum()) for t in range(8)]}
     tiers_info["warp_counters"] = ix.warp_counters()
-    fetch_t0 = int(prof["fetch"][prof["tier"] == 0].astype(np.int64).sum())
     fetch_all = int(prof["fetch"].astype(np.int64).sum())
     ix.set_tuning(t0_cap=args.t0_cap, keep_stats=False)
     peak, peak_kind = peaks()
-    achieved = 32.0 * fetch_t0 / t0_s / 1e9
+    # the dominant kernel: the tier with the most device time per step (timed steps); its algorithmic bytes
+    # are 32 B x the block fetches of the reads it finished
+    tier_ms = [statistics.mean(col) for col in zip(*tier_ms_steps)]
+    dom = max(range(len(tier_ms)), key=lambda t: tier_ms[t])
+    dom_s = tier_ms[dom] / 1e3
+    fetch_dom = tiers_info["fetches_finished"][dom]
+    achieved = 32.0 * fetch_dom / dom_s / 1e9
+    def gather_peak(nbytes):
+        g = ctypes.c_double(0)
+        rc_ = galn_b200.lib().galn_gather_peak(local, ctypes.c_uint64(nbytes), 5, ctypes.byref(g))
+        return g.value if rc_ == 0 else None
+    gather_gbs = gather_peak(4 << 30)          # HBM: a buffer 32x the L2
+    gather_l2_gbs = gather_peak(32 << 20)      # L2: a buffer a quarter of it
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
@@ -378,9 +398,15 @@ def main():
         "e2e": {"value": total_reads / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "search tier 0 (thread per read, persistent claim)",
-                     "algorithmic_bytes_per_launch": 32 * fetch_t0, "fetches_all_tiers": fetch_all,
-                     "ms_per_launch": 1e3 * t0_s},
+                     "kernel": TIER_NAMES[min(dom, 2)],
+                     "algorithmic_bytes_per_launch": 32 * fetch_dom, "fetches_all_tiers": fetch_all,
+                     "ms_per_launch": 1e3 * dom_s,
+                     "gather_peak_gbs": gather_gbs,
+                     "frac_of_gather_peak": achieved / gather_gbs if gather_gbs else None,
+                     "gather_l2_peak_gbs": gather_l2_gbs,
+                     "frac_of_gather_l2_peak": achieved / gather_l2_gbs if gather_l2_gbs else None,
+                     "gather_peak_how": "galn_gather_peak: random 32-B sectors of a 4 GiB buffer (HBM) and of a "
+                                        "32 MiB buffer (L2), best of 5 launches each"},
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,

@@ -330,6 +330,75 @@ int warp_resident(int device)
     return bps * sms;
 }
 
+// ---- random 32-byte gather peak (a measurement, not part of the search) ----
+// Every thread reads `per_thread` 32-byte sectors at pseudo-random sector indices of a power-of-two buffer
+// (a splitmix64 sequence per thread; independent loads, several in flight), and folds them into one word so
+// the loads are not dead. Bytes read / time is the device's random-sector read rate for that buffer size.
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+__global__ void __launch_bounds__(256) gather_kernel(const uint4 *buf, uint64_t sector_mask, int per_thread, uint32_t *sink)
+{
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t acc = 0;
+    constexpr int kInFlight = 8;
+    for (int i = 0; i < per_thread; i += kInFlight) {
+        uint4 a[kInFlight], b[kInFlight];
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) {
+            const uint64_t sct = mix64(tid * 0x100000001b3ull + (uint64_t)(i + u)) & sector_mask;
+            a[u] = __ldcg(buf + 2 * sct);
+            b[u] = __ldcg(buf + 2 * sct + 1);
+        }
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) acc ^= a[u].x ^ a[u].w ^ b[u].y ^ b[u].z;
+    }
+    if (acc == 0x9e3779b9u) sink[0] = acc;   // practically never; keeps the loads
+}
+
+extern "C" int galn_gather_peak(int device, uint64_t bytes, int repeats, double *gbs)
+{
+    if (!gbs || bytes < (1u << 20) || repeats < 1) return -20;
+    while (bytes & (bytes - 1)) bytes &= bytes - 1;      // the largest power of two not above it
+    if (cudaSetDevice(device) != cudaSuccess) return -22;
+    void *buf = nullptr, *sink = nullptr;
+    if (cudaMalloc(&buf, bytes) != cudaSuccess) { cudaGetLastError(); return -23; }
+    if (cudaMalloc(&sink, 64) != cudaSuccess) { cudaFree(buf); cudaGetLastError(); return -23; }
+    cudaMemset(buf, 0x5a, bytes);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int blocks = sms * 8, per_thread = 256;
+    const uint64_t sector_mask = bytes / 32 - 1;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    gather_kernel<<<blocks, 256>>>((const uint4 *)buf, sector_mask, per_thread, (uint32_t *)sink);   // warm-up
+    double best = 0;
+    for (int r = 0; r < repeats; ++r) {
+        cudaEventRecord(e0);
+        gather_kernel<<<blocks, 256>>>((const uint4 *)buf, sector_mask, per_thread, (uint32_t *)sink);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double v = (double)blocks * 256 * per_thread * 32 / (ms * 1e-3) / 1e9;
+        if (v > best) best = v;
+    }
+    const cudaError_t ce = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    cudaFree(sink);
+    if (ce != cudaSuccess) return -22;
+    *gbs = best;
+    return 0;
+}
+
 // ---- results in read order ----
 // Records are appended to out_rec in the order reads finish (an atomic counter per record block); the caller
 // wants them in read order. An exclusive scan of max(n_aln, 0) gives each read's first record in read order;

@@ -205,58 +205,169 @@ __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int ma
         bool pend = false;
         Entry e;
         int e_score = 0;
-        while (n_entries) {
-            if (n_entries > O.max_entries) break;
-            if (pend) {
-                pend = false;
-                --n_entries;
-            } else {
-                int b = best;
-                int idx = heads[b];
-                load_entry<WIDE>(ent, idx, b, e);
-                e_score = b;
-                int nx = link[idx];
-                heads[b] = nx;
-                if (FREELIST) { link[idx] = free_head; free_head = idx; }
-                --n_entries;
-                if (nx < 0) {
-                    if (b < 64) m0 &= ~(1ull << b); else if (b < 128) m1 &= ~(1ull << (b - 64));
-                    if (n_entries) {
-                        if (small_mask) best = next_bucket(m0, m1, b + 1);
-                        else { int t = b + 1; while (t < n_stacks && heads[t] < 0) ++t; best = t; }
-                    } else best = n_stacks;
+        // The exact walk of a pop with no difference left (bwt_match_exact_alt) goes one LF step per loop
+        // iteration and shares the iteration's one fetch, so that threads of a warp in a walk and threads
+        // expanding a pop wait for memory together.
+        bool walking = false;
+        uint64_t wk = 0, wl = 0;
+        int wi = 0;
+        int diffs = 0, m = 0, m_seed = 0;
+        uint64_t hk = 0, hl = 0;        // the interval of a hit
+        for (;;) {
+            uint64_t k1, l1;            // this iteration's Occ positions
+            int i = 0;
+            if (!walking) {
+                if (!n_entries) break;
+                if (n_entries > O.max_entries) break;
+                if (pend) {
+                    pend = false;
+                    --n_entries;
+                } else {
+                    int b = best;
+                    int idx = heads[b];
+                    load_entry<WIDE>(ent, idx, b, e);
+                    e_score = b;
+                    int nx = link[idx];
+                    heads[b] = nx;
+                    if (FREELIST) { link[idx] = free_head; free_head = idx; }
+                    --n_entries;
+                    if (nx < 0) {
+                        if (b < 64) m0 &= ~(1ull << b); else if (b < 128) m1 &= ~(1ull << (b - 64));
+                        if (n_entries) {
+                            if (small_mask) best = next_bucket(m0, m1, b + 1);
+                            else { int t = b + 1; while (t < n_stacks && heads[t] < 0) ++t; best = t; }
+                        } else best = n_stacks;
+                    }
                 }
+                ++pops;
+                if (TRACE) {
+                    uint64_t h = trace;
+                    h = trace_mix(h, e.info);
+                    h = trace_mix(h, e.k);
+                    h = trace_mix(h, e.l);
+                    h = trace_mix(h, (uint64_t)((uint32_t)(e.n_mm & 255) | (uint32_t)(e.n_gapo & 255) << 8
+                                                | (uint32_t)(e.n_gape & 255) << 16 | (uint32_t)(e.state & 255) << 24));
+                    h = trace_mix(h, (uint64_t)(e.n_ins & 0xffff) | (uint64_t)(e.n_del & 0xffff) << 16);
+                    h = trace_mix(h, (uint64_t)(uint32_t)e.ldp);
+                    h = trace_mix(h, (uint64_t)(uint32_t)n_entries);
+                    trace = h;
+                }
+                i = (int)(e.info & 0xffff);
+                if (!nonstop && (e.info >> 21) > (uint32_t)(best_score + s_mm)) break;
+                diffs = e.n_mm + e.n_gapo + (gape ? e.n_gape : 0);
+                m = max_diff - diffs;
+                if (m < 0) continue;
+                m_seed = use_seed ? O.max_seed_diff - diffs : 0;
+                if (i > 0 && m < (int)(W[i - 1] >> 48)) continue;
+                if (i == 0) { hk = e.k; hl = e.l; goto hit; }
+                if (m == 0 && (e.state == kStM || gape || e.n_gape == O.max_gape)) {
+                    // bwt_match_exact_alt over positions i-1 .. 0
+                    if (q[i - 1] > 3) continue;
+                    walking = true; wk = e.k; wl = e.l; wi = i;
+                    k1 = wk - 1; l1 = wl;
+                } else {
+                    k1 = e.k - 1; l1 = e.l;
+                }
+            } else {
+                if (q[wi - 1] > 3) { walking = false; continue; }
+                k1 = wk - 1; l1 = wl;
             }
-            ++pops;
-            if (TRACE) {
-                uint64_t h = trace;
-                h = trace_mix(h, e.info);
-                h = trace_mix(h, e.k);
-                h = trace_mix(h, e.l);
-                h = trace_mix(h, (uint64_t)((uint32_t)(e.n_mm & 255) | (uint32_t)(e.n_gapo & 255) << 8
-                                            | (uint32_t)(e.n_gape & 255) << 16 | (uint32_t)(e.state & 255) << 24));
-                h = trace_mix(h, (uint64_t)(e.n_ins & 0xffff) | (uint64_t)(e.n_del & 0xffff) << 16);
-                h = trace_mix(h, (uint64_t)(uint32_t)e.ldp);
-                h = trace_mix(h, (uint64_t)(uint32_t)n_entries);
-                trace = h;
+            {
+                uint64_t ck[4], cl[4];
+                occ4_pair_u(ix, k1, l1, ck, cl, fetches);
+                if (walking) {
+                    const int c = q[wi - 1];
+                    const uint64_t kk = ix.C[c] + sel4(c, ck[0], ck[1], ck[2], ck[3]) + 1;
+                    const uint64_t ll = ix.C[c] + sel4(c, cl[0], cl[1], cl[2], cl[3]);
+                    if (kk > ll) { walking = false; continue; }
+                    wk = kk; wl = ll;
+                    if (--wi > 0) continue;
+                    walking = false;
+                    hk = wk; hl = wl;
+                    goto hit;
+                }
+                const uint64_t k = e.k, l = e.l;
+                --i;
+                // child intervals of the four bases, in registers
+                const uint64_t kk0 = ix.C[0] + ck[0] + 1, ll0 = ix.C[0] + cl[0];
+                const uint64_t kk1 = ix.C[1] + ck[1] + 1, ll1 = ix.C[1] + cl[1];
+                const uint64_t kk2 = ix.C[2] + ck[2] + 1, ll2 = ix.C[2] + cl[2];
+                const uint64_t kk3 = ix.C[3] + ck[3] + 1, ll3 = ix.C[3] + cl[3];
+                uint64_t occ = l - k + 1;
+                int allow_diff = 1, allow_M = 1;
+                if (i > 0) {
+                    uint64_t wa = W[i - 1], wb = W[i];
+                    int ba = (int)(wa >> 48), bb = (int)(wb >> 48);
+                    if (ba > m - 1) allow_diff = 0;
+                    else if (ba == m - 1 && bb == m - 1 && (wa & kW48) == (wb & kW48)) allow_M = 0;
+                    int ii = i - (len - seed_len);
+                    if (use_seed && ii > 0) {
+                        uint64_t sa = SW[ii - 1], sb = SW[ii];
+                        int sba = (int)(sa >> 48), sbb = (int)(sb >> 48);
+                        if (sba > m_seed - 1) allow_diff = 0;
+                        else if (sba == m_seed - 1 && sbb == m_seed - 1 && (sa & kW48) == (sb & kW48)) allow_M = 0;
+                    }
+                }
+                int gaps = e.n_gapo + e.n_gape;
+                int tmp = (O.mode & kModeLoggap) ? (gaps ? (31 - __clz(gaps)) : 0) / 2 + 1 : gaps;
+                const int b0 = e_score;
+                if (allow_diff && i >= O.indel_end_skip + tmp && len - i >= O.indel_end_skip + tmp) {
+                    if (e.state == kStM) {
+                        if (e.n_gapo < O.max_gapo) {
+                            GALN_PUSH(b0 + s_gapo, i, k, l, e.n_mm, e.n_gapo + 1, e.n_gape, e.n_ins + 1, e.n_del, kStI, 1);
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) {
+                                uint64_t kk = sel4(c, kk0, kk1, kk2, kk3), ll = sel4(c, ll0, ll1, ll2, ll3);
+                                if (kk <= ll)
+                                    GALN_PUSH(b0 + s_gapo, i + 1, kk, ll, e.n_mm, e.n_gapo + 1, e.n_gape, e.n_ins, e.n_del + 1, kStD, 1);
+                            }
+                        }
+                    } else if (e.state == kStI) {
+                        if (e.n_gape < O.max_gape)
+                            GALN_PUSH(b0 + s_gape, i, k, l, e.n_mm, e.n_gapo, e.n_gape + 1, e.n_ins + 1, e.n_del, kStI, 1);
+                    } else if (e.state == kStD) {
+                        if (e.n_gape < O.max_gape && (gaps < max_diff || occ < (uint64_t)(int64_t)O.max_del_occ)) {
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) {
+                                uint64_t kk = sel4(c, kk0, kk1, kk2, kk3), ll = sel4(c, ll0, ll1, ll2, ll3);
+                                if (kk <= ll)
+                                    GALN_PUSH(b0 + s_gape, i + 1, kk, ll, e.n_mm, e.n_gapo, e.n_gape + 1, e.n_ins, e.n_del + 1, kStD, 1);
+                            }
+                        }
+                    }
+                }
+                const int base = q[i];
+                if (allow_diff && allow_M) {
+#pragma unroll
+                    for (int j = 1; j <= 4; ++j) {
+                        int c = (base + j) & 3;
+                        int mm = j != 4 || base > 3;
+                        uint64_t kk = sel4(c, kk0, kk1, kk2, kk3), ll = sel4(c, ll0, ll1, ll2, ll3);
+                        if (kk <= ll) {
+                            if (!mm && fuse) {
+                                e.k = kk; e.l = ll; e.info = (uint32_t)b0 << 21 | (uint32_t)i; e.ldp = 0; e.state = kStM;
+                                ++n_entries; if (n_entries > peak) peak = n_entries;
+                                pend = true;
+                            } else
+                                GALN_PUSH(b0 + (mm ? s_mm : 0), i, kk, ll, e.n_mm + mm, e.n_gapo, e.n_gape, e.n_ins, e.n_del, kStM, mm);
+                        }
+                    }
+                } else if (base < 4) {
+                    uint64_t kk = sel4(base, kk0, kk1, kk2, kk3), ll = sel4(base, ll0, ll1, ll2, ll3);
+                    if (kk <= ll) {
+                        if (fuse) {
+                            e.k = kk; e.l = ll; e.info = (uint32_t)b0 << 21 | (uint32_t)i; e.ldp = 0; e.state = kStM;
+                            ++n_entries; if (n_entries > peak) peak = n_entries;
+                            pend = true;
+                        } else
+                            GALN_PUSH(b0, i, kk, ll, e.n_mm, e.n_gapo, e.n_gape, e.n_ins, e.n_del, kStM, 0);
+                    }
+                }
+                continue;
             }
-            uint64_t k = e.k, l = e.l;
-            int i = (int)(e.info & 0xffff);
-            if (!nonstop && (e.info >> 21) > (uint32_t)(best_score + s_mm)) break;
-
-            int diffs = e.n_mm + e.n_gapo + (gape ? e.n_gape : 0);
-            int m = max_diff - diffs;
-            if (m < 0) continue;
-            int m_seed = use_seed ? O.max_seed_diff - diffs : 0;
-            if (i > 0 && m < (int)(W[i - 1] >> 48)) continue;
-
-            int hit = 0;
-            if (i == 0) hit = 1;
-            else if (m == 0 && (e.state == kStM || gape || e.n_gape == O.max_gape)) {
-                if (match_exact_alt(ix, i, q, k, l, fetches)) hit = 1;
-                else continue;
-            }
-            if (hit) {
+        hit:
+            {
+                const uint64_t k = hk, l = hl;
                 int sc = e.n_mm * s_mm + e.n_gapo * s_gapo + e.n_gape * s_gape;
                 if (n_aln == 0) {
                     best_score = sc;
@@ -286,86 +397,6 @@ __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int ma
                     aln[3 * n_aln + 1] = k;
                     aln[3 * n_aln + 2] = l;
                     ++n_aln;
-                }
-                continue;
-            }
-
-            --i;
-            uint64_t ck[4], cl[4];
-            occ4_pair(ix, k - 1, l, ck, cl, fetches);
-            // child intervals of the four bases, in registers
-            const uint64_t kk0 = ix.C[0] + ck[0] + 1, ll0 = ix.C[0] + cl[0];
-            const uint64_t kk1 = ix.C[1] + ck[1] + 1, ll1 = ix.C[1] + cl[1];
-            const uint64_t kk2 = ix.C[2] + ck[2] + 1, ll2 = ix.C[2] + cl[2];
-            const uint64_t kk3 = ix.C[3] + ck[3] + 1, ll3 = ix.C[3] + cl[3];
-            uint64_t occ = l - k + 1;
-            int allow_diff = 1, allow_M = 1;
-            if (i > 0) {
-                uint64_t wa = W[i - 1], wb = W[i];
-                int ba = (int)(wa >> 48), bb = (int)(wb >> 48);
-                if (ba > m - 1) allow_diff = 0;
-                else if (ba == m - 1 && bb == m - 1 && (wa & kW48) == (wb & kW48)) allow_M = 0;
-                int ii = i - (len - seed_len);
-                if (use_seed && ii > 0) {
-                    uint64_t sa = SW[ii - 1], sb = SW[ii];
-                    int sba = (int)(sa >> 48), sbb = (int)(sb >> 48);
-                    if (sba > m_seed - 1) allow_diff = 0;
-                    else if (sba == m_seed - 1 && sbb == m_seed - 1 && (sa & kW48) == (sb & kW48)) allow_M = 0;
-                }
-            }
-            int gaps = e.n_gapo + e.n_gape;
-            int tmp = (O.mode & kModeLoggap) ? (gaps ? (31 - __clz(gaps)) : 0) / 2 + 1 : gaps;
-            const int b0 = e_score;
-            if (allow_diff && i >= O.indel_end_skip + tmp && len - i >= O.indel_end_skip + tmp) {
-                if (e.state == kStM) {
-                    if (e.n_gapo < O.max_gapo) {
-                        GALN_PUSH(b0 + s_gapo, i, k, l, e.n_mm, e.n_gapo + 1, e.n_gape, e.n_ins + 1, e.n_del, kStI, 1);
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) {
-                            uint64_t kk = sel4(c, kk0, kk1, kk2, kk3), ll = sel4(c, ll0, ll1, ll2, ll3);
-                            if (kk <= ll)
-                                GALN_PUSH(b0 + s_gapo, i + 1, kk, ll, e.n_mm, e.n_gapo + 1, e.n_gape, e.n_ins, e.n_del + 1, kStD, 1);
-                        }
-                    }
-                } else if (e.state == kStI) {
-                    if (e.n_gape < O.max_gape)
-                        GALN_PUSH(b0 + s_gape, i, k, l, e.n_mm, e.n_gapo, e.n_gape + 1, e.n_ins + 1, e.n_del, kStI, 1);
-                } else if (e.state == kStD) {
-                    if (e.n_gape < O.max_gape && (gaps < max_diff || occ < (uint64_t)(int64_t)O.max_del_occ)) {
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) {
-                            uint64_t kk = sel4(c, kk0, kk1, kk2, kk3), ll = sel4(c, ll0, ll1, ll2, ll3);
-                            if (kk <= ll)
-                                GALN_PUSH(b0 + s_gape, i + 1, kk, ll, e.n_mm, e.n_gapo, e.n_gape + 1, e.n_ins, e.n_del + 1, kStD, 1);
-                        }
-                    }
-                }
-            }
-            const int base = q[i];
-            if (allow_diff && allow_M) {
-#pragma unroll
-                for (int j = 1; j <= 4; ++j) {
-                    int c = (base + j) & 3;
-                    int mm = j != 4 || base > 3;
-                    uint64_t kk = sel4(c, kk0, kk1, kk2, kk3), ll = sel4(c, ll0, ll1, ll2, ll3);
-                    if (kk <= ll) {
-                        if (!mm && fuse) {
-                            e.k = kk; e.l = ll; e.info = (uint32_t)b0 << 21 | (uint32_t)i; e.ldp = 0; e.state = kStM;
-                            ++n_entries; if (n_entries > peak) peak = n_entries;
-                            pend = true;
-                        } else
-                            GALN_PUSH(b0 + (mm ? s_mm : 0), i, kk, ll, e.n_mm + mm, e.n_gapo, e.n_gape, e.n_ins, e.n_del, kStM, mm);
-                    }
-                }
-            } else if (base < 4) {
-                uint64_t kk = sel4(base, kk0, kk1, kk2, kk3), ll = sel4(base, ll0, ll1, ll2, ll3);
-                if (kk <= ll) {
-                    if (fuse) {
-                        e.k = kk; e.l = ll; e.info = (uint32_t)b0 << 21 | (uint32_t)i; e.ldp = 0; e.state = kStM;
-                        ++n_entries; if (n_entries > peak) peak = n_entries;
-                        pend = true;
-                    } else
-                        GALN_PUSH(b0, i, kk, ll, e.n_mm, e.n_gapo, e.n_gape, e.n_ins, e.n_del, kStM, 0);
                 }
             }
         }

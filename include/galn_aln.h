@@ -218,6 +218,12 @@ int galn_last_warp_counters(galn_index *ix, uint64_t *counters, int n);
  * ms; the device span in ms. */
 int galn_last_run_phases(galn_index *ix, double *ms, int n);
 
+/* Random 32-byte gather peak of the device (no reference counterpart; a measurement for the roofline): the
+ * best of `repeats` timed launches of a kernel reading pseudo-random 32-byte sectors of a buffer of the
+ * largest power of two <= `bytes` (>= 1 MiB; larger than L2 for the HBM figure, smaller for L2), in GB/s
+ * of sectors read. */
+int galn_gather_peak(int device, uint64_t bytes, int repeats, double *gbs);
+
 /* Tier capacities (no reference counterpart; set by the autotuner): entries and records per thread in the
  * first tier, its block size (64/128/256/512), live entries and records per thread in the second tier, and
  * whether to keep the per-read profile. Results never depend on these values. */
