@@ -91,7 +91,7 @@ def lib():
     L.galn_server_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                     C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     L.galn_autotune.argtypes = [vp, C.POINTER(Options), C.POINTER(_Reads), C.c_int, C.POINTER(C.c_int),
-                                C.POINTER(C.c_int), C.POINTER(C.c_double)]
+                                C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.galn_autotune_clear.argtypes = [vp]
     L.galn_last_graph_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     L.galn_version.restype = C.c_char_p
@@ -165,14 +165,21 @@ class Index:
         return {k: int(x) for k, x in zip(names, v)}
 
     def autotune(self, args, reads: "Reads", max_sample: int = 131072) -> dict:
-        """Pick the first-tier stack depth and block size for these options on a sample of `reads`."""
+        """Pick the occurrence layout, first-tier stack depth and block size for these options on a sample of
+        `reads`."""
         opts = args if isinstance(args, Options) else parse_options(list(args))
         cr, keep = reads.c_struct()
-        cap, blk, ms = C.c_int(), C.c_int(), C.c_double()
-        rc = lib().galn_autotune(self.h, C.byref(opts), C.byref(cr), max_sample, C.byref(cap), C.byref(blk), C.byref(ms))
+        cap, blk, occ, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        rc = lib().galn_autotune(self.h, C.byref(opts), C.byref(cr), max_sample, C.byref(cap), C.byref(blk),
+                                 C.byref(occ), C.byref(ms))
         if rc:
             raise GalnError(f"autotune failed ({rc})")
-        return dict(t0_cap=cap.value, block=blk.value, ms=ms.value)
+        return dict(t0_cap=cap.value, block=blk.value, occ=occ.value, ms=ms.value)
+
+    def set_occ_layout(self, stride: int):
+        """Occurrence layout (64 or 80 symbols per 32-byte block) when the autotuner has no choice."""
+        if lib().galn_index_set_occ_layout(self.h, stride):
+            raise GalnError("bad occ layout")
 
     def set_trace(self, on: bool):
         lib().galn_index_set_trace(self.h, int(on))

@@ -1,19 +1,28 @@
 // galn_device.cuh -- device side of the `bwa aln` search for sm_100a.
 //
-// Occurrence layout ("occ64"): the $-free BWT is cut into blocks of 64 symbols; block b is 32 bytes
-// (one DRAM sector): four uint32 counts of each base before the block, relative to the block's
-// 2^32-symbol superblock, then the 64 symbols as two 64-bit bit planes (bit j of p0 = low bit of symbol j,
-// of p1 = high bit). One LF step for one position is one 32-byte fetch and at most four popcounts; the
-// reference's layout (src/bwtsearch.h:22-34, 128 symbols in 64 bytes) needs two sectors. The superblock
-// counts (Occ before each 2^32 symbols) are kernel parameters. Counts and intervals are the same integers
-// as bwt_occ / bwt_2occ / bwt_occ4 / bwt_2occ4 (src/bwtsearch.h:46-108, src/bwtgap_hd.h:135-192).
+// Two occurrence layouts, both one 32-byte sector (one DRAM sector) per block; the kernels take the stride
+// as a template parameter and an index holds both.
+//   occ64: blocks of 64 symbols of the $-free BWT: four uint32 counts of each base before the block,
+//          relative to the block's 2^32-symbol superblock, then the 64 symbols as two 64-bit bit planes
+//          (bit j of p0 = low bit of symbol j, of p1 = high bit).
+//   occ80: blocks of 80 symbols: three uint32 counts (A, C, G) before the block relative to its superblock
+//          of 2^25 blocks, a word holding bits 64-79 of both planes (p0 in the low half, p1 in the high),
+//          then bits 0-63 of p0 and p1. The count of T is the position's rank minus the other three.
+//          20% smaller (80 MB for a 100 Mbp genome, inside the device's persisting-L2 limit), and a pair
+//          (k-1, l) falls in one block more often.
+// One LF step for one position is one 32-byte fetch; the reference's layout (src/bwtsearch.h:22-34, 128
+// symbols in 64 bytes) needs two sectors. The superblock counts are kernel parameters. Counts and intervals
+// are the same integers as bwt_occ / bwt_2occ / bwt_occ4 / bwt_2occ4 (src/bwtsearch.h:46-108,
+// src/bwtgap_hd.h:135-192).
 #pragma once
 
 #include <stdint.h>
 
 namespace galn {
 
-constexpr int kMaxSuper = 16;          // 2^36 symbols
+constexpr int kMaxSuper = 16;          // superblocks: 2^36 symbols for occ64, 2^29 x 80 for occ80
+constexpr int kOcc64 = 64, kOcc80 = 80;   // the layouts' strides
+constexpr int kOcc80SuperShift = 25;   // occ80 blocks per superblock: 2^25
 constexpr int kModeGape = 0x01, kModeLoggap = 0x04, kModeNonstop = 0x10;
 constexpr int kStM = 0, kStI = 1, kStD = 2;
 constexpr int kErrStack = -1, kErrAln = -2, kErrScore = -3;
@@ -37,50 +46,26 @@ struct BatchOpt {
     int pad_;
 };
 
-__device__ __forceinline__ void load_block(const IndexView &ix, uint64_t p, uint4 &cnt, uint64_t &p0, uint64_t &p1)
+__device__ __forceinline__ uint64_t sel4(int c, uint64_t a0, uint64_t a1, uint64_t a2, uint64_t a3)
 {
-    const uint4 *b = ix.blk + ((p >> 6) << 1);
-    cnt = __ldg(b);
-    uint4 bits = __ldg(b + 1);
-    p0 = (uint64_t)bits.x | ((uint64_t)bits.y << 32);
-    p1 = (uint64_t)bits.z | ((uint64_t)bits.w << 32);
+    uint64_t lo = (c & 1) ? a1 : a0, hi = (c & 1) ? a3 : a2;
+    return (c & 2) ? hi : lo;
 }
 
-__device__ __forceinline__ uint64_t base_mask(uint64_t p0, uint64_t p1, int c)
-{
-    uint64_t a = (c & 1) ? p0 : ~p0;
-    uint64_t b = (c & 2) ? p1 : ~p1;
-    return a & b;
-}
-
-__device__ __forceinline__ uint32_t cnt_of(const uint4 &v, int c)
-{
-    return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
-}
-
-// Occ(c, pos) for all four bases; pos in [-1, seq_len]
-__device__ __forceinline__ void occ4_one(const IndexView &ix, uint64_t pos, uint64_t o[4])
-{
-    if (pos == ~0ull) { o[0] = o[1] = o[2] = o[3] = 0; return; }
-    uint64_t p = pos - (pos >= ix.primary);
-    uint4 cnt; uint64_t p0, p1;
-    load_block(ix, p, cnt, p0, p1);
-    uint64_t m = (2ull << (p & 63)) - 1;
-    const uint64_t *s = ix.sb[p >> 32];
-    o[0] = s[0] + cnt.x + __popcll(~p0 & ~p1 & m);
-    o[1] = s[1] + cnt.y + __popcll(p0 & ~p1 & m);
-    o[2] = s[2] + cnt.z + __popcll(~p0 & p1 & m);
-    o[3] = s[3] + cnt.w + __popcll(p0 & p1 & m);
-}
-
-// Occ(c, k1) and Occ(c, l) for all four bases, without a branch around the loads: both blocks are read (the
-// same address twice when k1 and l share a block, which the L1 merges), so threads of a warp that differ in
-// that respect still wait for one round trip together. `fetches` counts the distinct 32-byte blocks (the
-// roofline's unit of algorithmic traffic): one when both positions fall in one block.
+// Occ(c, k1) and Occ(c, l) for all four bases (positions in [-1, seq_len]; Occ(., -1) = 0), without a branch
+// around the loads: both blocks are read (the same address twice when k1 and l share a block, which the L1
+// merges), so threads of a warp that differ in that respect still wait for one round trip together.
+// `fetches` counts the distinct 32-byte blocks (the roofline's unit of algorithmic traffic): one when both
+// positions fall in one block.
+template <int S>
 __device__ __forceinline__ void occ4_pair_u(const IndexView &ix, uint64_t k1, uint64_t l, uint64_t ok[4], uint64_t ol[4],
-                                            uint32_t &fetches)
+                                            uint32_t &fetches);
+
+template <>
+__device__ __forceinline__ void occ4_pair_u<kOcc64>(const IndexView &ix, uint64_t k1, uint64_t l, uint64_t ok[4],
+                                                    uint64_t ol[4], uint32_t &fetches)
 {
-    const bool kn = k1 == ~0ull, ln = l == ~0ull;   // Occ(., -1) = 0
+    const bool kn = k1 == ~0ull, ln = l == ~0ull;
     const uint64_t pk = kn ? 0 : k1 - (k1 >= ix.primary);
     const uint64_t pl = ln ? 0 : l - (l >= ix.primary);
     const bool same = !kn && !ln && (pk >> 6) == (pl >> 6);
@@ -101,68 +86,48 @@ __device__ __forceinline__ void occ4_pair_u(const IndexView &ix, uint64_t k1, ui
     ol[3] = ln ? 0 : sl[3] + cl.w + __popcll(p0l & p1l & ml);
 }
 
-// Occ(c, k1) and Occ(c, l) for all four bases, one fetch when both fall in one block. `fetches` counts the
-// 32-byte blocks read (the roofline's unit of algorithmic traffic).
-__device__ __forceinline__ void occ4_pair(const IndexView &ix, uint64_t k1, uint64_t l, uint64_t ok[4], uint64_t ol[4],
-                                          uint32_t &fetches)
+// Occ of the four bases up to $-free position p at offset j of occ80 block b (its two uint4 halves c, x)
+__device__ __forceinline__ void occ80_counts(const IndexView &ix, uint4 c, uint4 x, uint64_t p, int j, uint64_t b,
+                                             uint64_t o[4])
 {
-    if (k1 != ~0ull) {
-        uint64_t pk = k1 - (k1 >= ix.primary), pl = l - (l >= ix.primary);
-        if ((pk >> 6) == (pl >> 6)) {
-            ++fetches;
-            uint4 cnt; uint64_t p0, p1;
-            load_block(ix, pk, cnt, p0, p1);
-            uint64_t mk = (2ull << (pk & 63)) - 1, ml = (2ull << (pl & 63)) - 1;
-            const uint64_t *s = ix.sb[pk >> 32];
-            uint64_t a = ~p0 & ~p1, c = p0 & ~p1, g = ~p0 & p1, t = p0 & p1;
-            ok[0] = s[0] + cnt.x + __popcll(a & mk); ol[0] = s[0] + cnt.x + __popcll(a & ml);
-            ok[1] = s[1] + cnt.y + __popcll(c & mk); ol[1] = s[1] + cnt.y + __popcll(c & ml);
-            ok[2] = s[2] + cnt.z + __popcll(g & mk); ol[2] = s[2] + cnt.z + __popcll(g & ml);
-            ok[3] = s[3] + cnt.w + __popcll(t & mk); ol[3] = s[3] + cnt.w + __popcll(t & ml);
-            return;
-        }
-    }
-    fetches += (k1 != ~0ull) + (l != ~0ull);
-    occ4_one(ix, k1, ok);
-    occ4_one(ix, l, ol);
+    const uint64_t lo0 = (uint64_t)x.x | ((uint64_t)x.y << 32), lo1 = (uint64_t)x.z | ((uint64_t)x.w << 32);
+    const uint32_t h0 = c.w & 0xffffu, h1 = c.w >> 16;
+    const uint64_t mlo = j >= 63 ? ~0ull : (2ull << j) - 1;
+    const uint32_t mhi = j >= 64 ? (2u << (j - 64)) - 1 : 0u;
+    const uint64_t *s = ix.sb[b >> kOcc80SuperShift];
+    const uint64_t a = s[0] + c.x + __popcll(~lo0 & ~lo1 & mlo) + __popc(~h0 & ~h1 & mhi);
+    const uint64_t cc = s[1] + c.y + __popcll(lo0 & ~lo1 & mlo) + __popc(h0 & ~h1 & mhi);
+    const uint64_t g = s[2] + c.z + __popcll(~lo0 & lo1 & mlo) + __popc(~h0 & h1 & mhi);
+    o[0] = a; o[1] = cc; o[2] = g;
+    o[3] = p + 1 - a - cc - g;
 }
 
-// Occ(c, pos) for one base
-__device__ __forceinline__ uint64_t occ1(const IndexView &ix, uint64_t pos, int c)
+template <>
+__device__ __forceinline__ void occ4_pair_u<kOcc80>(const IndexView &ix, uint64_t k1, uint64_t l, uint64_t ok[4],
+                                                    uint64_t ol[4], uint32_t &fetches)
 {
-    if (pos == ~0ull) return 0;
-    uint64_t p = pos - (pos >= ix.primary);
-    uint4 cnt; uint64_t p0, p1;
-    load_block(ix, p, cnt, p0, p1);
-    uint64_t m = (2ull << (p & 63)) - 1;
-    return ix.sb[p >> 32][c] + cnt_of(cnt, c) + __popcll(base_mask(p0, p1, c) & m);
+    const bool kn = k1 == ~0ull, ln = l == ~0ull;
+    const uint64_t pk = kn ? 0 : k1 - (k1 >= ix.primary);
+    const uint64_t pl = ln ? 0 : l - (l >= ix.primary);
+    const uint64_t bk = pk / 80, bl = pl / 80;
+    const bool same = !kn && !ln && bk == bl;
+    fetches += same ? 1u : (uint32_t)(!kn) + (uint32_t)(!ln);
+    const uint4 *qk = ix.blk + (bk << 1), *ql = ix.blk + (bl << 1);
+    const uint4 ck = __ldg(qk), xk = __ldg(qk + 1), cl = __ldg(ql), xl = __ldg(ql + 1);
+    occ80_counts(ix, ck, xk, pk, (int)(pk - 80 * bk), bk, ok);
+    occ80_counts(ix, cl, xl, pl, (int)(pl - 80 * bl), bl, ol);
+    if (kn) { ok[0] = ok[1] = ok[2] = ok[3] = 0; }
+    if (ln) { ol[0] = ol[1] = ol[2] = ol[3] = 0; }
 }
 
 // (k, l) <- interval of base c prepended: [C(c) + Occ(c, k-1) + 1, C(c) + Occ(c, l)]
+template <int S>
 __device__ __forceinline__ void extend1(const IndexView &ix, int c, uint64_t &k, uint64_t &l, uint32_t &fetches)
 {
-    uint64_t k1 = k - 1;
-    uint64_t ok, ol;
-    if (k1 != ~0ull) {
-        uint64_t pk = k1 - (k1 >= ix.primary), pl = l - (l >= ix.primary);
-        if ((pk >> 6) == (pl >> 6)) {
-            ++fetches;
-            uint4 cnt; uint64_t p0, p1;
-            load_block(ix, pk, cnt, p0, p1);
-            uint64_t bm = base_mask(p0, p1, c);
-            uint64_t base = ix.sb[pk >> 32][c] + cnt_of(cnt, c);
-            ok = base + __popcll(bm & ((2ull << (pk & 63)) - 1));
-            ol = base + __popcll(bm & ((2ull << (pl & 63)) - 1));
-            k = ix.C[c] + ok + 1;
-            l = ix.C[c] + ol;
-            return;
-        }
-    }
-    fetches += (k1 != ~0ull) + (l != ~0ull);
-    ok = occ1(ix, k1, c);
-    ol = occ1(ix, l, c);
-    k = ix.C[c] + ok + 1;
-    l = ix.C[c] + ol;
+    uint64_t ok[4], ol[4];
+    occ4_pair_u<S>(ix, k - 1, l, ok, ol, fetches);
+    k = ix.C[c] + sel4(c, ok[0], ok[1], ok[2], ok[3]) + 1;
+    l = ix.C[c] + sel4(c, ol[0], ol[1], ol[2], ol[3]);
 }
 
 __device__ __forceinline__ uint64_t trace_mix(uint64_t h, uint64_t v) { return (h ^ v) * kTracePrime; }

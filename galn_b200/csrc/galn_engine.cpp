@@ -203,6 +203,17 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     job.out_rec = (uint64_t *)B.out_rec.p; job.rec_top = (unsigned long long *)B.rec_top.p; job.rec_cap = rec_cap;
     job.list_a = (int32_t *)B.list_a.p; job.list_b = (int32_t *)B.list_b.p; job.counters = (int32_t *)B.counters.p;
     if (job.seed_len < 0) job.seed_len = 0;
+    // the occurrence layout: the autotuner's for this option set, else the index's default; the stream's
+    // persisting L2 window follows it
+    job.occ = ix->occ;
+    if (engine != GALN_ENGINE_PLAIN && !ix->tune_active) {
+        auto it = ix->tuned.find(opts_key(&sets[0]));
+        if (it != ix->tuned.end()) job.occ = it->second.occ;
+    }
+    if (ctx.l2_occ != job.occ) {
+        index_l2_policy(ix, st, job.occ);
+        ctx.l2_occ = job.occ;
+    }
     cudaEvent_t span0, span1;
     ECK(cudaEventCreate(&span0));
     ECK(cudaEventCreate(&span1));
@@ -297,7 +308,7 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     if (engine != GALN_ENGINE_PLAIN && !ix->tune_active && !ix->tuned.empty()) {
         // the autotuner's choice for this option set (single-set jobs; mixed jobs use the first set's)
         auto it = ix->tuned.find(opts_key(&sets[0]));
-        if (it != ix->tuned.end()) { t0.cap = it->second.first; t0.block = it->second.second; }
+        if (it != ix->tuned.end()) { t0.cap = it->second.cap; t0.block = it->second.block; }
     }
     if (engine == GALN_ENGINE_PERSISTENT) {
         t0.persistent = true;
@@ -615,8 +626,16 @@ extern "C" int galn_index_set_l2_persist(galn_index *ix, int on)
     if (!ix) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
     ix->l2_persist = on != 0;
-    if (ix->l2_persist) galn::index_l2_policy(ix, ix->stream);
+    if (ix->l2_persist) galn::index_l2_policy(ix, ix->stream, ix->main.l2_occ ? ix->main.l2_occ : ix->occ);
     else galn::index_l2_clear(ix, ix->stream);
+    return 0;
+}
+
+extern "C" int galn_index_set_occ_layout(galn_index *ix, int stride)
+{
+    if (!ix || (stride != 64 && stride != 80)) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    ix->occ = stride;
     return 0;
 }
 

@@ -283,7 +283,8 @@ static galn_index *index_from_words(const uint64_t hdr[5], const uint32_t *body,
         if (err) *err = rc;
         return nullptr;
     }
-    galn::index_l2_policy(ix, ix->stream);
+    galn::index_l2_policy(ix, ix->stream, ix->occ);
+    ix->main.l2_occ = ix->occ;
     if (err) *err = 0;
     return ix;
 }
@@ -292,19 +293,21 @@ static galn_index *index_from_words(const uint64_t hdr[5], const uint32_t *body,
 // searches (the set-aside is a limit of this process's context and ends with it). The search reads the
 // index at random on every step, while stack pushes and pops stream through; without the window the
 // stream evicts the index.
-void galn::index_l2_policy(galn_index *ix, cudaStream_t st)
+void galn::index_l2_policy(galn_index *ix, cudaStream_t st, int occ)
 {
-    if (!ix->l2_persist || !ix->dev.blocks) return;
+    const void *blocks = occ == 80 ? ix->dev.blocks80 : ix->dev.blocks;
+    const uint64_t n_blocks = occ == 80 ? ix->dev.n_blocks80 : ix->dev.n_blocks;
+    if (!ix->l2_persist || !blocks) return;
     int maxw = 0, maxp = 0;
     cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, ix->dev.device);
     cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, ix->dev.device);
     if (maxw <= 0 || maxp <= 0) return;
-    const size_t bytes = std::min<size_t>((size_t)ix->dev.n_blocks * 32, (size_t)maxw);
+    const size_t bytes = std::min<size_t>((size_t)n_blocks * 32, (size_t)maxw);
     const size_t persist = std::min<size_t>(bytes, (size_t)maxp);
     if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist) != cudaSuccess) { cudaGetLastError(); return; }
     cudaStreamAttrValue v;
     memset(&v, 0, sizeof(v));
-    v.accessPolicyWindow.base_ptr = ix->dev.blocks;
+    v.accessPolicyWindow.base_ptr = const_cast<void *>(blocks);
     v.accessPolicyWindow.num_bytes = bytes;
     v.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)persist / (double)bytes);
     v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;

@@ -78,6 +78,7 @@ struct ExecCtx {
     RunStats last;
     double mem_share = 1.0;            // of the budget this context's workspace may take
     cudaGraphExec_t graph_exec = nullptr;   // the persistent first-tier launch, captured
+    int l2_occ = 0;                    // the layout the stream's persisting L2 window covers (0: none set)
     void release()
     {
         if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
@@ -101,7 +102,9 @@ struct galn_index {
     bool keep_stats = false;            // keep per-read fetch counts and tiers of the last run
     bool trace = true;                  // compute the per-read trace hash (the reference's --verify data)
     bool use_warp = true;               // the warp tier for reads that overflow T0
-    std::map<uint64_t, std::pair<int, int>> tuned;   // option-set key -> (first-tier depth, block), autotuner
+    struct TuneChoice { int cap, block, occ; };
+    std::map<uint64_t, TuneChoice> tuned;   // option-set key -> the autotuner's choice
+    int occ = 64;                       // occurrence layout when the autotuner has no choice (64 or 80)
     bool tune_active = false;           // the autotuner is timing a candidate: ignore the table
     bool use_graph = true;              // launch the persistent first tier through a CUDA graph
     int warp_arena = 1 << 14;           // 32-entry chunks per warp
@@ -143,7 +146,7 @@ struct ResultsPriv {
         out->_priv = this;
     }
 };
-void index_l2_policy(galn_index *ix, cudaStream_t st);
+void index_l2_policy(galn_index *ix, cudaStream_t st, int occ);
 void index_l2_clear(galn_index *ix, cudaStream_t st);
 int run_job(galn_index *ix, ExecCtx &ctx, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);
 int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_sets, const int32_t *batch_set,

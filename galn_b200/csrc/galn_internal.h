@@ -24,7 +24,10 @@ struct DevIndex {
     uint64_t primary = 0, seq_len = 0, n_blocks = 0;
     uint64_t L2[5] = {0, 0, 0, 0, 0};
     uint64_t sb[16][4] = {};
-    void *blocks = nullptr;            // n_blocks * 32 bytes, device
+    void *blocks = nullptr;            // n_blocks * 32 bytes, device (occ64)
+    uint64_t n_blocks80 = 0;
+    uint64_t sb80[16][4] = {};
+    void *blocks80 = nullptr;          // n_blocks80 * 32 bytes, device (occ80)
 };
 
 // Builds the occ64 layout on the device from the .bwt body words (host memory).
@@ -41,6 +44,7 @@ struct DevJob {
     int32_t *maxdiff = nullptr;        // per read
     HostBatchOpt *bopt = nullptr;      // per batch (device copy)
     int seed_len = 0;
+    int occ = 64;                      // occurrence layout of the kernels (64 or 80 symbols per block)
     int max_len = 0;
     int max_stacks = 0;
     int any_wide = 0;

@@ -70,6 +70,60 @@ __global__ void convert_kernel(const uint32_t *__restrict__ body, uint64_t n_wor
     out[2 * b + 1] = make_uint4((uint32_t)p0, (uint32_t)(p0 >> 32), (uint32_t)p1, (uint32_t)(p1 >> 32));
 }
 
+// occ64 blocks -> occ80 blocks. Block b covers symbols [80b, 80b+80): the counts of A, C, G before it
+// (Occ at 80b - 1, relative to its superblock's sb80 entry) and the two bit planes of its 80 symbols, taken
+// from the occ64 planes (positions past the text are 0 there and stay 0).
+__global__ void convert80_kernel(const uint4 *__restrict__ occ64, uint64_t n_blocks64, const uint64_t *__restrict__ sb64,
+                                 uint64_t n_blocks80, const uint64_t *__restrict__ sb80, uint4 *__restrict__ out)
+{
+    const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n_blocks80) return;
+    const uint64_t start = 80 * b;
+    uint64_t cnt[3] = {0, 0, 0};
+    if (start > 0) {
+        const uint64_t q = start - 1, B = q >> 6;
+        const uint4 c = occ64[2 * B], x = occ64[2 * B + 1];
+        const uint64_t p0 = (uint64_t)x.x | ((uint64_t)x.y << 32), p1 = (uint64_t)x.z | ((uint64_t)x.w << 32);
+        const uint64_t m = (q & 63) == 63 ? ~0ull : (2ull << (q & 63)) - 1;
+        const uint64_t *s = sb64 + (q >> 32) * 4;
+        cnt[0] = s[0] + c.x + __popcll(~p0 & ~p1 & m);
+        cnt[1] = s[1] + c.y + __popcll(p0 & ~p1 & m);
+        cnt[2] = s[2] + c.z + __popcll(~p0 & p1 & m);
+    }
+    uint64_t w0[3], w1[3];   // planes 0 and 1 of occ64 blocks B0, B0+1, B0+2
+    const uint64_t B0 = start >> 6;
+    for (int t = 0; t < 3; ++t) {
+        const uint64_t Bi = B0 + t;
+        if (Bi < n_blocks64) {
+            const uint4 x = occ64[2 * Bi + 1];
+            w0[t] = (uint64_t)x.x | ((uint64_t)x.y << 32);
+            w1[t] = (uint64_t)x.z | ((uint64_t)x.w << 32);
+        } else w0[t] = w1[t] = 0;
+    }
+    const int off = (int)(start & 63);
+    const uint64_t lo0 = off ? (w0[0] >> off) | (w0[1] << (64 - off)) : w0[0];
+    const uint64_t lo1 = off ? (w1[0] >> off) | (w1[1] << (64 - off)) : w1[0];
+    const uint64_t hi0 = off ? (w0[1] >> off) | (w0[2] << (64 - off)) : w0[1];
+    const uint64_t hi1 = off ? (w1[1] >> off) | (w1[2] << (64 - off)) : w1[1];
+    const uint64_t *base = sb80 + (b >> kOcc80SuperShift) * 4;
+    out[2 * b] = make_uint4((uint32_t)(cnt[0] - base[0]), (uint32_t)(cnt[1] - base[1]), (uint32_t)(cnt[2] - base[2]),
+                            (uint32_t)(hi0 & 0xffffu) | ((uint32_t)(hi1 & 0xffffu) << 16));
+    out[2 * b + 1] = make_uint4((uint32_t)lo0, (uint32_t)(lo0 >> 32), (uint32_t)lo1, (uint32_t)(lo1 >> 32));
+}
+
+// Occ of each base before $-free position pos, from the .bwt body (per 128 symbols: 4 x u64 counts, then 8
+// words of 16 symbols, first symbol in the top bits)
+static void body_occ_before(const uint32_t *body, uint64_t n_words, uint64_t pos, uint64_t cnt[4])
+{
+    const uint64_t B = pos >> 7;
+    for (int c = 0; c < 4; ++c) cnt[c] = (uint64_t)body[B * 16 + 2 * c] | ((uint64_t)body[B * 16 + 2 * c + 1] << 32);
+    for (uint64_t p = B << 7; p < pos; ++p) {
+        const uint64_t wi = B * 16 + 8 + ((p & 127) >> 4);
+        const uint32_t w = wi < n_words ? body[wi] : 0u;
+        ++cnt[(w >> (30 - 2 * (p & 15))) & 3];
+    }
+}
+
 int dev_index_build(DevIndex &ix, const uint32_t *body, uint64_t n_words, cudaStream_t st)
 {
     const uint64_t n = ix.seq_len;
@@ -94,19 +148,33 @@ int dev_index_build(DevIndex &ix, const uint32_t *body, uint64_t n_words, cudaSt
     convert_kernel<<<grid, 256, 0, st>>>((const uint32_t *)d_body, n_words, n, ix.n_blocks, (const uint64_t *)d_sb,
                                          (uint4 *)ix.blocks);
     GALN_CUDA(cudaGetLastError());
+    // the occ80 layout from the occ64 one
+    ix.n_blocks80 = n / 80 + 1;
+    const uint64_t n_super80 = (ix.n_blocks80 >> kOcc80SuperShift) + 1;
+    if (n_super80 > 16) { cudaFree(d_body); cudaFree(d_sb); return -20; }
+    for (uint64_t s = 0; s < 16; ++s)
+        for (int c = 0; c < 4; ++c) ix.sb80[s][c] = 0;
+    for (uint64_t s = 1; s < n_super80; ++s) body_occ_before(body, n_words, (s << kOcc80SuperShift) * 80, ix.sb80[s]);
+    void *d_sb80 = nullptr;
+    GALN_CUDA(cudaMalloc(&ix.blocks80, ix.n_blocks80 * 32));
+    GALN_CUDA(cudaMalloc(&d_sb80, sizeof(ix.sb80)));
+    GALN_CUDA(cudaMemcpyAsync(d_sb80, ix.sb80, sizeof(ix.sb80), cudaMemcpyHostToDevice, st));
+    grid = (unsigned)((ix.n_blocks80 + 255) / 256);
+    convert80_kernel<<<grid, 256, 0, st>>>((const uint4 *)ix.blocks, ix.n_blocks, (const uint64_t *)d_sb, ix.n_blocks80,
+                                           (const uint64_t *)d_sb80, (uint4 *)ix.blocks80);
+    GALN_CUDA(cudaGetLastError());
     GALN_CUDA(cudaStreamSynchronize(st));
     cudaFree(d_body);
     cudaFree(d_sb);
+    cudaFree(d_sb80);
     return 0;
 }
 
 void dev_index_free(DevIndex &ix)
 {
-    if (ix.blocks) {
-        cudaSetDevice(ix.device);
-        cudaFree(ix.blocks);
-        ix.blocks = nullptr;
-    }
+    cudaSetDevice(ix.device);
+    if (ix.blocks) { cudaFree(ix.blocks); ix.blocks = nullptr; }
+    if (ix.blocks80) { cudaFree(ix.blocks80); ix.blocks80 = nullptr; }
 }
 
 // ---------------------------------------------------------------------------------------------------
@@ -172,7 +240,7 @@ struct KArgs {
     int32_t *ovf_n;
 };
 
-template <bool WIDE, bool FREELIST, bool TRACE>
+template <bool WIDE, bool FREELIST, bool TRACE, int S>
 __device__ __forceinline__ void run_read(const KArgs &a, int pos, int slot)
 {
     const int r = a.list[pos];
@@ -185,9 +253,9 @@ __device__ __forceinline__ void run_read(const KArgs &a, int pos, int slot)
     uint64_t *SW = W + (len + 1);
     const bool use_seed = len > bo.seed_len;
     uint32_t fetches = 0;
-    cal_width(a.ix, len, q, W, fetches);
-    if (use_seed) cal_width(a.ix, bo.seed_len, q + (len - bo.seed_len), SW, fetches);
-    SearchResult R = match_gap<WIDE, FREELIST, TRACE>(a.ix, bo, md, len, q, W, SW, use_seed, a.ws, slot, fetches);
+    cal_width<S>(a.ix, len, q, W, fetches);
+    if (use_seed) cal_width<S>(a.ix, bo.seed_len, q + (len - bo.seed_len), SW, fetches);
+    SearchResult R = match_gap<WIDE, FREELIST, TRACE, S>(a.ix, bo, md, len, q, W, SW, use_seed, a.ws, slot, fetches);
     int ret = R.ret;
     if (ret > 0) {
         unsigned long long o = atomicAdd(a.rec_top, (unsigned long long)ret);
@@ -208,19 +276,19 @@ __device__ __forceinline__ void run_read(const KArgs &a, int pos, int slot)
     a.out_tier[r] = (int8_t)a.tier;
 }
 
-template <bool WIDE, bool FREELIST, bool TRACE>
+template <bool WIDE, bool FREELIST, bool TRACE, int S>
 __global__ void __launch_bounds__(512) search_kernel(const __grid_constant__ KArgs a)
 {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= a.n_slots) return;
     if (!a.persistent) {
-        if (slot < a.n) run_read<WIDE, FREELIST, TRACE>(a, slot, slot);
+        if (slot < a.n) run_read<WIDE, FREELIST, TRACE, S>(a, slot, slot);
         return;
     }
     for (;;) {
         int pos = atomicAdd(a.claim, 1);
         if (pos >= a.n) break;
-        run_read<WIDE, FREELIST, TRACE>(a, pos, slot);
+        run_read<WIDE, FREELIST, TRACE, S>(a, pos, slot);
     }
 }
 
@@ -252,13 +320,33 @@ size_t ws_bytes(const TierCfg &cfg, const DevJob &job)
     return off[5];
 }
 
-template <bool WIDE, bool FREELIST>
+template <bool WIDE, bool FREELIST, int S>
 static int launch(const KArgs &a, int threads, int block, cudaStream_t st)
 {
     unsigned grid = (unsigned)((threads + block - 1) / block);
-    if (a.trace) search_kernel<WIDE, FREELIST, true><<<grid, block, 0, st>>>(a);
-    else search_kernel<WIDE, FREELIST, false><<<grid, block, 0, st>>>(a);
+    if (a.trace) search_kernel<WIDE, FREELIST, true, S><<<grid, block, 0, st>>>(a);
+    else search_kernel<WIDE, FREELIST, false, S><<<grid, block, 0, st>>>(a);
     GALN_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <int S>
+static int launch_s(const KArgs &a, bool wide, bool freelist, int threads, int block, cudaStream_t st)
+{
+    if (wide) return freelist ? launch<true, true, S>(a, threads, block, st) : launch<true, false, S>(a, threads, block, st);
+    return freelist ? launch<false, true, S>(a, threads, block, st) : launch<false, false, S>(a, threads, block, st);
+}
+
+// the kernels' view of the index in the job's occurrence layout
+static int index_view(const DevIndex &ix, int occ, IndexView &v)
+{
+    if (occ != kOcc64 && occ != kOcc80) return -20;
+    if (occ == kOcc80 && !ix.blocks80) return -20;
+    v.blk = (const uint4 *)(occ == kOcc64 ? ix.blocks : ix.blocks80);
+    v.primary = ix.primary;
+    v.seq_len = ix.seq_len;
+    for (int c = 0; c < 4; ++c) v.C[c] = ix.L2[c];
+    memcpy(v.sb, occ == kOcc64 ? ix.sb : ix.sb80, sizeof(v.sb));
     return 0;
 }
 
@@ -268,11 +356,7 @@ int dev_search(const DevIndex &ix, DevJob &job, const TierCfg &cfg, const int32_
     if (n == 0) return 0;
     KArgs a;
     memset(&a, 0, sizeof(a));
-    a.ix.blk = (const uint4 *)ix.blocks;
-    a.ix.primary = ix.primary;
-    a.ix.seq_len = ix.seq_len;
-    for (int c = 0; c < 4; ++c) a.ix.C[c] = ix.L2[c];
-    memcpy(a.ix.sb, ix.sb, sizeof(a.ix.sb));
+    if (index_view(ix, job.occ, a.ix)) return -20;
     a.query = job.query; a.off = job.off; a.bidx = job.bidx; a.maxdiff = job.maxdiff;
     a.bopt = (const BatchOpt *)job.bopt; a.seed_len = job.seed_len;
     a.list = list; a.n = n; a.persistent = cfg.persistent ? 1 : 0; a.claim = job.counters;
@@ -294,21 +378,36 @@ int dev_search(const DevIndex &ix, DevJob &job, const TierCfg &cfg, const int32_
     a.ovf = ovf; a.ovf_n = job.counters + 1;
     if (!cfg.persistent && cfg.threads < n) return -20;
     int threads = cfg.persistent ? cfg.threads : n;
-    if (job.any_wide)
-        return cfg.freelist ? launch<true, true>(a, threads, cfg.block, st) : launch<true, false>(a, threads, cfg.block, st);
-    return cfg.freelist ? launch<false, true>(a, threads, cfg.block, st) : launch<false, false>(a, threads, cfg.block, st);
+    if (job.occ == kOcc80) return launch_s<kOcc80>(a, job.any_wide, cfg.freelist, threads, cfg.block, st);
+    return launch_s<kOcc64>(a, job.any_wide, cfg.freelist, threads, cfg.block, st);
 }
 
 int dev_resident_threads(const TierCfg &cfg, bool wide, int device)
 {
     int bps = 0;
     cudaError_t e;
-    if (wide)
-        e = cfg.freelist ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<true, true, true>, cfg.block, 0)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<true, false, true>, cfg.block, 0);
-    else
-        e = cfg.freelist ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<false, true, true>, cfg.block, 0)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, search_kernel<false, false, true>, cfg.block, 0);
+    // the smallest residency over the layouts and trace modes of this tier's kernel
+    const void *fns[4];
+    if (wide && cfg.freelist) {
+        fns[0] = (const void *)search_kernel<true, true, true, kOcc64>; fns[1] = (const void *)search_kernel<true, true, false, kOcc64>;
+        fns[2] = (const void *)search_kernel<true, true, true, kOcc80>; fns[3] = (const void *)search_kernel<true, true, false, kOcc80>;
+    } else if (wide) {
+        fns[0] = (const void *)search_kernel<true, false, true, kOcc64>; fns[1] = (const void *)search_kernel<true, false, false, kOcc64>;
+        fns[2] = (const void *)search_kernel<true, false, true, kOcc80>; fns[3] = (const void *)search_kernel<true, false, false, kOcc80>;
+    } else if (cfg.freelist) {
+        fns[0] = (const void *)search_kernel<false, true, true, kOcc64>; fns[1] = (const void *)search_kernel<false, true, false, kOcc64>;
+        fns[2] = (const void *)search_kernel<false, true, true, kOcc80>; fns[3] = (const void *)search_kernel<false, true, false, kOcc80>;
+    } else {
+        fns[0] = (const void *)search_kernel<false, false, true, kOcc64>; fns[1] = (const void *)search_kernel<false, false, false, kOcc64>;
+        fns[2] = (const void *)search_kernel<false, false, true, kOcc80>; fns[3] = (const void *)search_kernel<false, false, false, kOcc80>;
+    }
+    e = cudaSuccess;
+    bps = 1 << 30;
+    for (const void *f : fns) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, cfg.block, 0) != cudaSuccess) { e = cudaErrorInvalidValue; break; }
+        bps = std::min(bps, b);
+    }
     if (e != cudaSuccess) return -22;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -324,7 +423,14 @@ int warp_resident(int device)
 {
     int bps = 0;
     size_t smem = sizeof(WarpSmem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, warp_kernel<false>, 32, smem) != cudaSuccess) return -22;
+    const void *fns[4] = {(const void *)warp_kernel<false, kOcc64>, (const void *)warp_kernel<true, kOcc64>,
+                          (const void *)warp_kernel<false, kOcc80>, (const void *)warp_kernel<true, kOcc80>};
+    bps = 1 << 30;
+    for (const void *f : fns) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, 32, smem) != cudaSuccess) return -22;
+        bps = std::min(bps, b);
+    }
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return bps * sms;
@@ -543,11 +649,7 @@ int dev_search_warp(const DevIndex &ix, DevJob &job, const WarpCfg &c, int tier,
     if (c.n_big < 0 || c.n_big > c.n_warps || (c.n_big > 0 && c.big_chunks < 1) || c.arena_chunks < 1) return -20;   // GALN_EINVAL
     WArgs a;
     memset(&a, 0, sizeof(a));
-    a.ix.blk = (const uint4 *)ix.blocks;
-    a.ix.primary = ix.primary;
-    a.ix.seq_len = ix.seq_len;
-    for (int q = 0; q < 4; ++q) a.ix.C[q] = ix.L2[q];
-    memcpy(a.ix.sb, ix.sb, sizeof(a.ix.sb));
+    if (index_view(ix, job.occ, a.ix)) return -20;
     a.query = job.query; a.off = job.off; a.bidx = job.bidx; a.maxdiff = job.maxdiff;
     a.bopt = (const BatchOpt *)job.bopt; a.seed_len = job.seed_len;
     a.list = list; a.n = n; a.claim = job.counters; a.n_warps = c.n_warps;
@@ -573,8 +675,13 @@ int dev_search_warp(const DevIndex &ix, DevJob &job, const WarpCfg &c, int tier,
     a.ovf = ovf; a.ovf_n = job.counters + 1;
     a.dbg = dbg;
     size_t smem = sizeof(WarpSmem);
-    if (job.trace) warp_kernel<true><<<n_warps, 32, smem, st>>>(a);
-    else warp_kernel<false><<<n_warps, 32, smem, st>>>(a);
+    if (job.occ == kOcc80) {
+        if (job.trace) warp_kernel<true, kOcc80><<<n_warps, 32, smem, st>>>(a);
+        else warp_kernel<false, kOcc80><<<n_warps, 32, smem, st>>>(a);
+    } else {
+        if (job.trace) warp_kernel<true, kOcc64><<<n_warps, 32, smem, st>>>(a);
+        else warp_kernel<false, kOcc64><<<n_warps, 32, smem, st>>>(a);
+    }
     GALN_CUDA(cudaGetLastError());
     return 0;
 }

@@ -58,6 +58,7 @@ __device__ __forceinline__ int next_bucket(uint64_t m0, uint64_t m1, int from)
 }
 
 // bwt_cal_width on the reversed+complemented query (the complement is undone per base)
+template <int S = kOcc64>
 __device__ __forceinline__ void cal_width(const IndexView &ix, int len, const uint8_t *q, uint64_t *w, uint32_t &fetches)
 {
     uint64_t k = 0, l = ix.seq_len;
@@ -65,33 +66,12 @@ __device__ __forceinline__ void cal_width(const IndexView &ix, int len, const ui
     for (int i = 0; i < len; ++i) {
         int c = q[i];
         c = c > 3 ? 4 : 3 - c;
-        if (c < 4) extend1(ix, c, k, l, fetches);
+        if (c < 4) extend1<S>(ix, c, k, l, fetches);
         if (k > l || c > 3) { k = 0; l = ix.seq_len; ++bid; }
         w[i] = (bid << 48) | ((l - k + 1) & kW48);
     }
     ++bid;
     w[len] = bid << 48;
-}
-
-// bwt_match_exact_alt; returns (int)(l - k + 1) or 0
-__device__ __forceinline__ int match_exact_alt(const IndexView &ix, int len, const uint8_t *q, uint64_t &k0, uint64_t &l0,
-                                               uint32_t &fetches)
-{
-    uint64_t k = k0, l = l0;
-    for (int i = len - 1; i >= 0; --i) {
-        int c = q[i];
-        if (c > 3) return 0;
-        extend1(ix, c, k, l, fetches);
-        if (k > l) return 0;
-    }
-    k0 = k; l0 = l;
-    return (int)(l - k + 1);
-}
-
-__device__ __forceinline__ uint64_t sel4(int c, uint64_t a0, uint64_t a1, uint64_t a2, uint64_t a3)
-{
-    uint64_t lo = (c & 1) ? a1 : a0, hi = (c & 1) ? a3 : a2;
-    return (c & 2) ? hi : lo;
 }
 
 struct Entry {
@@ -153,7 +133,7 @@ __device__ __forceinline__ void load_entry(const uint4 *ent, int idx, int score,
 
 // One read. q: reversed+complemented codes (0..3, 4 ambiguous). W / SW: width and seed width, already
 // computed. Records go to aln (3 uint64 each). Returns the search result (n_aln or an error code).
-template <bool WIDE, bool FREELIST, bool TRACE>
+template <bool WIDE, bool FREELIST, bool TRACE, int S = kOcc64>
 __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int max_diff0, int len, const uint8_t *q,
                                   uint64_t *W, uint64_t *SW, bool use_seed, const Workspace &ws, int slot,
                                   uint32_t fetches)
@@ -274,7 +254,7 @@ __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int ma
             }
             {
                 uint64_t ck[4], cl[4];
-                occ4_pair_u(ix, k1, l1, ck, cl, fetches);
+                occ4_pair_u<S>(ix, k1, l1, ck, cl, fetches);
                 if (walking) {
                     const int c = q[wi - 1];
                     const uint64_t kk = ix.C[c] + sel4(c, ck[0], ck[1], ck[2], ck[3]) + 1;

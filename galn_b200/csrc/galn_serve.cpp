@@ -261,7 +261,8 @@ extern "C" galn_server *galn_server_start(galn_index *ix, size_t stack_bytes, in
             delete s;
             return nullptr;
         }
-        galn::index_l2_policy(ix, c->stream);
+        galn::index_l2_policy(ix, c->stream, ix->occ);
+        c->l2_occ = ix->occ;
         s->ctxs.push_back(c);
     }
     for (auto *c : s->ctxs) s->workers.emplace_back(serve_loop, s, c);

@@ -1,10 +1,12 @@
-// galn_tune.cpp -- the autotuner: per option set, the first tier's stack depth and block size.
+// galn_tune.cpp -- the autotuner: per option set, the occurrence layout, the first tier's stack depth and
+// block size.
 //
 // The first tier's stack depth decides the split between the thread-per-read and the warp-per-read tiers:
 // a read whose search needs more stack than that leaves the thread tier and is searched by a warp. The
 // best depth depends on the options (how many reads backtrack deeply) and on the index (how long
 // exact-match chains run), so it is measured: a sample of the job's reads is searched once per candidate
-// (depth x block size) and the fastest device time wins. Results never depend on the choice; only speed
+// (layout x depth x block size) and the fastest device time wins. The layout (64 or 80 symbols per 32-byte
+// block) trades index size, which decides how much of it stays in L2, against popcounts per lookup. Results never depend on the choice; only speed
 // does. The table is keyed by the option block, so every parameter set has its own entry.
 #include <string.h>
 
@@ -31,7 +33,7 @@ uint64_t opts_key(const galn_opts *o)
 using namespace galn;
 
 extern "C" int galn_autotune(galn_index *ix, const galn_opts *o, const galn_reads *in, int max_sample, int *best_cap,
-                             int *best_block, double *best_ms)
+                             int *best_block, int *best_occ, double *best_ms)
 {
     if (!ix || !o || !in || in->n_reads < 0) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
@@ -39,33 +41,38 @@ extern "C" int galn_autotune(galn_index *ix, const galn_opts *o, const galn_read
     if (max_sample > 0 && s.n_reads > max_sample) s.n_reads = max_sample;
     static const int caps[] = {256, 512, 1024, 2048, 4096};
     static const int blocks[] = {128, 256};
-    const int saved_cap = ix->t0_cap, saved_block = ix->t0_block;
+    static const int layouts[] = {64, 80};
+    const int saved_cap = ix->t0_cap, saved_block = ix->t0_block, saved_occ = ix->occ;
     const bool saved_stats = ix->keep_stats;
     ix->keep_stats = false;
-    int bc = saved_cap, bb = saved_block;
+    int bc = saved_cap, bb = saved_block, bo = saved_occ;
     double bms = 1e300;
     int rc = 0;
-    for (int cap : caps)
-        for (int blk : blocks) {
-            ix->t0_cap = cap;
-            ix->t0_block = blk;
-            ix->tune_active = true;
-            galn_results res;
-            memset(&res, 0, sizeof(res));
-            rc = run_job(ix, ix->main, o, &s, GALN_ENGINE_PERSISTENT, &res);
-            ix->tune_active = false;
-            if (rc) break;
-            galn_results_free(&res);
-            double ms = ix->main.last.ms_device;
-            if (ms < bms) { bms = ms; bc = cap; bb = blk; }
-        }
+    for (int occ : layouts)
+        for (int cap : caps)
+            for (int blk : blocks) {
+                ix->t0_cap = cap;
+                ix->t0_block = blk;
+                ix->occ = occ;
+                ix->tune_active = true;
+                galn_results res;
+                memset(&res, 0, sizeof(res));
+                rc = run_job(ix, ix->main, o, &s, GALN_ENGINE_PERSISTENT, &res);
+                ix->tune_active = false;
+                if (rc) break;
+                galn_results_free(&res);
+                double ms = ix->main.last.ms_device;
+                if (ms < bms) { bms = ms; bc = cap; bb = blk; bo = occ; }
+            }
     ix->t0_cap = saved_cap;
     ix->t0_block = saved_block;
+    ix->occ = saved_occ;
     ix->keep_stats = saved_stats;
     if (rc) return rc;
-    ix->tuned[opts_key(o)] = std::make_pair(bc, bb);
+    ix->tuned[opts_key(o)] = galn_index::TuneChoice{bc, bb, bo};
     if (best_cap) *best_cap = bc;
     if (best_block) *best_block = bb;
+    if (best_occ) *best_occ = bo;
     if (best_ms) *best_ms = bms;
     return 0;
 }

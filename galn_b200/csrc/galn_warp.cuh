@@ -196,7 +196,7 @@ struct WWalk {
 // D->meta[lane][lp] (and to mt); its pushes are appended to this lane's staging lists (st: list L at
 // st + L * 32 * kWL; tl: list of each push kind, mismatch, gap open, gap extension); in trace mode the popped
 // entry goes to pr[lp].
-template <bool TRACE>
+template <bool TRACE, int ST>
 __device__ __forceinline__ int lane_step(const IndexView &ix, const BatchOpt &O, const WCtx &c, WarpSmem *S, WSide *D,
                                          int lane, WEnt &x, WWalk &wk, int b, uint32_t &fetches, uint4 *st, const int tl[3],
                                          uint4 *pr, int &lp, int &nl0, int &nl1, int &nl2, uint32_t &mt)
@@ -234,7 +234,7 @@ __device__ __forceinline__ int lane_step(const IndexView &ix, const BatchOpt &O,
     uint32_t df = 0;
     if (load) {
         const uint32_t f0 = fetches;
-        occ4_pair_u(ix, k1, l1, ck, cl, fetches);
+        occ4_pair_u<ST>(ix, k1, l1, ck, cl, fetches);
         df = fetches - f0;
     }
     if (load && wk.on) {
@@ -410,7 +410,7 @@ __device__ __forceinline__ uint64_t trace_pop(uint64_t h, uint32_t binfo, const 
     return h;
 }
 
-template <bool TRACE>
+template <bool TRACE, int ST>
 __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
 {
     const unsigned FULL = 0xffffffffu;
@@ -429,8 +429,8 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
     uint32_t fetches = 0;   // index blocks read by this lane (chains include discarded speculation)
     const bool use_seed = len > O.seed_len;
     if (lane == 0) {
-        cal_width(ix, len, S->q, S->W, fetches);
-        if (use_seed) cal_width(ix, O.seed_len, S->q + (len - O.seed_len), S->SW, fetches);
+        cal_width<ST>(ix, len, S->q, S->W, fetches);
+        if (use_seed) cal_width<ST>(ix, O.seed_len, S->q + (len - O.seed_len), S->SW, fetches);
     }
     __syncwarp();
     uint32_t f_alg = __shfl_sync(FULL, fetches, 0);   // algorithmic count: widths, then replayed chains
@@ -583,7 +583,7 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
                 int stop_e = 0x7fffffff;
                 if (ce >= 0) {
                     uint32_t mt = 0;
-                    const int endc = lane_step<TRACE>(ix, O, c, S, D, lane, x, wk, b, fetches, stage_lane, tl,
+                    const int endc = lane_step<TRACE, ST>(ix, O, c, S, D, lane, x, wk, b, fetches, stage_lane, tl,
                                                       prec_w + (size_t)lane * kWP, lp, nl0, nl1, nl2, mt);
                     if (endc == -2) goto next_step;          // an exact walk goes on
                     ++e_np;
@@ -945,7 +945,7 @@ __device__ __noinline__ int big_next(const WArgs &a)
     }
 }
 
-template <bool TRACE>
+template <bool TRACE, int ST>
 __global__ void __launch_bounds__(32, 16) warp_kernel(const __grid_constant__ WArgs a)
 {
     extern __shared__ __align__(16) unsigned char wsm_raw[];
@@ -965,7 +965,7 @@ __global__ void __launch_bounds__(32, 16) warp_kernel(const __grid_constant__ WA
         }
         r = __shfl_sync(0xffffffffu, r, 0);
         if (r < 0) break;
-        warp_read<TRACE>(a, r, wid, S, lane);
+        warp_read<TRACE, ST>(a, r, wid, S, lane);
     }
     if (!big && a.n_big > 0 && lane == 0) {
         __threadfence();

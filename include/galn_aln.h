@@ -197,11 +197,12 @@ int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, in
                           uint32_t *fetch, int8_t *tier, int32_t n);
 
 /* The autotuner (no reference counterpart): times the first max_sample reads (0: all) once per candidate
- * first-tier stack depth (256..4096 entries: the split between thread-per-read and warp-per-read) and block
- * size, and keeps the fastest for this option set; later searches with the same options use it. Returns
- * the choice and its device milliseconds. galn_autotune_clear forgets all choices. */
+ * occurrence layout (64 or 80 symbols per 32-byte block), first-tier stack depth (256..4096 entries: the
+ * split between thread-per-read and warp-per-read) and block size, and keeps the fastest for this option
+ * set; later searches with the same options use it. Returns the choice and its device milliseconds.
+ * galn_autotune_clear forgets all choices. */
 int galn_autotune(galn_index *ix, const galn_opts *o, const galn_reads *in, int max_sample, int *best_cap,
-                  int *best_block, double *best_ms);
+                  int *best_block, int *best_occ, double *best_ms);
 int galn_autotune_clear(galn_index *ix);
 
 /* How many of the last run's kernel launches went through a CUDA graph (no reference counterpart). */
@@ -236,6 +237,11 @@ int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks);
 /* The occurrence blocks in a persisting L2 access-policy window on the index's streams (no reference
  * counterpart; on by default; results never depend on it). */
 int galn_index_set_l2_persist(galn_index *ix, int on);
+
+/* The occurrence layout the kernels use when the autotuner has no choice for the options (no reference
+ * counterpart; 64 by default): 64 or 80 symbols per 32-byte block. The index holds both. Results never
+ * depend on it; only the per-read count of blocks read does (it counts blocks of the layout used). */
+int galn_index_set_occ_layout(galn_index *ix, int stride);
 
 /* Trace hashes on or off (on by default). The reference computes them only in its --verify mode
  * (gapw_kernel<TRACE>, src/gapw.cuh:716-795); off, the kernels skip the hash and results carry 0 in

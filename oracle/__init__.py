@@ -210,7 +210,9 @@ class Result:
         L.orc_result_dump(h, _ptr(self.n_aln), _ptr(self.pops), _ptr(self.trace), _ptr(self.peak),
                           _ptr(self.fetch128), _ptr(self.fetch64), _ptr(self.n_stacks), _ptr(self.max_diff),
                           _ptr(self.rec_off), _ptr(self.records))
-        for a in ("n_aln", "pops", "trace", "peak", "fetch128", "fetch64", "n_stacks", "max_diff"):
+        self.fetch80 = np.zeros(max(1, n), np.uint64)
+        L.orc_result_fetch80(h, _ptr(self.fetch80))
+        for a in ("n_aln", "pops", "trace", "peak", "fetch128", "fetch64", "fetch80", "n_stacks", "max_diff"):
             setattr(self, a, getattr(self, a)[:n])
         self.records = self.records[:tot]
 

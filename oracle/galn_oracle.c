@@ -99,6 +99,15 @@ static inline uint64_t fetches(const oindex_t *x, uint64_t k, uint64_t l, int sh
     return (pk >> shift) == (pl >> shift) ? 1 : 2;
 }
 
+/* the same for blocks of `size` symbols that need not be a power of two (the build's 80-symbol layout) */
+static inline uint64_t fetches_div(const oindex_t *x, uint64_t k, uint64_t l, uint64_t size)
+{
+    int hk = k != (uint64_t)-1, hl = l != (uint64_t)-1;
+    if (!hk || !hl) return (uint64_t)(hk + hl);
+    uint64_t pk = k - (k >= x->primary), pl = l - (l >= x->primary);
+    return pk / size == pl / size ? 1 : 2;
+}
+
 /* ------------------------------------------------------------------------------------------------ */
 /* per-read search state */
 
@@ -126,7 +135,7 @@ typedef struct {
     bucket_t *b;
     int nb, best;
     long n_entries, peak;
-    uint64_t pops, trace, f128, f64;
+    uint64_t pops, trace, f128, f64, f80;
     rec_t *rec; long n_rec, m_rec;
     width_t *w, *sw; int w_cap, sw_cap;
 } ws_t;
@@ -188,6 +197,7 @@ static inline void extend1(ws_t *s, const oindex_t *x, int c, uint64_t *k, uint6
 {
     s->f128 += fetches(x, *k - 1, *l, 7);
     s->f64 += fetches(x, *k - 1, *l, 6);
+    s->f80 += fetches_div(x, *k - 1, *l, 80);
     uint64_t ok = occ(x, *k - 1, c), ol = occ(x, *l, c);
     *k = x->L2[c] + ok + 1;
     *l = x->L2[c] + ol;
@@ -310,6 +320,7 @@ static int match_gap(ws_t *s, const oindex_t *x, int len, const uint8_t *q, widt
         uint64_t ck[4], cl[4];
         s->f128 += fetches(x, k - 1, l, 7);
         s->f64 += fetches(x, k - 1, l, 6);
+        s->f80 += fetches_div(x, k - 1, l, 80);
         for (int c = 0; c < 4; ++c) { ck[c] = occ(x, k - 1, c); cl[c] = occ(x, l, c); }
         uint64_t width_now = l - k + 1;
         int allow_diff = 1, allow_M = 1;
@@ -398,7 +409,7 @@ static int batch_opt(const orc_gap_opt_t *u, int max_len, ropt_t *b)
 typedef struct {
     int n;
     int32_t *n_aln, *peak, *n_stacks, *max_diff;
-    uint64_t *pops, *trace, *f128, *f64;
+    uint64_t *pops, *trace, *f128, *f64, *f80;
     rec_t **rec;
 } ores_t;
 
@@ -447,14 +458,14 @@ static void *worker(void *arg)
                 s.sw_cap = J->u->seed_len + 1;
                 s.sw = (width_t*)realloc(s.sw, (size_t)s.sw_cap * sizeof(width_t));
             }
-            s.f128 = s.f64 = 0;
+            s.f128 = s.f64 = s.f80 = 0;
             cal_width(&s, J->x, len, q, s.w);
             if (use_seed) cal_width(&s, J->x, J->u->seed_len, q + (len - J->u->seed_len), s.sw);
             s.pops = 0; s.trace = FNV_OFFSET; s.peak = 0;
             int ret = match_gap(&s, J->x, len, q, s.w, use_seed ? s.sw : NULL, &o);
             ores_t *R = J->res;
             R->n_aln[r] = ret; R->pops[r] = s.pops; R->trace[r] = s.trace; R->peak[r] = (int32_t)s.peak;
-            R->f128[r] = s.f128; R->f64[r] = s.f64; R->n_stacks[r] = ns; R->max_diff[r] = o.max_diff;
+            R->f128[r] = s.f128; R->f64[r] = s.f64; R->f80[r] = s.f80; R->n_stacks[r] = ns; R->max_diff[r] = o.max_diff;
             if (ret > 0) {
                 R->rec[r] = (rec_t*)malloc((size_t)ret * sizeof(rec_t));
                 memcpy(R->rec[r], s.rec, (size_t)ret * sizeof(rec_t));
@@ -485,7 +496,7 @@ void *orc_aln_bmax(const void *index, const orc_gap_opt_t *u, const uint8_t *que
     R->n_aln = (int32_t*)calloc(nn, 4); R->peak = (int32_t*)calloc(nn, 4);
     R->n_stacks = (int32_t*)calloc(nn, 4); R->max_diff = (int32_t*)calloc(nn, 4);
     R->pops = (uint64_t*)calloc(nn, 8); R->trace = (uint64_t*)calloc(nn, 8);
-    R->f128 = (uint64_t*)calloc(nn, 8); R->f64 = (uint64_t*)calloc(nn, 8);
+    R->f128 = (uint64_t*)calloc(nn, 8); R->f64 = (uint64_t*)calloc(nn, 8); R->f80 = (uint64_t*)calloc(nn, 8);
     R->rec = (rec_t**)calloc(nn, sizeof(rec_t*));
     ojob_t J;
     memset(&J, 0, sizeof(J));
@@ -535,6 +546,14 @@ int orc_result_dump(const void *p, int32_t *n_aln, uint64_t *pops, uint64_t *tra
 
 /* "SAI\1", the 64-byte option block, then per read int32 n_aln and n_aln 24-byte records; a read whose
  * search failed is written with 0 records (galn.cu:1250-1263) and the call returns 4 */
+/* per-read block fetches under the 80-symbol layout */
+int orc_result_fetch80(const void *res, uint64_t *fetch80)
+{
+    const ores_t *R = (const ores_t *)res;
+    for (int r = 0; r < R->n; ++r) fetch80[r] = R->f80[r];
+    return 0;
+}
+
 int orc_result_write_sai(const void *p, const orc_gap_opt_t *opt, const char *path)
 {
     const ores_t *R = (const ores_t*)p;
@@ -559,7 +578,7 @@ void orc_result_free(void *p)
     if (!R) return;
     for (int r = 0; r < R->n; ++r) free(R->rec[r]);
     free(R->rec); free(R->n_aln); free(R->peak); free(R->n_stacks); free(R->max_diff);
-    free(R->pops); free(R->trace); free(R->f128); free(R->f64);
+    free(R->pops); free(R->trace); free(R->f128); free(R->f64); free(R->f80);
     free(R);
 }
 

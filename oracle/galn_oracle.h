@@ -54,6 +54,7 @@ int64_t orc_result_total(const void *res);
 int   orc_result_dump(const void *res, int32_t *n_aln, uint64_t *pops, uint64_t *trace, int32_t *peak,
                       uint64_t *fetch128, uint64_t *fetch64, int32_t *n_stacks, int32_t *max_diff,
                       int64_t *rec_off, void *records);
+int   orc_result_fetch80(const void *res, uint64_t *fetch80);
 int   orc_result_write_sai(const void *res, const orc_gap_opt_t *opt, const char *path);
 void  orc_result_free(void *res);
 

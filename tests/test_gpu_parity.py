@@ -31,13 +31,16 @@ def index_for(refdir):
     return _ix_cache[refdir]
 
 
+@pytest.mark.parametrize("occ", [64, 80])
 @pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_golden_case(name, engine):
+def test_golden_case(name, engine, occ):
     meta = CASES[name]
     p = case_paths(name, meta)
     ix = index_for(meta["ref"])
+    ix.set_occ_layout(occ)
     res = galn_b200.aln(ix, meta["opts"], p["fq"], engine)
+    ix.set_occ_layout(64)
     expected = open(p["sai"], "rb").read()
     assert res.sai_bytes() == expected
     pr = np.load(p["per_read"])
@@ -46,17 +49,20 @@ def test_golden_case(name, engine):
     np.testing.assert_array_equal(res.trace, pr["trace"])
 
 
+@pytest.mark.parametrize("occ", [64, 80])
 @pytest.mark.parametrize("trace", [True, False])
 @pytest.mark.parametrize("warp", [(True, 16384), (True, 64), (False, 64)])
 @pytest.mark.parametrize("caps", [(16, 1, 64, 16, 1), (64, 2, 256, 128, 2), (300, 4, 128, 1000, 3)])
-def test_tier_migration_gives_same_bytes(caps, warp, trace):
+def test_tier_migration_gives_same_bytes(caps, warp, trace, occ):
     """Tiny first- and second-tier capacities push many reads through every tier (the warp tier with a
-    normal and a tiny arena, or without it); the bytes and traces stay the reference's."""
+    normal and a tiny arena, or without it), in both occurrence layouts; the bytes and traces stay the
+    reference's and the per-read block fetches are the oracle's count for the layout."""
     ix = galn_b200.Index(os.path.join(GOLDEN, "small", "ref"))
     t0_cap, t0_aln, block, t1_cap, t1_aln = caps
     ix.set_tuning(t0_cap, t0_aln, block, t1_cap, t1_aln, keep_stats=True)
     ix.set_warp_tier(*warp)
     ix.set_trace(trace)
+    ix.set_occ_layout(occ)
     for name in ("adna", "divergent", "edge_nonstop", "tiny_queue"):
         meta = CASES[name]
         p = case_paths(name, meta)
@@ -72,15 +78,18 @@ def test_tier_migration_gives_same_bytes(caps, warp, trace):
                 np.testing.assert_array_equal(res.trace, pr["trace"])
             np.testing.assert_array_equal(res.pops, pr["pops"])
             prof = ix.last_profile(len(res))
-            np.testing.assert_array_equal(prof["fetch"].astype(np.uint64), o.fetch64)
+            np.testing.assert_array_equal(prof["fetch"].astype(np.uint64), o.fetch64 if occ == 64 else o.fetch80)
         st = ix.last_stats()
         assert st["tiers"] >= 2 or name in ("edge_nonstop", "tiny_queue")
 
 
-def test_fetch_counts_match_oracle():
-    """The per-read count of 32-byte index blocks the kernels read is the oracle's algorithmic count."""
+@pytest.mark.parametrize("occ", [64, 80])
+def test_fetch_counts_match_oracle(occ):
+    """The per-read count of 32-byte index blocks the kernels read is the oracle's algorithmic count, for
+    the layout in use."""
     ix = galn_b200.Index(os.path.join(GOLDEN, "small", "ref"))
     ix.set_tuning(keep_stats=True)
+    ix.set_occ_layout(occ)
     for name in ("plain", "adna", "edge_seed"):
         meta = CASES[name]
         p = case_paths(name, meta)
@@ -90,7 +99,7 @@ def test_fetch_counts_match_oracle():
         o = oracle.aln(oracle.Index(meta and os.path.join(GOLDEN, meta["ref"], "ref.bwt")),
                        oracle.opt_bytes(oracle.parse_aln_args(meta["opts"])), rd["query"], rd["off"], rd["len"],
                        rd["batch"], 4)
-        np.testing.assert_array_equal(prof["fetch"].astype(np.uint64), o.fetch64)
+        np.testing.assert_array_equal(prof["fetch"].astype(np.uint64), o.fetch64 if occ == 64 else o.fetch80)
 
 
 def test_index_from_memory():
@@ -102,21 +111,23 @@ def test_index_from_memory():
     assert res.sai_bytes() == open(p["sai"], "rb").read()
 
 
-def _compare_with_oracle(prefix, reads, opts, engines=ENGINES, trace=True):
+def _compare_with_oracle(prefix, reads, opts, engines=ENGINES, trace=True, layouts=(64,)):
     ix = galn_b200.Index(prefix)
     ix.set_trace(trace)
     q = oracle.encode_queries(reads.seq, reads.offset)
     batch = reads.batch if reads.batch is not None else oracle.batches_for(len(reads))
     o = oracle.aln(oracle.Index(prefix + ".bwt"), oracle.opt_bytes(oracle.parse_aln_args(opts)), q, reads.offset,
                    np.diff(reads.offset).astype(np.int32), batch, 0)
-    for engine in engines:
-        res = galn_b200.aln(ix, opts, reads, engine)
-        np.testing.assert_array_equal(res.n_aln, o.n_aln)
-        np.testing.assert_array_equal(res.pops, o.pops)
-        if trace:
-            np.testing.assert_array_equal(res.trace, o.trace)
-        np.testing.assert_array_equal(res.rec_offset, o.rec_off)
-        assert res.records.tobytes() == o.records.tobytes()
+    for occ in layouts:
+        ix.set_occ_layout(occ)
+        for engine in engines:
+            res = galn_b200.aln(ix, opts, reads, engine)
+            np.testing.assert_array_equal(res.n_aln, o.n_aln)
+            np.testing.assert_array_equal(res.pops, o.pops)
+            if trace:
+                np.testing.assert_array_equal(res.trace, o.trace)
+            np.testing.assert_array_equal(res.rec_offset, o.rec_off)
+            assert res.records.tobytes() == o.records.tobytes()
 
 
 @pytest.fixture(scope="module")
@@ -141,7 +152,7 @@ def test_synthetic_against_oracle(adna_index, workload, n, seed, trace):
         r = synth.simulate_reads(ref, n, seed, 100, sub_rate=0.01, indel_rate=0.001, random_frac=0.02)
         opts = []
     reads = galn_b200.Reads(r.ascii(), r.off)
-    _compare_with_oracle(prefix, reads, opts, trace=trace)
+    _compare_with_oracle(prefix, reads, opts, trace=trace, layouts=(64, 80) if not trace else (64,))
 
 
 def test_batch_boundary_mixed_lengths(adna_index):
@@ -162,7 +173,7 @@ def test_genome_with_ambiguous_bases(tmp_path):
     prefix = str(tmp_path / "g")
     index_build.build_from_reference(ref, prefix)
     r = synth.simulate_reads(ref, 8000, 52, 150, sub_rate=lambda x: 0.001 + 0.014 * x, indel_rate=0.0005)
-    _compare_with_oracle(prefix, galn_b200.Reads(r.ascii(), r.off), [])
+    _compare_with_oracle(prefix, galn_b200.Reads(r.ascii(), r.off), [], layouts=(64, 80))
 
 
 def test_empty_and_single_read():
@@ -181,6 +192,7 @@ def test_autotune_and_graph_keep_bytes():
     reads = galn_b200.read_fastq(p["fq"])
     tune = ix.autotune(meta["opts"], reads)
     assert tune["t0_cap"] in (256, 512, 1024, 2048, 4096) and tune["block"] in (128, 256)
+    assert tune["occ"] in (64, 80)
     for _ in range(2):   # the second run updates the instantiated graph
         res = galn_b200.aln(ix, meta["opts"], reads)
         assert res.sai_bytes() == open(p["sai"], "rb").read()
