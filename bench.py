@@ -355,6 +355,9 @@ def main():
         return g.value if rc_ == 0 else None
     gather_gbs = gather_peak(4 << 30)          # HBM: a buffer 32x the L2
     gather_l2_gbs = gather_peak(32 << 20)      # L2: a buffer a quarter of it
+    ix_bytes = os.path.getsize(prefix + ".bwt")   # the occ64 index has the .bwt body's size
+    ix_pow2 = 1 << max(20, (ix_bytes - 1).bit_length())
+    gather_ix_gbs = gather_peak(ix_pow2)       # a buffer of the index's size (next power of two)
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
@@ -405,8 +408,10 @@ def main():
                      "frac_of_gather_peak": achieved / gather_gbs if gather_gbs else None,
                      "gather_l2_peak_gbs": gather_l2_gbs,
                      "frac_of_gather_l2_peak": achieved / gather_l2_gbs if gather_l2_gbs else None,
-                     "gather_peak_how": "galn_gather_peak: random 32-B sectors of a 4 GiB buffer (HBM) and of a "
-                                        "32 MiB buffer (L2), best of 5 launches each"},
+                     "gather_index_size_peak_gbs": gather_ix_gbs, "gather_index_size_bytes": ix_pow2,
+                     "frac_of_gather_index_size_peak": achieved / gather_ix_gbs if gather_ix_gbs else None,
+                     "gather_peak_how": "galn_gather_peak: random 32-B sectors of a 4 GiB buffer (HBM), a 32 MiB "
+                                        "buffer (L2) and a buffer of the index's size, best of 5 launches each"},
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,

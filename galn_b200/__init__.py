@@ -12,4 +12,4 @@ There is no CPU fallback: if the library is missing or no sm_100 device is prese
 from __future__ import annotations
 
 from .api import (GALN_ENGINE_PERSISTENT, GALN_ENGINE_PLAIN, GalnError, Index, Options, Reads, Results,  # noqa: F401
-                  Server, aln, cal_maxdiff, lib, lib_path, parse_options, read_fastq, write_sai)
+                  Server, aln, cal_maxdiff, lib, lib_path, parse_options, read_fastq, read_fastq_batches, write_sai)

@@ -71,6 +71,10 @@ def lib():
     L.galn_index_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.galn_fastq_read.argtypes = [C.c_char_p, C.POINTER(_ReadSet)]
     L.galn_read_set_free.argtypes = [C.POINTER(_ReadSet)]
+    L.galn_fastq_open.restype = vp
+    L.galn_fastq_open.argtypes = [C.c_char_p, C.POINTER(C.c_int)]
+    L.galn_fastq_next.argtypes = [vp, C.POINTER(_ReadSet)]
+    L.galn_fastq_close.argtypes = [vp]
     L.galn_results_free.argtypes = [C.POINTER(_Results)]
     L.galn_aln_run_batch.argtypes = [vp, C.POINTER(Options), C.POINTER(_Reads), C.c_int, C.POINTER(_Results)]
     L.galn_sai_write.argtypes = [C.c_char_p, C.POINTER(Options), C.POINTER(_Results)]
@@ -262,12 +266,7 @@ class Reads:
         return r, keep
 
 
-def read_fastq(path: str) -> Reads:
-    """A FASTQ/FASTA file read by the library with the reference's rules (batch ids included)."""
-    rs = _ReadSet()
-    rc = lib().galn_fastq_read(path.encode(), C.byref(rs))
-    if rc != 0:
-        raise GalnError(f"cannot read {path} ({rc})")
+def _reads_from_set(rs: _ReadSet) -> Reads:
     n = rs.reads.n_reads
     off = np.ctypeslib.as_array(C.cast(rs.reads.offset, C.POINTER(C.c_int64)), (n + 1,)).copy()
     total = int(off[-1])
@@ -278,6 +277,35 @@ def read_fastq(path: str) -> Reads:
     names = [rs.names[i].decode() for i in range(n)]
     lib().galn_read_set_free(C.byref(rs))
     return Reads(seq, off, batch, None, names)
+
+
+def read_fastq(path: str) -> Reads:
+    """A FASTQ/FASTA file read by the library with the reference's rules (batch ids included)."""
+    rs = _ReadSet()
+    rc = lib().galn_fastq_read(path.encode(), C.byref(rs))
+    if rc != 0:
+        raise GalnError(f"cannot read {path} ({rc})")
+    return _reads_from_set(rs)
+
+
+def read_fastq_batches(path: str):
+    """The same reads one bwa batch at a time (a generator of Reads; batch ids as in the whole file)."""
+    err = C.c_int(0)
+    st = lib().galn_fastq_open(path.encode(), C.byref(err))
+    if not st:
+        raise GalnError(f"cannot read {path} ({err.value})")
+    try:
+        while True:
+            rs = _ReadSet()
+            rc = lib().galn_fastq_next(st, C.byref(rs))
+            if rc != 0:
+                raise GalnError(f"cannot read {path} ({rc})")
+            if rs.reads.n_reads == 0:
+                lib().galn_read_set_free(C.byref(rs))
+                return
+            yield _reads_from_set(rs)
+    finally:
+        lib().galn_fastq_close(st)
 
 
 class Results:
@@ -343,7 +371,8 @@ def write_sai(path: str, res: Results) -> int:
 class Server:
     """Continuous-batching request loop on a resident index (galn_server_*)."""
 
-    def __init__(self, index: Index, stack_bytes: int = 0, step_reads: int | None = None, max_active: int = 64):
+    def __init__(self, index: Index, stack_bytes: int = 0, step_reads: int | None = None, max_active: int = 64,
+                 fill_reads: int = 0):
         err = C.c_int(0)
         self.index = index
         self.h = lib().galn_server_start(index.h, stack_bytes, C.byref(err))
@@ -351,6 +380,8 @@ class Server:
             raise GalnError(f"cannot start the server ({err.value})")
         if step_reads is not None:
             lib().galn_server_configure(self.h, step_reads, max_active)
+        if fill_reads:
+            lib().galn_server_set_step_fill(self.h, fill_reads)
         self._keep = {}
 
     def submit(self, args: list[str] | Options, reads: Reads) -> int:

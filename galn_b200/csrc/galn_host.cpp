@@ -120,20 +120,44 @@ extern "C" int galn_cal_maxdiff(int l, double err, double thres)
 
 namespace {
 
+// the input as a byte stream: decompressed in 4 MiB steps and parsed as it arrives; bytes already consumed
+// are dropped from the front of the buffer
 struct Src {
-    const unsigned char *p;
-    size_t n, i;
-    int getc_() { return i < n ? p[i++] : -1; }
+    gzFile fp = nullptr;
+    std::vector<unsigned char> buf;
+    size_t n = 0, i = 0;
+    bool eof = false, err = false;
+    bool fill()
+    {
+        if (eof) return false;
+        if (i > 0 && i == n) { n = 0; i = 0; }
+        else if (i > (size_t)(16 << 20)) { memmove(buf.data(), buf.data() + i, n - i); n -= i; i = 0; }
+        if (buf.size() - n < (size_t)(4 << 20)) buf.resize(std::max(buf.size() * 2, n + (size_t)(8 << 20)));
+        int r = gzread(fp, buf.data() + n, (unsigned)(buf.size() - n));
+        if (r < 0) { err = true; eof = true; return false; }
+        if (r == 0) { eof = true; return false; }
+        n += (size_t)r;
+        return true;
+    }
+    int getc_() { return (i < n || fill()) ? buf[i++] : -1; }
 };
 
 // append up to the next '\n' (consumed); drop a trailing '\r' of the whole string when longer than 1
 long read_line(Src &s, std::string &t)
 {
-    if (s.i >= s.n) return -1;
-    const unsigned char *nl = (const unsigned char *)memchr(s.p + s.i, '\n', s.n - s.i);
-    size_t e = nl ? (size_t)(nl - s.p) : s.n;
-    t.append((const char *)s.p + s.i, e - s.i);
-    s.i = nl ? e + 1 : e;
+    if (s.i >= s.n && !s.fill()) return -1;
+    for (;;) {
+        const unsigned char *p = s.buf.data() + s.i;
+        const unsigned char *nl = (const unsigned char *)memchr(p, '\n', s.n - s.i);
+        if (nl) {
+            t.append((const char *)p, (size_t)(nl - p));
+            s.i += (size_t)(nl - p) + 1;
+            break;
+        }
+        t.append((const char *)p, s.n - s.i);
+        s.i = s.n;
+        if (!s.fill()) break;
+    }
     if (t.size() > 1 && t.back() == '\r') t.pop_back();
     return (long)t.size();
 }
@@ -151,12 +175,13 @@ struct RecordReader {
             last = c;
         }
         name.clear(); seq.clear(); qual.clear();
-        if (s.i >= s.n) return -1;
-        size_t st = s.i;
-        while (s.i < s.n && !isspace(s.p[s.i])) ++s.i;
-        name.assign((const char *)s.p + st, s.i - st);
-        int delim = s.i < s.n ? s.p[s.i++] : 0;
-        if (delim != '\n') { std::string tmp; read_line(s, tmp); }
+        if (s.i >= s.n && !s.fill()) return -1;
+        int delim = 0;
+        while ((c = s.getc_()) != -1) {
+            if (isspace(c)) { delim = c; break; }
+            name.push_back((char)c);
+        }
+        if (delim && delim != '\n') { std::string tmp; read_line(s, tmp); }
         while ((c = s.getc_()) != -1 && c != '>' && c != '+' && c != '@') {
             if (c == '\n') continue;
             seq.push_back((char)c);
@@ -179,55 +204,99 @@ struct ReadSetPriv {
     std::vector<int32_t> batch;
     std::vector<std::string> names;
     std::vector<char *> name_ptrs;
+    void publish(galn_read_set *out)
+    {
+        name_ptrs.resize(names.size());
+        for (size_t i = 0; i < names.size(); ++i) name_ptrs[i] = (char *)names[i].c_str();
+        out->reads.n_reads = (int32_t)batch.size();
+        out->reads.seq = seq.data();
+        out->reads.offset = off.data();
+        out->reads.batch = batch.data();
+        out->names = name_ptrs.data();
+        out->_priv = this;
+    }
 };
 
 }  // namespace
+
+// An open input: the record reader and the bwa batch it is in (read_fastq's rules, src/host_io.c:151-205:
+// 0x40000 reads per batch, empty reads skipped, a malformed record dropped and ending its batch, and ending
+// the input when it comes first in a batch).
+struct galn_fastq_stream {
+    Src src;
+    RecordReader rr;
+    int batch = 0;
+    bool done = false;
+};
+
+// Appends the records of the current batch to P (batch ids as in the whole input); false when the input is
+// done. Stops at the batch's end.
+static bool stream_batch(galn_fastq_stream *st, ReadSetPriv *P)
+{
+    if (st->done) return false;
+    int in_batch = 0;
+    for (;;) {
+        int l = st->rr.next(st->src);
+        if (l < 0) {
+            if (in_batch == 0 || l == -1) { st->done = true; return in_batch > 0; }
+            ++st->batch;                // a malformed record ends the batch
+            return true;
+        }
+        if (st->rr.seq.empty()) continue;  // empty reads are skipped
+        P->seq.insert(P->seq.end(), st->rr.seq.begin(), st->rr.seq.end());
+        P->off.push_back((int64_t)P->seq.size());
+        P->batch.push_back(st->batch);
+        P->names.push_back(st->rr.name);
+        if (++in_batch == kBatchReads) { ++st->batch; return true; }
+    }
+}
+
+extern "C" galn_fastq_stream *galn_fastq_open(const char *path, int *err)
+{
+    if (!path) { if (err) *err = GALN_EINVAL; return nullptr; }
+    gzFile fp = gzopen(path, "rb");
+    if (!fp) { if (err) *err = GALN_EIO; return nullptr; }
+    gzbuffer(fp, 1 << 20);
+    auto *st = new galn_fastq_stream();
+    st->src.fp = fp;
+    if (err) *err = 0;
+    return st;
+}
+
+extern "C" int galn_fastq_next(galn_fastq_stream *st, galn_read_set *out)
+{
+    if (!st || !out) return GALN_EINVAL;
+    memset(out, 0, sizeof(*out));
+    auto *P = new ReadSetPriv();
+    P->off.push_back(0);
+    stream_batch(st, P);
+    if (st->src.err) { delete P; return GALN_EIO; }
+    P->publish(out);
+    return 0;
+}
+
+extern "C" int galn_fastq_close(galn_fastq_stream *st)
+{
+    if (!st) return GALN_EINVAL;
+    int rc = st->src.fp && gzclose(st->src.fp) != Z_OK ? GALN_EIO : 0;
+    delete st;
+    return rc;
+}
 
 extern "C" int galn_fastq_read(const char *path, galn_read_set *out)
 {
     if (!path || !out) return GALN_EINVAL;
     memset(out, 0, sizeof(*out));
-    gzFile fp = gzopen(path, "rb");
-    if (!fp) return GALN_EIO;
-    gzbuffer(fp, 1 << 20);
-    std::vector<unsigned char> buf;
-    size_t n = 0;
-    buf.resize(1 << 22);
-    for (;;) {
-        if (buf.size() - n < (1 << 20)) buf.resize(buf.size() * 2);
-        int r = gzread(fp, buf.data() + n, (unsigned)(buf.size() - n));
-        if (r < 0) { gzclose(fp); return GALN_EIO; }
-        if (r == 0) break;
-        n += (size_t)r;
-    }
-    if (gzclose(fp) != Z_OK) return GALN_EIO;
+    int e = 0;
+    galn_fastq_stream *st = galn_fastq_open(path, &e);
+    if (!st) return e;
     auto *P = new ReadSetPriv();
-    Src s{buf.data(), n, 0};
-    RecordReader rr;
-    int batch = 0, in_batch = 0;
     P->off.push_back(0);
-    for (;;) {
-        int l = rr.next(s);
-        if (l < 0) {
-            if (in_batch == 0 || l == -1) break;
-            ++batch; in_batch = 0;      // a malformed record ends the batch
-            continue;
-        }
-        if (rr.seq.empty()) continue;  // empty reads are skipped
-        P->seq.insert(P->seq.end(), rr.seq.begin(), rr.seq.end());
-        P->off.push_back((int64_t)P->seq.size());
-        P->batch.push_back(batch);
-        P->names.push_back(rr.name);
-        if (++in_batch == kBatchReads) { ++batch; in_batch = 0; }
-    }
-    P->name_ptrs.resize(P->names.size());
-    for (size_t i = 0; i < P->names.size(); ++i) P->name_ptrs[i] = (char *)P->names[i].c_str();
-    out->reads.n_reads = (int32_t)P->batch.size();
-    out->reads.seq = P->seq.data();
-    out->reads.offset = P->off.data();
-    out->reads.batch = P->batch.data();
-    out->names = P->name_ptrs.data();
-    out->_priv = P;
+    while (stream_batch(st, P)) {}
+    const bool bad = st->src.err;
+    const int rc = galn_fastq_close(st);
+    if (bad || rc) { delete P; return GALN_EIO; }
+    P->publish(out);
     return 0;
 }
 
@@ -390,30 +459,70 @@ extern "C" int galn_results_free(galn_results *res)
     return 0;
 }
 
+// an open .sai stream: the header is written at open, then the reads of each appended result set
+struct galn_sai_writer {
+    FILE *fp = nullptr;
+    bool own = false;
+    int err = 0;                        // 4: a read with an error code was written with 0 records; 5: I/O
+    std::vector<char> buf;
+    void put(const void *p, size_t n)
+    {
+        buf.insert(buf.end(), (const char *)p, (const char *)p + n);
+        if (buf.size() >= (1 << 20)) flush();
+    }
+    void flush()
+    {
+        if (!buf.empty() && fwrite(buf.data(), 1, buf.size(), fp) != buf.size()) err = 5;
+        buf.clear();
+    }
+};
+
+extern "C" galn_sai_writer *galn_sai_open(const char *path, const galn_opts *o, int *err)
+{
+    static_assert(sizeof(galn_opts) == 64, "gap_opt_t is 64 bytes");
+    static_assert(sizeof(galn_aln1) == 24, "bwt_aln1_t is 24 bytes");
+    if (!o) { if (err) *err = GALN_EINVAL; return nullptr; }
+    FILE *fp = path ? fopen(path, "wb") : stdout;
+    if (!fp) { if (err) *err = 5; return nullptr; }
+    auto *w = new galn_sai_writer();
+    w->fp = fp;
+    w->own = path != nullptr;
+    w->buf.reserve(1 << 20);
+    w->put("SAI\1", 4);
+    w->put(o, sizeof(*o));
+    if (err) *err = 0;
+    return w;
+}
+
+extern "C" int galn_sai_append(galn_sai_writer *w, const galn_results *res)
+{
+    if (!w || !res) return GALN_EINVAL;
+    for (int r = 0; r < res->n_reads; ++r) {
+        int32_t na = res->n_aln[r];
+        if (na < 0) { if (!w->err) w->err = 4; na = 0; }
+        w->put(&na, 4);
+        if (na > 0) w->put(res->rec + res->rec_offset[r], (size_t)na * sizeof(galn_aln1));
+    }
+    return w->err == 5 ? 5 : 0;
+}
+
+extern "C" int galn_sai_close(galn_sai_writer *w)
+{
+    if (!w) return GALN_EINVAL;
+    w->flush();
+    if (fflush(w->fp) != 0 || ferror(w->fp)) w->err = 5;
+    if (w->own && fclose(w->fp) != 0) w->err = 5;
+    const int err = w->err;
+    delete w;
+    return err;
+}
+
 extern "C" int galn_sai_write(const char *path, const galn_opts *o, const galn_results *res)
 {
     if (!o || !res) return GALN_EINVAL;
-    FILE *fp = path ? fopen(path, "wb") : stdout;
-    if (!fp) return 5;
-    static_assert(sizeof(galn_opts) == 64, "gap_opt_t is 64 bytes");
-    static_assert(sizeof(galn_aln1) == 24, "bwt_aln1_t is 24 bytes");
-    int err = 0;
-    std::vector<char> buf;
-    buf.reserve(1 << 20);
-    auto put = [&](const void *p, size_t n) {
-        buf.insert(buf.end(), (const char *)p, (const char *)p + n);
-        if (buf.size() >= (1 << 20)) { if (fwrite(buf.data(), 1, buf.size(), fp) != buf.size()) err = 5; buf.clear(); }
-    };
-    put("SAI\1", 4);
-    put(o, sizeof(*o));
-    for (int r = 0; r < res->n_reads; ++r) {
-        int32_t na = res->n_aln[r];
-        if (na < 0) { if (!err) err = 4; na = 0; }
-        put(&na, 4);
-        if (na > 0) put(res->rec + res->rec_offset[r], (size_t)na * sizeof(galn_aln1));
-    }
-    if (!buf.empty() && fwrite(buf.data(), 1, buf.size(), fp) != buf.size()) err = 5;
-    if (fflush(fp) != 0 || ferror(fp)) err = 5;
-    if (path && fclose(fp) != 0) err = 5;
-    return err;
+    int e = 0;
+    galn_sai_writer *w = galn_sai_open(path, o, &e);
+    if (!w) return e;
+    galn_sai_append(w, res);
+    return galn_sai_close(w);
 }

@@ -35,9 +35,9 @@ double now_ms()
 
 struct Chunk {                         // results of reads [r0, r0 + m) of a request
     int r0 = 0, m = 0;
-    std::vector<int32_t> n_aln;
-    std::vector<galn_aln1> rec;
-    std::vector<uint64_t> pops, trace;
+    galn::hvec<int32_t> n_aln;
+    galn::hvec<galn_aln1> rec;
+    galn::hvec<uint64_t> pops, trace;
 };
 
 struct Request {
@@ -73,6 +73,8 @@ struct galn_server {
     size_t max_queued = 1 << 16;
     int max_active = 64;
     int step_reads = 1 << 18;
+    int fill_reads = 0;                // with a step running, wait for this many reads before the next (0: start at once)
+    int running = 0;                   // steps on the device now
     int n_workers = 2;
     std::vector<galn::ExecCtx *> ctxs;
     std::vector<std::thread> workers;
@@ -134,7 +136,17 @@ static void serve_loop(galn_server *s, galn::ExecCtx *ctx)
                     if (rq->next < rq->n || (rq->n == 0 && rq->next == 0)) return true;
                 return false;
             };
-            s->cv_work.wait(lk, [&] { return s->stop || has_work(); });
+            // with a step already running, a fill target makes the next step wait until it can take that
+            // many reads (or the running step ends): fewer, fuller steps when requests arrive quickly
+            auto can_start = [&] {
+                if (s->running == 0 || s->fill_reads == 0) return true;
+                int64_t avail = 0;
+                for (Request *rq : s->active) avail += std::max(0, rq->n - rq->next);
+                for (size_t q = 0; q < s->queue.size() && (int)s->active.size() + (int)q < s->max_active; ++q)
+                    avail += s->queue[q]->n;
+                return avail >= std::min(s->fill_reads, s->step_reads);
+            };
+            s->cv_work.wait(lk, [&] { return s->stop || (has_work() && can_start()); });
             if (s->stop && !has_work()) return;
             while (!s->queue.empty() && (int)s->active.size() < s->max_active) {
                 s->active.push_back(s->queue.front());
@@ -165,6 +177,7 @@ static void serve_loop(galn_server *s, galn::ExecCtx *ctx)
                     if (rq->n == 0) rq->next = 1;   // an empty request is taken once
                 }
             }
+            if (!pieces.empty()) ++s->running;
         }
         if (pieces.empty()) continue;
         // one combined job: every request is one option set, every (request, own batch) one batch
@@ -172,19 +185,26 @@ static void serve_loop(galn_server *s, galn::ExecCtx *ctx)
         off.push_back(0);
         for (size_t p = 0; p < pieces.size(); ++p) {
             Request *rq = pieces[p].rq;
+            const int r0 = pieces[p].r0, r1 = pieces[p].r0 + pieces[p].m;
             sets.push_back(rq->opt);
             std::map<int, int> gb;   // own batch -> batch of the step
-            for (int r = pieces[p].r0; r < pieces[p].r0 + pieces[p].m; ++r) {
-                int own = rq->batch[r];
-                auto it = gb.find(own);
-                if (it == gb.end()) {
-                    it = gb.emplace(own, (int)bmax.size()).first;
-                    bmax.push_back(rq->bmax[own]);
-                    bset.push_back((int32_t)p);
+            const int64_t sbase = (int64_t)seq.size() - (r1 > r0 ? rq->off[r0] : 0);
+            if (r1 > r0) seq.insert(seq.end(), rq->seq.begin() + rq->off[r0], rq->seq.begin() + rq->off[r1]);
+            int last_own = -1, last_step = -1;
+            for (int r = r0; r < r1; ++r) {
+                const int own = rq->batch[r];
+                if (own != last_own) {
+                    auto it = gb.find(own);
+                    if (it == gb.end()) {
+                        it = gb.emplace(own, (int)bmax.size()).first;
+                        bmax.push_back(rq->bmax[own]);
+                        bset.push_back((int32_t)p);
+                    }
+                    last_own = own;
+                    last_step = it->second;
                 }
-                seq.insert(seq.end(), rq->seq.begin() + rq->off[r], rq->seq.begin() + rq->off[r + 1]);
-                off.push_back((int64_t)seq.size());
-                batch.push_back(it->second);
+                off.push_back(sbase + rq->off[r + 1]);
+                batch.push_back(last_step);
             }
         }
         galn_reads in;
@@ -204,24 +224,36 @@ static void serve_loop(galn_server *s, galn::ExecCtx *ctx)
                                      &res);
         }
         double t1 = now_ms();
+        // each piece's results, copied outside the lock (the step's results are in read order)
+        std::vector<Chunk> chunks(pieces.size());
+        {
+            int j = 0;
+            for (size_t p = 0; p < pieces.size(); ++p) {
+                Chunk &ch = chunks[p];
+                const int m = pieces[p].m;
+                ch.r0 = pieces[p].r0; ch.m = m;
+                if (rc) {
+                    ch.n_aln.assign((size_t)m, GALN_ERR_STACK);
+                    ch.pops.assign((size_t)m, 0);
+                    ch.trace.assign((size_t)m, 0);
+                } else if (m > 0) {
+                    ch.n_aln.assign(res.n_aln + j, res.n_aln + j + m);
+                    ch.pops.assign(res.n_pops + j, res.n_pops + j + m);
+                    ch.trace.assign(res.trace + j, res.trace + j + m);
+                    ch.rec.assign(res.rec + res.rec_offset[j], res.rec + res.rec_offset[j + m]);
+                }
+                j += m;
+            }
+        }
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->busy_ms += t1 - t0;
             ++s->steps;
-            int j = 0;
-            for (auto &pc : pieces) {
+            --s->running;
+            for (size_t p = 0; p < pieces.size(); ++p) {
+                auto &pc = pieces[p];
                 Request *rq = pc.rq;
-                Chunk ch;
-                ch.r0 = pc.r0; ch.m = pc.m;
-                for (int t = 0; t < pc.m; ++t, ++j) {
-                    int na = rc ? GALN_ERR_STACK : res.n_aln[j];
-                    ch.n_aln.push_back(na);
-                    ch.pops.push_back(rc ? 0 : res.n_pops[j]);
-                    ch.trace.push_back(rc ? 0 : res.trace[j]);
-                    if (!rc && na > 0)
-                        ch.rec.insert(ch.rec.end(), res.rec + res.rec_offset[j], res.rec + res.rec_offset[j + 1]);
-                }
-                rq->chunks.push_back(std::move(ch));
+                rq->chunks.push_back(std::move(chunks[p]));
                 if (rc) rq->rc = rc;
                 rq->done_reads += pc.m;
                 s->reads_done += pc.m;
@@ -276,6 +308,15 @@ extern "C" int galn_server_configure(galn_server *s, int step_reads, int max_act
     std::lock_guard<std::mutex> lk(s->mu);
     s->step_reads = step_reads;
     s->max_active = max_active;
+    return 0;
+}
+
+extern "C" int galn_server_set_step_fill(galn_server *s, int fill_reads)
+{
+    if (!s || fill_reads < 0) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->fill_reads = fill_reads;
+    s->cv_work.notify_all();
     return 0;
 }
 

@@ -107,6 +107,15 @@ typedef struct {
 int galn_fastq_read(const char *path, galn_read_set *out);
 int galn_read_set_free(galn_read_set *rs);
 
+/* The same reader one bwa batch at a time (no reference counterpart; the reference reads batches in a
+ * thread of its own, src/galn.cu:580-640): galn_fastq_next fills `out` with the next batch (batch ids as in
+ * the whole input; n_reads 0 at the end), freed with galn_read_set_free; the batches of a stream are
+ * exactly those galn_fastq_read returns. */
+typedef struct galn_fastq_stream galn_fastq_stream;
+galn_fastq_stream *galn_fastq_open(const char *path, int *err);
+int galn_fastq_next(galn_fastq_stream *s, galn_read_set *out);
+int galn_fastq_close(galn_fastq_stream *s);
+
 /* ---- results ------------------------------------------------------------------------------------------ */
 /* Per read: n_aln (>= 0, or GALN_ERR_SCORE), records rec[rec_offset[r] .. rec_offset[r+1]) in discovery
  * order (the order the reference writes them), and the instrumentation the reference's --verify compares
@@ -140,6 +149,14 @@ int galn_aln_run_batch(galn_index *ix, const galn_opts *o, const galn_reads *in,
  * write error. */
 int galn_sai_write(const char *path, const galn_opts *o, const galn_results *res);
 
+/* The same stream written in parts (no reference counterpart): open writes the header (path NULL:
+ * stdout), each append the reads of one result set in order, close returns what galn_sai_write would
+ * (0, 4 or 5). galn_sai_write is open + one append + close. */
+typedef struct galn_sai_writer galn_sai_writer;
+galn_sai_writer *galn_sai_open(const char *path, const galn_opts *o, int *err);
+int galn_sai_append(galn_sai_writer *w, const galn_results *res);
+int galn_sai_close(galn_sai_writer *w);
+
 /* ---- serving ---------------------------------------------------------------------------------------------- */
 /* A resident index serves requests with their own options and batch boundaries (continuous batching):
  * steps of up to step_reads reads are taken from all admitted requests (equal shares, then oldest first)
@@ -157,6 +174,11 @@ int galn_aln_wait(galn_server *s, int64_t id, int timeout_ms, galn_results *out)
 /* reads per step (the device workspace of one step) and requests in flight at once (no reference
  * counterpart; defaults 262144 and 64) */
 int galn_server_configure(galn_server *s, int step_reads, int max_active);
+/* While a step is on the device, start the next only once fill_reads reads (at most a step's worth) are
+ * waiting, or when the running step ends (no reference counterpart; 0, the default, starts at once):
+ * fuller steps for a caller that submits faster than the device searches, such as a file read batch by
+ * batch; results never depend on it. */
+int galn_server_set_step_fill(galn_server *s, int fill_reads);
 /* submit-to-result latency percentiles of the finished requests, requests and reads finished, device
  * busy milliseconds and steps run (no reference counterpart) */
 int galn_server_stats(galn_server *s, double *p50_ms, double *p99_ms, int64_t *n_requests, int64_t *n_reads,

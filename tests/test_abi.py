@@ -110,6 +110,48 @@ def test_fastq_reader_edge_cases(i, tmp_path):
     np.testing.assert_array_equal(mine2.seq, mine.seq)
 
 
+def _big_fastq(path, n, malformed_at=None):
+    rng = np.random.default_rng(5)
+    with open(path, "w") as f:
+        for i in range(n):
+            L = int(rng.integers(1, 40))
+            s = "".join("ACGTN"[int(x)] for x in rng.integers(0, 5, L))
+            if i == malformed_at:
+                f.write(f"@bad{i}\n{s}A\n+\n{'I' * (L + 3)}\n")
+            else:
+                f.write(f"@r{i}\n{s}\n+\n{'I' * L}\n")
+
+
+@pytest.mark.parametrize("case", list(range(len(READER_EDGE))) + ["big", "big_malformed"])
+def test_fastq_batches_equal_whole_read(case, tmp_path):
+    """Reading one bwa batch at a time gives the whole-file read's reads and batch ids, batch by batch
+    (0x40000 reads per batch; a malformed record ends its batch)."""
+    path = str(tmp_path / "b.fq")
+    if case == "big":
+        _big_fastq(path, 0x40000 + 1000)
+    elif case == "big_malformed":
+        _big_fastq(path, 0x40000 + 5000, malformed_at=1234)
+    else:
+        with open(path, "wb") as f:
+            f.write(READER_EDGE[case])
+    whole = galn_b200.read_fastq(path)
+    parts = list(galn_b200.read_fastq_batches(path))
+    n = sum(len(p) for p in parts)
+    assert n == len(whole)
+    if n:
+        np.testing.assert_array_equal(np.concatenate([p.batch for p in parts]), whole.batch)
+        seq = np.concatenate([p.seq for p in parts])
+        np.testing.assert_array_equal(seq, whole.seq)
+        lens = np.concatenate([np.diff(p.offset) for p in parts])
+        np.testing.assert_array_equal(lens, np.diff(whole.offset))
+        for p in parts:
+            assert len(set(p.batch.tolist())) == 1
+    if case == "big":
+        assert [len(p) for p in parts] == [0x40000, 1000]
+    if case == "big_malformed":
+        assert len(parts) == 3 and len(parts[0]) < 0x40000
+
+
 def test_fastq_reader_against_reference_harness(tmp_path):
     """The reference's own reader (read_fastq via the dump harness) on the reader edge cases."""
     if not oracle.ref_available():

@@ -29,11 +29,11 @@ def _requests():
     return out
 
 
-@pytest.mark.parametrize("step", [1024, 4096, 1 << 18])
-def test_mixed_requests_equal_alone_and_golden(ix, step):
+@pytest.mark.parametrize("step,fill", [(1024, 0), (4096, 0), (1 << 18, 0), (4096, 4096), (1 << 18, 1 << 18)])
+def test_mixed_requests_equal_alone_and_golden(ix, step, fill):
     reqs = _requests()
     alone = {name: galn_b200.aln(ix, opts, reads) for name, opts, reads in reqs}
-    srv = galn_b200.Server(ix, step_reads=step, max_active=64)
+    srv = galn_b200.Server(ix, step_reads=step, max_active=64, fill_reads=fill)
     try:
         ids = [(name, srv.submit(opts, reads)) for name, opts, reads in reqs]
         ids += [(name + "#2", srv.submit(opts, reads)) for name, opts, reads in reqs]   # every request twice
