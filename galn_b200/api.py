@@ -75,6 +75,9 @@ def lib():
     L.galn_fastq_open.argtypes = [C.c_char_p, C.POINTER(C.c_int)]
     L.galn_fastq_next.argtypes = [vp, C.POINTER(_ReadSet)]
     L.galn_fastq_close.argtypes = [vp]
+    L.galn_index_load_sa.argtypes = [vp, C.c_char_p]
+    L.galn_bwt_sa.argtypes = [vp, vp, C.c_int64, vp]
+    L.galn_sa2pos.argtypes = [vp, vp, vp, C.c_int64, vp, vp]
     L.galn_results_free.argtypes = [C.POINTER(_Results)]
     L.galn_aln_run_batch.argtypes = [vp, C.POINTER(Options), C.POINTER(_Reads), C.c_int, C.POINTER(_Results)]
     L.galn_sai_write.argtypes = [C.c_char_p, C.POINTER(Options), C.POINTER(_Results)]
@@ -155,6 +158,32 @@ class Index:
     def set_warp_tier(self, on: bool, arena_chunks: int = 1 << 14):
         if lib().galn_index_set_warp_tier(self.h, int(on), arena_chunks):
             raise GalnError("bad warp tier setting")
+
+    def load_sa(self, prefix: str):
+        """Put <prefix>.sa (the suffix-array samples of this index) on the device for positions."""
+        rc = lib().galn_index_load_sa(self.h, prefix.encode())
+        if rc:
+            raise GalnError(f"cannot load {prefix}.sa ({rc})")
+
+    def bwt_sa(self, rows) -> np.ndarray:
+        """bwt_sa of each suffix-array row (the forward-reverse coordinate; row 0 gives 2**64 - 1)."""
+        k = np.ascontiguousarray(rows, np.uint64)
+        out = np.zeros(max(1, len(k)), np.uint64)
+        rc = lib().galn_bwt_sa(self.h, k.ctypes.data, len(k), out.ctypes.data)
+        if rc:
+            raise GalnError(f"galn_bwt_sa failed ({rc})")
+        return out[:len(k)]
+
+    def sa2pos(self, rows, ref_len):
+        """bwa_sa2pos of each (row, reference length of the hit): (positions, strands)."""
+        k = np.ascontiguousarray(rows, np.uint64)
+        rl = np.ascontiguousarray(ref_len, np.int32)
+        pos = np.zeros(max(1, len(k)), np.uint64)
+        strand = np.zeros(max(1, len(k)), np.int8)
+        rc = lib().galn_sa2pos(self.h, k.ctypes.data, rl.ctypes.data, len(k), pos.ctypes.data, strand.ctypes.data)
+        if rc:
+            raise GalnError(f"galn_sa2pos failed ({rc})")
+        return pos[:len(k)], strand[:len(k)]
 
     def set_l2_persist(self, on: bool):
         """Keep the occurrence blocks in a persisting L2 window (on by default)."""

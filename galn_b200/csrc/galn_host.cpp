@@ -433,10 +433,82 @@ extern "C" int galn_index_close(galn_index *ix)
     if (!ix) return GALN_EINVAL;
     cudaSetDevice(ix->dev.device);
     ix->main.release();
+    galn::Buf *sa[] = {&ix->sa_samples, &ix->sa_k, &ix->sa_len, &ix->sa_pos, &ix->sa_strand};
+    for (Buf *b : sa) b->release();
     dev_index_free(ix->dev);
     if (ix->stream) cudaStreamDestroy(ix->stream);
     delete ix;
     return 0;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// suffix-array positions (samse's coordinate step)
+
+extern "C" int galn_index_load_sa(galn_index *ix, const char *prefix)
+{
+    if (!ix || !prefix) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    // bwt_restore_sa (bwa's bwt.c:421-441): primary, 4 counts (skipped), interval, seq_len, then the samples
+    // of rows intv, 2 intv, ...; row 0 (the $ row) is -1
+    const std::string fn = std::string(prefix) + ".sa";
+    FILE *fp = fopen(fn.c_str(), "rb");
+    if (!fp) return GALN_EIO;
+    uint64_t hdr[7];
+    if (fread(hdr, 8, 7, fp) != 7) { fclose(fp); return GALN_EIO; }
+    const uint64_t primary = hdr[0], intv = hdr[5], seq_len = hdr[6];
+    if (primary != ix->dev.primary || seq_len != ix->dev.seq_len || intv == 0 || (intv & (intv - 1))) {
+        fclose(fp);
+        return GALN_EIO;
+    }
+    const uint64_t n_sa = (seq_len + intv) / intv;
+    std::vector<uint64_t> sa((size_t)n_sa);
+    sa[0] = ~0ull;
+    const size_t got = n_sa > 1 ? fread(sa.data() + 1, 8, (size_t)(n_sa - 1), fp) : 0;
+    fclose(fp);
+    if (got != n_sa - 1) return GALN_EIO;
+    if (cudaSetDevice(ix->dev.device) != cudaSuccess) return GALN_ECUDA;
+    if (ix->sa_samples.ensure((size_t)n_sa * 8)) return GALN_ENOMEM;
+    if (cudaMemcpy(ix->sa_samples.p, sa.data(), (size_t)n_sa * 8, cudaMemcpyHostToDevice) != cudaSuccess) return GALN_ECUDA;
+    ix->sa_intv = intv;
+    ix->n_sa = n_sa;
+    return 0;
+}
+
+static int sa_query(galn_index *ix, const uint64_t *rows, const int32_t *ref_len, int64_t n, uint64_t *pos, int8_t *strand)
+{
+    if (!ix || n < 0 || (n > 0 && (!rows || !pos || (ref_len && !strand)))) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    if (!ix->n_sa) return GALN_EINVAL;                 // galn_index_load_sa first
+    if (n == 0) return 0;
+    if (cudaSetDevice(ix->dev.device) != cudaSuccess) return GALN_ECUDA;
+    const size_t nn = (size_t)n;
+    if (ix->sa_k.ensure(nn * 8) || ix->sa_pos.ensure(nn * 8) || (ref_len && (ix->sa_len.ensure(nn * 4) ||
+                                                                               ix->sa_strand.ensure(nn))))
+        return GALN_ENOMEM;
+    cudaStream_t st = ix->stream;
+    if (cudaMemcpyAsync(ix->sa_k.p, rows, nn * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) return GALN_ECUDA;
+    if (ref_len && cudaMemcpyAsync(ix->sa_len.p, ref_len, nn * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return GALN_ECUDA;
+    int rc = galn::dev_sa_walk(ix->dev, (const uint64_t *)ix->sa_samples.p, ix->sa_intv, (const uint64_t *)ix->sa_k.p, n,
+                               ref_len ? (const int32_t *)ix->sa_len.p : nullptr, (uint64_t *)ix->sa_pos.p,
+                               ref_len ? (int8_t *)ix->sa_strand.p : nullptr, st);
+    if (rc) return rc;
+    if (cudaMemcpyAsync(pos, ix->sa_pos.p, nn * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess) return GALN_ECUDA;
+    if (ref_len && cudaMemcpyAsync(strand, ix->sa_strand.p, nn, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return GALN_ECUDA;
+    return cudaStreamSynchronize(st) == cudaSuccess ? 0 : GALN_ECUDA;
+}
+
+extern "C" int galn_bwt_sa(galn_index *ix, const uint64_t *rows, int64_t n, uint64_t *sa)
+{
+    return sa_query(ix, rows, nullptr, n, sa, nullptr);
+}
+
+extern "C" int galn_sa2pos(galn_index *ix, const uint64_t *rows, const int32_t *ref_len, int64_t n, uint64_t *pos,
+                           int8_t *strand)
+{
+    if (!ref_len) return GALN_EINVAL;
+    return sa_query(ix, rows, ref_len, n, pos, strand);
 }
 
 extern "C" int galn_index_info(const galn_index *ix, uint64_t *seq_len, uint64_t *primary, uint64_t *device_bytes)

@@ -109,6 +109,9 @@ struct galn_index {
     bool use_graph = true;              // launch the persistent first tier through a CUDA graph
     int warp_arena = 1 << 14;           // 32-entry chunks per warp
     bool l2_persist = true;             // the occurrence blocks in a persisting L2 window
+    // suffix-array samples (<prefix>.sa) for positions; sample 0 is the $ row (-1)
+    galn::Buf sa_samples, sa_k, sa_len, sa_pos, sa_strand;
+    uint64_t sa_intv = 0, n_sa = 0;
 };
 
 namespace galn {

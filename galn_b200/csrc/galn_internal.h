@@ -104,6 +104,10 @@ size_t warp_ws_bytes(const WarpCfg &c, int n);
 constexpr int kWarpDbg = 15;   // counters of the warp tier when profiling is on
 int dev_search_warp(const DevIndex &ix, DevJob &job, const WarpCfg &c, int tier, const int32_t *list, int n,
                     int32_t *ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg);
+// bwt_sa for n rows d_k (d_ref_len NULL: the forward-reverse coordinate into d_pos) or bwa_sa2pos (with
+// d_ref_len: position and strand, ~0 for a hit across the forward/reverse boundary)
+int dev_sa_walk(const DevIndex &ix, const uint64_t *d_samples, uint64_t intv, const uint64_t *d_k, int64_t n,
+                const int32_t *d_ref_len, uint64_t *d_pos, int8_t *d_strand, cudaStream_t st);
 // Results in read order: rec_off[0..n] (exclusive scan of max(out_n, 0)) and the records gathered from
 // out_rec into rec_ord; tile_sum holds order_tile_bytes(n) bytes of scratch. Three kernels on st.
 int dev_order_results(const DevJob &job, int n, int64_t *rec_off, uint64_t *rec_ord, int64_t *tile_sum, cudaStream_t st);

@@ -436,6 +436,61 @@ int warp_resident(int device)
     return bps * sms;
 }
 
+// ---- suffix-array positions (the coordinate step of samse: bwt_sa, bwa_sa2pos) ----
+// bwt_sa (bwa's bwt.c:86-96, as used by samse/bwa_upstream/bwase.c:112-125): from row k, step back with
+// invPsi(k) = L2[c] + Occ(c, k) (c = the row's BWT symbol; the $ row goes to 0) until k is a multiple of the
+// sampling interval, then add the steps to the sample (sample 0, the $ row, is -1). One thread per query;
+// each step reads one occ64 block, which holds both the symbol and its count.
+__global__ void sa_walk_kernel(IndexView ix, const uint64_t *__restrict__ samples, uint64_t intv_mask, int intv_shift,
+                               const uint64_t *__restrict__ k_in, int64_t n, const int32_t *__restrict__ ref_len,
+                               uint64_t l_pac, uint64_t *__restrict__ pos_out, int8_t *__restrict__ strand_out)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    uint64_t k = k_in[t], sa = 0;
+    if (k > ix.seq_len) { pos_out[t] = ~0ull; if (strand_out) strand_out[t] = 0; return; }
+    while (k & intv_mask) {
+        ++sa;
+        if (k == ix.primary) { k = 0; continue; }
+        const uint64_t p = k - (k >= ix.primary);         // the row's $-free position
+        const uint4 *b = ix.blk + ((p >> 6) << 1);
+        const uint4 cnt = __ldg(b), bits = __ldg(b + 1);
+        const uint64_t p0 = (uint64_t)bits.x | ((uint64_t)bits.y << 32), p1 = (uint64_t)bits.z | ((uint64_t)bits.w << 32);
+        const int j = (int)(p & 63);
+        const int c = (int)(((p0 >> j) & 1) | (((p1 >> j) & 1) << 1));
+        const uint64_t m = j == 63 ? ~0ull : (2ull << j) - 1;
+        const uint64_t a = c & 1 ? p0 : ~p0, h = c & 2 ? p1 : ~p1;
+        const uint32_t cc = c == 0 ? cnt.x : c == 1 ? cnt.y : c == 2 ? cnt.z : cnt.w;
+        k = ix.C[c] + ix.sb[p >> 32][c] + cc + __popcll(a & h & m);
+    }
+    uint64_t pos_f = sa + samples[k >> intv_shift];
+    if (!ref_len) { pos_out[t] = pos_f; return; }
+    // bwa_sa2pos: a hit across the forward/reverse boundary has no position; on the reverse half the
+    // position is mirrored and moved to the hit's first base
+    const uint64_t rl = (uint64_t)(int64_t)ref_len[t];
+    if (pos_f < l_pac && l_pac < pos_f + rl) { pos_out[t] = ~0ull; strand_out[t] = 0; return; }
+    const bool rev = pos_f >= l_pac;
+    if (rev) pos_f = (l_pac << 1) - 1 - pos_f;
+    if (rev) pos_f = pos_f + 1 < rl ? 0 : pos_f - rl + 1;
+    pos_out[t] = pos_f;
+    strand_out[t] = rev ? 0 : 1;
+}
+
+int dev_sa_walk(const DevIndex &ix, const uint64_t *d_samples, uint64_t intv, const uint64_t *d_k, int64_t n,
+                const int32_t *d_ref_len, uint64_t *d_pos, int8_t *d_strand, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    if (intv == 0 || (intv & (intv - 1))) return -20;
+    IndexView v;
+    if (index_view(ix, kOcc64, v)) return -20;
+    int shift = 0;
+    while ((1ull << shift) < intv) ++shift;
+    const unsigned grid = (unsigned)((n + 255) / 256);
+    sa_walk_kernel<<<grid, 256, 0, st>>>(v, d_samples, intv - 1, shift, d_k, n, d_ref_len, ix.seq_len / 2, d_pos, d_strand);
+    GALN_CUDA(cudaGetLastError());
+    return 0;
+}
+
 // ---- random 32-byte gather peak (a measurement, not part of the search) ----
 // Every thread reads `per_thread` 32-byte sectors at pseudo-random sector indices of a power-of-two buffer
 // (a splitmix64 sequence per thread; independent loads, several in flight), and folds them into one word so

@@ -143,6 +143,18 @@ int galn_results_free(galn_results *res);
 /* Synchronous search of a whole read set (host buffers in, host results out). */
 int galn_aln_run_batch(galn_index *ix, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);
 
+/* ---- positions (samse's coordinate step) -----------------------------------------------------------------
+ * The next consumer of the .sai records turns a suffix-array row of a hit into a genome position
+ * (bwa_cal_pac_pos_core / bwa_sa2pos, src/samse/bwa_upstream/bwase.c:112-139): an LF walk from the row to
+ * the nearest sampled row (bwt_sa, bwa's bwt.c:86-96) on the GPU. galn_index_load_sa puts <prefix>.sa on the
+ * device (it must belong to the index's .bwt). galn_bwt_sa gives each row's suffix-array value (the
+ * forward-reverse coordinate); galn_sa2pos gives bwa_sa2pos's position and strand for a hit of ref_len
+ * reference bases (strand 1 = forward, as bwa's !is_rev; position ~0 for a hit across the forward/reverse
+ * boundary). Host arrays in and out. */
+int galn_index_load_sa(galn_index *ix, const char *prefix);
+int galn_bwt_sa(galn_index *ix, const uint64_t *rows, int64_t n, uint64_t *sa);
+int galn_sa2pos(galn_index *ix, const uint64_t *rows, const int32_t *ref_len, int64_t n, uint64_t *pos, int8_t *strand);
+
 /* ---- .sai ----------------------------------------------------------------------------------------------- */
 /* "SAI\1", the option block, then per read int32 n_aln and the records (src/sai_writer.h:9-21). A read
  * with an error code is written with 0 records and the call returns 4 (src/galn.cu:1250-1263); 5 on a

@@ -134,6 +134,10 @@ def lib():
         L.orc_result_dump.argtypes = [vp] + [vp] * 10
         L.orc_result_write_sai.argtypes = [vp, C.c_char_p, C.c_char_p]
         L.orc_result_free.argtypes = [vp]
+        L.orc_bwt_sa.restype = C.c_uint64
+        L.orc_bwt_sa.argtypes = [vp, vp, C.c_uint64, C.c_uint64]
+        L.orc_sa2pos.restype = C.c_uint64
+        L.orc_sa2pos.argtypes = [vp, vp, C.c_uint64, C.c_uint64, C.c_int, ip]
         _lib = L
     return _lib
 
@@ -157,6 +161,36 @@ class Index:
         if getattr(self, "h", None):
             lib().orc_index_free(self.h)
             self.h = None
+
+
+def load_sa(prefix: str):
+    """<prefix>.sa as bwt_restore_sa reads it (bwa's bwt.c:421-441): (samples with samples[0] = -1, interval)."""
+    raw = np.fromfile(prefix + ".sa", dtype=np.uint64)
+    intv, seq_len = int(raw[5]), int(raw[6])
+    n_sa = (seq_len + intv) // intv
+    samples = np.empty(n_sa, np.uint64)
+    samples[0] = np.uint64(2**64 - 1)
+    samples[1:] = raw[7:7 + n_sa - 1]
+    return samples, intv
+
+
+def bwt_sa(index: "Index", samples: np.ndarray, intv: int, rows) -> np.ndarray:
+    """bwt_sa of each row (the oracle's restatement)."""
+    L = lib()
+    sp = np.ascontiguousarray(samples, np.uint64)
+    return np.array([L.orc_bwt_sa(index.h, sp.ctypes.data, intv, int(k)) for k in rows], np.uint64)
+
+
+def sa2pos(index: "Index", samples: np.ndarray, intv: int, rows, ref_len):
+    """bwa_sa2pos of each (row, ref_len): (positions, strands)."""
+    L = lib()
+    sp = np.ascontiguousarray(samples, np.uint64)
+    pos, strand = [], []
+    st = C.c_int(0)
+    for k, rl in zip(rows, ref_len):
+        pos.append(L.orc_sa2pos(index.h, sp.ctypes.data, intv, int(k), int(rl), C.byref(st)))
+        strand.append(st.value)
+    return np.array(pos, np.uint64), np.array(strand, np.int8)
 
 
 def load_reads(path: str) -> dict:

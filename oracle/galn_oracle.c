@@ -90,6 +90,48 @@ static uint64_t occ(const oindex_t *x, uint64_t k, int c)
     return n;
 }
 
+/* ------------------------------------------------------------------------------------------------ */
+/* positions from suffix-array rows (samse's coordinate step) */
+
+/* the BWT symbol of row k (k != primary): the $-free position k - (k > primary), from the packed words */
+static int bwt_symbol(const oindex_t *x, uint64_t k)
+{
+    uint64_t p = k - (k > x->primary);
+    uint32_t w = x->body[(p >> 7) * 16 + 8 + ((p & 127) >> 4)];
+    return (int)((w >> ((~p & 15) << 1)) & 3);
+}
+
+/* bwt_sa (bwa's bwt.c:86-96 with bwt_invPsi, bwt.c:53-59): step back with invPsi(k) = L2[c] + Occ(c, k),
+ * the $ row going to 0, until k is a multiple of intv; samples[k / intv] + steps (samples[0] = -1) */
+uint64_t orc_bwt_sa(const void *index, const uint64_t *samples, uint64_t intv, uint64_t k)
+{
+    const oindex_t *x = (const oindex_t*)index;
+    uint64_t sa = 0;
+    while (k % intv) {
+        ++sa;
+        if (k == x->primary) { k = 0; continue; }
+        int c = bwt_symbol(x, k);
+        k = x->L2[c] + occ(x, k, c);
+    }
+    return sa + samples[k / intv];
+}
+
+/* bwa_sa2pos (src/samse/bwa_upstream/bwase.c:112-125) with bns_depos (bntseq.h:87-90); l_pac = seq_len / 2.
+ * Returns the position (or (uint64)-1 for a hit across the forward/reverse boundary), strand = !is_rev. */
+uint64_t orc_sa2pos(const void *index, const uint64_t *samples, uint64_t intv, uint64_t k, int ref_len, int *strand)
+{
+    const oindex_t *x = (const oindex_t*)index;
+    uint64_t l_pac = x->seq_len / 2;
+    uint64_t pos_f = orc_bwt_sa(index, samples, intv, k);
+    *strand = 0;
+    if (pos_f < l_pac && l_pac < pos_f + (uint64_t)(int64_t)ref_len) return (uint64_t)-1;
+    int is_rev = pos_f >= l_pac;
+    if (is_rev) pos_f = (l_pac << 1) - 1 - pos_f;
+    *strand = !is_rev;
+    if (is_rev) pos_f = pos_f + 1 < (uint64_t)(int64_t)ref_len ? 0 : pos_f - (uint64_t)(int64_t)ref_len + 1;
+    return pos_f;
+}
+
 /* fetch accounting for the roofline: blocks touched by a lookup of (k', l') under a block size */
 static inline uint64_t fetches(const oindex_t *x, uint64_t k, uint64_t l, int shift)
 {

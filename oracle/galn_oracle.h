@@ -55,6 +55,9 @@ int   orc_result_dump(const void *res, int32_t *n_aln, uint64_t *pops, uint64_t 
                       uint64_t *fetch128, uint64_t *fetch64, int32_t *n_stacks, int32_t *max_diff,
                       int64_t *rec_off, void *records);
 int   orc_result_fetch80(const void *res, uint64_t *fetch80);
+/* bwt_sa and bwa_sa2pos over the index and its .sa samples (samples[0] = -1) */
+uint64_t orc_bwt_sa(const void *index, const uint64_t *samples, uint64_t intv, uint64_t k);
+uint64_t orc_sa2pos(const void *index, const uint64_t *samples, uint64_t intv, uint64_t k, int ref_len, int *strand);
 int   orc_result_write_sai(const void *res, const orc_gap_opt_t *opt, const char *path);
 void  orc_result_free(void *res);
 

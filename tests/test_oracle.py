@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import case_paths, golden_cases
+from conftest import GOLDEN, case_paths, golden_cases
 from galn_b200 import index_build
 
 CASES = golden_cases()
@@ -64,3 +64,53 @@ def test_cal_maxdiff_known_values():
     assert oracle.cal_maxdiff(150, 0.02, np.float32(0.04)) == 6
     assert oracle.cal_maxdiff(50, 0.02, np.float32(0.01)) == 4
     assert oracle.cal_maxdiff(120, 0.02, np.float32(0.01)) == 7
+
+
+_SA = {}
+
+
+def _full_sa(prefix, tmp):
+    """The suffix array of the index's text F.revcomp(F) (rows 0..n): F as the builder packs it (N bases
+    replaced as bwa does), sorted by the fixture builder."""
+    if prefix not in _SA:
+        names, comments, seqs = index_build.read_fasta(prefix + ".fa")
+        F = index_build.write_pac_ann_amb(str(tmp / "t"), names, comments, seqs)
+        T = np.concatenate([F, (3 - F[::-1]).astype(np.uint8)])
+        _SA[prefix] = index_build.suffix_array(T, "cpu")
+    return _SA[prefix]
+
+
+def test_oracle_bwt_sa_is_the_suffix_array(tmp_path):
+    """The oracle's bwt_sa walk over the reference-built .bwt/.sa gives the suffix array itself at every row
+    (row 0, the $ suffix, is bwa's -1)."""
+    prefix = os.path.join(GOLDEN, "small", "ref")
+    ix = oracle.Index(prefix + ".bwt")
+    samples, intv = oracle.load_sa(prefix)
+    sa = _full_sa(prefix, tmp_path)
+    n = len(sa)
+    got = oracle.bwt_sa(ix, samples, intv, range(n))
+    assert got[0] == np.uint64(2**64 - 1)
+    np.testing.assert_array_equal(got[1:], sa[1:].astype(np.uint64))
+
+
+def test_oracle_sa2pos_rules(tmp_path):
+    """bwa_sa2pos on top of bwt_sa: forward hits keep their coordinate (strand 1), reverse-half hits are
+    mirrored to the first base (strand 0), hits across the forward/reverse boundary get -1."""
+    prefix = os.path.join(GOLDEN, "small", "ref")
+    ix = oracle.Index(prefix + ".bwt")
+    samples, intv = oracle.load_sa(prefix)
+    sa = _full_sa(prefix, tmp_path)
+    l_pac = (len(sa) - 1) // 2
+    rng = np.random.default_rng(3)
+    rows = rng.integers(1, len(sa), 3000)
+    rl = rng.integers(1, 200, 3000).astype(np.int32)
+    pos, strand = oracle.sa2pos(ix, samples, intv, rows, rl)
+    for k, r, p, st in zip(rows, rl, pos, strand):
+        f = int(sa[k])
+        if f < l_pac < f + r:
+            assert p == np.uint64(2**64 - 1)
+        elif f >= l_pac:
+            g = 2 * l_pac - 1 - f
+            assert st == 0 and int(p) == (0 if g + 1 < r else g - r + 1)
+        else:
+            assert st == 1 and int(p) == f
