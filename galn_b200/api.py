@@ -337,38 +337,70 @@ def read_fastq_batches(path: str):
         lib().galn_fastq_close(st)
 
 
+class _ResultsOwner:
+    """Owns a galn_results of the library; freed when the last array viewing it is gone."""
+
+    def __init__(self, r: _Results):
+        self.r = r
+
+    def __del__(self):
+        try:
+            lib().galn_results_free(C.byref(self.r))
+        except Exception:   # noqa: BLE001 -- interpreter shutdown
+            pass
+
+
+def _view(owner: _ResultsOwner, addr: int, ctype, n: int, dtype) -> np.ndarray:
+    """A numpy array over n items of the owner's memory at addr; it keeps the owner alive."""
+    buf = (ctype * n).from_address(addr)
+    buf._owner = owner
+    return np.frombuffer(buf, dtype)
+
+
 class Results:
+    """Per-read results of one search. The arrays are views of the library's result memory (no copy); it is
+    freed when the Results and every array taken from it are gone."""
+
     def __init__(self, r: _Results, opts: Options):
         n = r.n_reads
         self.opts = opts
         if n == 0:
+            lib().galn_results_free(C.byref(r))
             self.n_aln = np.zeros(0, np.int32)
             self.rec_offset = np.zeros(1, np.int64)
             self.records = np.zeros(0, REC_DTYPE)
             self.pops = np.zeros(0, np.uint64)
             self.trace = np.zeros(0, np.uint64)
             return
-        self.n_aln = np.ctypeslib.as_array(r.n_aln, (n,)).copy()
-        self.rec_offset = np.ctypeslib.as_array(r.rec_offset, (n + 1,)).copy()
+        owner = _ResultsOwner(r)
+        self.n_aln = _view(owner, C.cast(r.n_aln, C.c_void_p).value, C.c_int32, n, np.int32)
+        self.rec_offset = _view(owner, C.cast(r.rec_offset, C.c_void_p).value, C.c_int64, n + 1, np.int64)
         tot = int(self.rec_offset[-1])
-        self.records = (np.frombuffer((C.c_char * (24 * tot)).from_address(r.rec), REC_DTYPE).copy()
-                        if tot else np.zeros(0, REC_DTYPE))
-        self.pops = np.ctypeslib.as_array(r.n_pops, (n,)).copy()
-        self.trace = np.ctypeslib.as_array(r.trace, (n,)).copy()
+        self.records = _view(owner, r.rec, C.c_char, 24 * tot, REC_DTYPE) if tot else np.zeros(0, REC_DTYPE)
+        self.pops = _view(owner, C.cast(r.n_pops, C.c_void_p).value, C.c_uint64, n, np.uint64)
+        self.trace = _view(owner, C.cast(r.trace, C.c_void_p).value, C.c_uint64, n, np.uint64)
 
     def __len__(self):
         return len(self.n_aln)
 
     def sai_bytes(self) -> bytes:
-        out = [b"SAI\x01", bytes(self.opts)]
-        for r in range(len(self.n_aln)):
-            na = int(self.n_aln[r])
-            if na < 0:
-                na = 0
-            out.append(np.int32(na).tobytes())
-            if na:
-                out.append(self.records[self.rec_offset[r]:self.rec_offset[r] + na].tobytes())
-        return b"".join(out)
+        """The .sai stream: header, then per read int32 n_aln (0 for an error code) and its records."""
+        n = len(self.n_aln)
+        na = np.maximum(self.n_aln, 0).astype(np.int64)
+        tot = int(na.sum())
+        hdr = b"SAI\x01" + bytes(self.opts)
+        out = np.empty(len(hdr) + 4 * n + 24 * tot, np.uint8)
+        out[:len(hdr)] = np.frombuffer(hdr, np.uint8)
+        first = np.zeros(n + 1, np.int64)            # each read's first record in the output order
+        first[1:] = np.cumsum(na)
+        at = len(hdr) + 4 * np.arange(n, dtype=np.int64) + 24 * first[:-1]
+        out[at[:, None] + np.arange(4)] = na.astype(np.int32).view(np.uint8).reshape(n, 4)
+        if tot:
+            owner = np.repeat(np.arange(n), na)
+            src = np.repeat(self.rec_offset[:-1], na) + (np.arange(tot) - np.repeat(first[:-1], na))
+            dst = len(hdr) + 4 * (owner + 1) + 24 * np.arange(tot, dtype=np.int64)
+            out[dst[:, None] + np.arange(24)] = self.records[src].view(np.uint8).reshape(tot, 24)
+        return out.tobytes()
 
     def write_sai(self, path: str) -> int:
         with open(path, "wb") as f:
@@ -387,8 +419,7 @@ def aln(index: Index, args: list[str] | Options, reads: Reads | str,
     rc = lib().galn_aln_run_batch(index.h, C.byref(opts), C.byref(cr), engine, C.byref(res))
     if rc != 0:
         raise GalnError(f"galn_aln_run_batch failed ({rc})")
-    out = Results(res, opts)
-    lib().galn_results_free(C.byref(res))
+    out = Results(res, opts)   # takes ownership of the library's result memory
     del keep
     return out
 
@@ -427,8 +458,7 @@ class Server:
         rc = lib().galn_aln_wait(self.h, rid, timeout_ms, C.byref(res))
         if rc != 0:
             raise GalnError(f"request {rid} failed ({rc})")
-        out = Results(res, self._keep.pop(rid))
-        lib().galn_results_free(C.byref(res))
+        out = Results(res, self._keep.pop(rid))   # takes ownership
         return out
 
     def stats(self) -> dict:

@@ -19,7 +19,9 @@
 
 #include <algorithm>
 #include <chrono>
+#include <functional>
 #include <numeric>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -67,22 +69,72 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     cudaStream_t st = ctx.stream;
     ECK(cudaSetDevice(ix->dev.device));
 
-    // ---- per-read lengths, batches, options ----
-    std::vector<int32_t> bid((size_t)std::max(n, 1));
+    // ---- per-read lengths, batches, options: a few passes over the reads, on several host threads ----
+    size_t nn = (size_t)std::max(n, 1);
+    RCK(B.h_off.ensure((nn + 1) * 8));
+    RCK(B.h_list.ensure(nn * 4 * 3));
+    const int64_t total = n > 0 ? in->offset[n] - in->offset[0] : 0;
+    const int64_t base = n > 0 ? in->offset[0] : 0;
+    int64_t *h_off = (int64_t *)B.h_off.p;
+    int32_t *h_bid = (int32_t *)B.h_list.p, *h_md = h_bid + nn, *h_list = h_md + nn;
+    const int32_t *bid = h_bid, *maxdiff = h_md;
+    const int T = n >= (1 << 16) ? (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    auto par = [&](const std::function<void(int, int, int)> &fn) {
+        if (T == 1) { fn(0, n, 0); return; }
+        std::vector<std::thread> th;
+        for (int t = 0; t < T; ++t)
+            th.emplace_back(fn, (int)((int64_t)n * t / T), (int)((int64_t)n * (t + 1) / T), t);
+        for (auto &x : th) x.join();
+    };
+    // pass 1: lengths, batch ids, offsets; per thread the longest read and size of each batch, the lengths seen
+    struct Part {
+        int max_len = 0;
+        bool bad = false, sorted = true;
+        std::vector<int> bmax, bcount;
+        std::vector<uint8_t> seen;
+    };
+    std::vector<Part> parts((size_t)T);
+    par([&](int r0, int r1, int t) {
+        Part &P = parts[(size_t)t];
+        P.seen.assign(65536, 0);
+        int prev = -1;
+        for (int r = r0; r < r1; ++r) {
+            const int64_t len = in->offset[r + 1] - in->offset[r];
+            const int b = in->batch ? in->batch[r] : r / kBatchReads;
+            if (len < 0 || len > 65535 || b < 0) { P.bad = true; return; }
+            h_bid[r] = b;
+            h_off[r] = in->offset[r] - base;
+            if (b < prev) P.sorted = false;
+            prev = b;
+            if ((size_t)b >= P.bmax.size()) { P.bmax.resize((size_t)b + 1, 0); P.bcount.resize((size_t)b + 1, 0); }
+            P.bmax[(size_t)b] = std::max(P.bmax[(size_t)b], (int)len);
+            ++P.bcount[(size_t)b];
+            P.max_len = std::max(P.max_len, (int)len);
+            P.seen[(size_t)len] = 1;
+        }
+    });
+    if (n >= 0) h_off[n] = total;
     int n_batches = 0, max_len = 0;
-    for (int r = 0; r < n; ++r) {
-        int64_t len = in->offset[r + 1] - in->offset[r];
-        if (len < 0 || len > 65535) return GALN_EINVAL;
-        int b = in->batch ? in->batch[r] : r / kBatchReads;
-        if (b < 0) return GALN_EINVAL;
-        bid[r] = b;
-        n_batches = std::max(n_batches, b + 1);
-        max_len = std::max(max_len, (int)len);
+    bool sorted = true;
+    for (int t = 0; t < T; ++t) {
+        const Part &P = parts[(size_t)t];
+        if (P.bad) return GALN_EINVAL;
+        n_batches = std::max(n_batches, (int)P.bmax.size());
+        max_len = std::max(max_len, P.max_len);
+        sorted = sorted && P.sorted;
+        if (t > 0 && sorted) {   // batch ids across the threads' boundary
+            const int r = (int)((int64_t)n * t / T);
+            if (r > 0 && r < n && h_bid[r] < h_bid[r - 1]) sorted = false;
+        }
     }
     // the longest read of each batch: given by the caller when these reads are a shard of a larger input
     if (in->batch_max_len && in->n_batches > n_batches) n_batches = in->n_batches;
-    std::vector<int> bmax((size_t)std::max(n_batches, 1), 0);
-    for (int r = 0; r < n; ++r) bmax[bid[r]] = std::max(bmax[bid[r]], (int)(in->offset[r + 1] - in->offset[r]));
+    std::vector<int> bmax((size_t)std::max(n_batches, 1), 0), bcount((size_t)std::max(n_batches, 1), 0);
+    for (const Part &P : parts)
+        for (size_t b = 0; b < P.bmax.size(); ++b) {
+            bmax[b] = std::max(bmax[b], P.bmax[b]);
+            bcount[b] += P.bcount[b];
+        }
     if (in->batch_max_len) {
         if (in->n_batches < n_batches) return GALN_EINVAL;
         for (int b = 0; b < n_batches; ++b) bmax[b] = std::max(bmax[b], (int)in->batch_max_len[b]);
@@ -117,36 +169,39 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
         max_stacks = std::max(max_stacks, h.n_stacks);
         if (h.max_gapo > 126 || h.max_gape > 126) wide = true;
     }
-    std::vector<int32_t> maxdiff((size_t)std::max(n, 1));
+    // bwa_cal_maxdiff by read length: a table per option set with -n as a fraction, over the lengths present
+    std::vector<std::vector<int32_t>> md_tab((size_t)n_sets);
     {
-        // bwa_cal_maxdiff by read length, one table per distinct -n fraction among the option sets
-        std::vector<float> fnrs;
-        std::vector<std::vector<int32_t>> tabs;
-        for (int r = 0; r < n; ++r) {
-            const int len = (int)(in->offset[r + 1] - in->offset[r]);
-            const galn_opts *o = bset[bid[r]];
-            int md;
-            if (o->fnr > 0.0) {
-                size_t t = 0;
-                while (t < fnrs.size() && memcmp(&fnrs[t], &o->fnr, 4) != 0) ++t;
-                if (t == fnrs.size()) {
-                    fnrs.push_back(o->fnr);
-                    tabs.emplace_back((size_t)max_len + 1, -1);
-                }
-                int32_t &slot = tabs[t][(size_t)len];
-                if (slot < 0) slot = galn_cal_maxdiff(len, 0.02, o->fnr);
-                md = slot;
-            } else md = bopt[bid[r]].max_diff;
-            maxdiff[r] = md;
-            if (md > 125) wide = true;
+        std::vector<uint8_t> seen((size_t)max_len + 1, 0);
+        for (const Part &P : parts)
+            for (int L = 0; L <= max_len; ++L) seen[(size_t)L] |= P.seen[(size_t)L];
+        for (int k = 0; k < n_sets; ++k) {
+            if (!(sets[k].fnr > 0.0)) continue;
+            int same = -1;   // an earlier set with the same fraction shares its table
+            for (int j = 0; j < k && same < 0; ++j)
+                if (sets[j].fnr > 0.0 && memcmp(&sets[j].fnr, &sets[k].fnr, 4) == 0) same = j;
+            if (same >= 0) { md_tab[(size_t)k] = md_tab[(size_t)same]; continue; }
+            md_tab[(size_t)k].assign((size_t)max_len + 1, 0);
+            for (int L = 0; L <= max_len; ++L)
+                if (seen[(size_t)L]) md_tab[(size_t)k][(size_t)L] = galn_cal_maxdiff(L, 0.02, sets[k].fnr);
         }
     }
+    // pass 2: each read's max_diff
+    std::vector<uint8_t> wide_t((size_t)T, 0);
+    par([&](int r0, int r1, int t) {
+        for (int r = r0; r < r1; ++r) {
+            const int b = h_bid[r];
+            const int k = batch_set ? batch_set[b] : 0;
+            const int md = sets[k].fnr > 0.0 ? md_tab[(size_t)k][(size_t)(in->offset[r + 1] - in->offset[r])]
+                                             : bopt[(size_t)b].max_diff;
+            h_md[r] = md;
+            if (md > 125) wide_t[(size_t)t] = 1;
+        }
+    });
+    for (uint8_t w : wide_t) wide = wide || w;
     for (auto &h : bopt) h.wide = wide ? 1 : 0;
 
     // ---- device buffers ----
-    const int64_t total = n > 0 ? in->offset[n] - in->offset[0] : 0;
-    const int64_t base = n > 0 ? in->offset[0] : 0;
-    size_t nn = (size_t)std::max(n, 1);
     RCK(B.seq.ensure((size_t)std::max<int64_t>(total, 1)));
     RCK(B.query.ensure((size_t)std::max<int64_t>(total, 1)));
     RCK(B.off.ensure((nn + 1) * 8));
@@ -167,21 +222,14 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     int64_t rec_cap = (int64_t)n * 2 + 65536;
     RCK(B.out_rec.ensure((size_t)rec_cap * 24));
     rec_cap = (int64_t)(B.out_rec.n / 24);
-    // host staging
-    RCK(B.h_off.ensure((nn + 1) * 8));
-    RCK(B.h_list.ensure(nn * 4 * 3));
-    int64_t *h_off = (int64_t *)B.h_off.p;
-    for (int r = 0; r <= n; ++r) h_off[r] = in->offset[r] - base;
-    int32_t *h_bid = (int32_t *)B.h_list.p, *h_md = h_bid + nn, *h_list = h_md + nn;
-    memcpy(h_bid, bid.data(), (size_t)n * 4);
-    memcpy(h_md, maxdiff.data(), (size_t)n * 4);
     // reads ordered by batch (stable): each batch is one contiguous segment of the list
     std::vector<int> bstart((size_t)n_batches + 1, 0);
-    for (int r = 0; r < n; ++r) ++bstart[bid[r] + 1];
-    for (int b = 0; b < n_batches; ++b) bstart[b + 1] += bstart[b];
-    {
+    for (int b = 0; b < n_batches; ++b) bstart[(size_t)b + 1] = bstart[(size_t)b] + bcount[(size_t)b];
+    if (sorted) {
+        par([&](int r0, int r1, int) { for (int r = r0; r < r1; ++r) h_list[r] = r; });
+    } else {
         std::vector<int> fill(bstart.begin(), bstart.end() - 1);
-        for (int r = 0; r < n; ++r) h_list[fill[bid[r]]++] = r;
+        for (int r = 0; r < n; ++r) h_list[fill[(size_t)bid[r]]++] = r;
     }
     if (total > 0) ECK(cudaMemcpyAsync(B.seq.p, in->seq + base, (size_t)total, cudaMemcpyHostToDevice, st));
     ECK(cudaMemcpyAsync(B.off.p, h_off, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice, st));
@@ -528,12 +576,17 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     P->rec_off[0] = 0;
     cudaError_t ce = cudaSuccess;
     if (n > 0) {
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(P->n_aln.data(), job.out_n, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(P->rec_off.data(), B.rec_off.p, ((size_t)n + 1) * 8, cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess && n_rec)
-            ce = cudaMemcpyAsync(P->rec.data(), B.rec_ord.p, (size_t)n_rec * 24, cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(P->pops.data(), job.out_pops, (size_t)n * 8, cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(P->trace.data(), job.out_trace, (size_t)n * 8, cudaMemcpyDeviceToHost, st);
+        // one copy into reused pinned memory, then the result arrays filled by several host threads
+        const size_t b_n = (size_t)n * 4, b_off = ((size_t)n + 1) * 8, b_rec = (size_t)n_rec * 24, b_p = (size_t)n * 8;
+        const size_t o_off = (b_n + 255) & ~(size_t)255, o_rec = o_off + ((b_off + 255) & ~(size_t)255);
+        const size_t o_pops = o_rec + ((b_rec + 255) & ~(size_t)255), o_trace = o_pops + ((b_p + 255) & ~(size_t)255);
+        if (B.h_res.ensure(o_trace + b_p)) { delete P; return GALN_ENOMEM; }
+        char *hr = (char *)B.h_res.p;
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hr, job.out_n, b_n, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hr + o_off, B.rec_off.p, b_off, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess && n_rec) ce = cudaMemcpyAsync(hr + o_rec, B.rec_ord.p, b_rec, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hr + o_pops, job.out_pops, b_p, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hr + o_trace, job.out_trace, b_p, cudaMemcpyDeviceToHost, st);
         if (ce == cudaSuccess && ix->keep_stats) {
             S.fetch.resize(nn);
             S.tier_of.resize(nn);
@@ -541,6 +594,26 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
             if (ce == cudaSuccess) ce = cudaMemcpyAsync(S.tier_of.data(), job.out_tier, (size_t)n, cudaMemcpyDeviceToHost, st);
         }
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+        if (ce == cudaSuccess) {
+            struct Piece { void *dst; const char *src; size_t bytes; };
+            const Piece pieces[5] = {{P->n_aln.data(), hr, b_n}, {P->rec_off.data(), hr + o_off, b_off},
+                                     {P->rec.data(), hr + o_rec, b_rec}, {P->pops.data(), hr + o_pops, b_p},
+                                     {P->trace.data(), hr + o_trace, b_p}};
+            const size_t all = b_n + b_off + b_rec + 2 * b_p;
+            const int TT = all >= ((size_t)16 << 20) ? (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+            auto copy_part = [&](int t) {   // thread t copies its share of every array
+                for (const Piece &pc : pieces) {
+                    const size_t c0 = pc.bytes * (size_t)t / (size_t)TT, c1 = pc.bytes * (size_t)(t + 1) / (size_t)TT;
+                    if (c1 > c0) memcpy((char *)pc.dst + c0, pc.src + c0, c1 - c0);
+                }
+            };
+            if (TT == 1) copy_part(0);
+            else {
+                std::vector<std::thread> th;
+                for (int t = 0; t < TT; ++t) th.emplace_back(copy_part, t);
+                for (auto &x : th) x.join();
+            }
+        }
     }
     if (ce != cudaSuccess) {
         delete P;

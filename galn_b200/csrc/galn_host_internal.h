@@ -41,16 +41,16 @@ struct Buf {
 struct JobBufs {
     Buf seq, query, off, bidx, maxdiff, bopt, out_n, out_off, out_pops, out_trace, out_peak, out_fetch, out_tier,
         out_rec, rec_top, list_a, list_b, counters, ws, dbg, rec_off, rec_ord, tile;
-    Buf h_n, h_off, h_pops, h_trace, h_rec, h_list, h_misc;
+    Buf h_n, h_off, h_pops, h_trace, h_rec, h_list, h_misc, h_res;
     JobBufs()
     {
-        h_n.host = h_off.host = h_pops.host = h_trace.host = h_rec.host = h_list.host = h_misc.host = true;
+        h_n.host = h_off.host = h_pops.host = h_trace.host = h_rec.host = h_list.host = h_misc.host = h_res.host = true;
     }
     void release()
     {
         Buf *all[] = {&seq, &query, &off, &bidx, &maxdiff, &bopt, &out_n, &out_off, &out_pops, &out_trace, &out_peak,
                       &out_fetch, &out_tier, &dbg, &out_rec, &rec_top, &list_a, &list_b, &counters, &ws, &rec_off,
-                      &rec_ord, &tile, &h_n, &h_off, &h_pops, &h_trace, &h_rec, &h_list, &h_misc};
+                      &rec_ord, &tile, &h_n, &h_off, &h_pops, &h_trace, &h_rec, &h_list, &h_misc, &h_res};
         for (Buf *b : all) b->release();
     }
 };
