@@ -299,15 +299,26 @@ __device__ __forceinline__ int lane_step(const IndexView &ix, const BatchOpt &O,
         const uint64_t h1_del = w1b + gap1;
         const uint64_t h0_mm = (w0b + (1ull << 54)) | ((uint64_t)(uint32_t)i << 38) | ((uint64_t)kStM << 61);
         const int base = S->q[i];
+        // the children in mismatch order: rk[j], rl[j] = child of base (base + j) & 3 (j = 4: the read's own base,
+        // the exact child), a rotation by base & 3 done once with compile-time indices after it
+        uint64_t rk[5], rl[5];
+        {
+            const int r = base & 3;
+            uint64_t a0 = kk[0], a1 = kk[1], a2 = kk[2], a3 = kk[3], b0 = ll[0], b1 = ll[1], b2 = ll[2], b3 = ll[3];
+            if (r & 1) { uint64_t t = a0; a0 = a1; a1 = a2; a2 = a3; a3 = t; t = b0; b0 = b1; b1 = b2; b2 = b3; b3 = t; }
+            if (r & 2) { uint64_t t = a0; a0 = a2; a2 = t; t = a1; a1 = a3; a3 = t; t = b0; b0 = b2; b2 = t; t = b1; b1 = b3; b3 = t; }
+            rk[1] = a1; rk[2] = a2; rk[3] = a3; rk[4] = a0;   // a_j = child of base (r + j) & 3
+            rl[1] = b1; rl[2] = b2; rl[3] = b3; rl[4] = b0;
+            rk[0] = rl[0] = 0;
+        }
         // which slots push: bit 0 the kept-interval gap child, bits 1-4 deletions by base, bits 5-8 mismatches
         uint32_t slots = self_ok ? 1u : 0u;
 #pragma unroll
         for (int q = 0; q < 4; ++q) if (del_ok && kk[q] <= ll[q]) slots |= 2u << q;
 #pragma unroll
         for (int j = 1; j <= 4; ++j) {
-            const int q = (base + j) & 3;
             const bool mm = j != 4 || base > 3;
-            if (mm_ok && mm && sel4(q, kk[0], kk[1], kk[2], kk[3]) <= sel4(q, ll[0], ll[1], ll[2], ll[3])) slots |= 32u << (j - 1);
+            if (mm_ok && mm && rk[j] <= rl[j]) slots |= 32u << (j - 1);
         }
         // a push at or past n_stacks ends the read (BWTGAP_ERR_SCORE); nothing else of this pop matters then
         err = ((slots & 0x1fu) && g_bkt >= O.n_stacks) || ((slots & 0x1e0u) && m_bkt >= O.n_stacks);
@@ -321,9 +332,8 @@ __device__ __forceinline__ int lane_step(const IndexView &ix, const BatchOpt &O,
                 else if (t <= 4) {
                     w0 = (kk[t - 1] & kK38) | h0_del; w1 = (ll[t - 1] & kK38) | h1_del; L = g_list;
                 } else {
-                    const int q = (base + t - 4) & 3;
-                    w0 = (sel4(q, kk[0], kk[1], kk[2], kk[3]) & kK38) | h0_mm;
-                    w1 = (sel4(q, ll[0], ll[1], ll[2], ll[3]) & kK38) | w1b;
+                    w0 = (rk[t - 4] & kK38) | h0_mm;
+                    w1 = (rl[t - 4] & kK38) | w1b;
                     L = tl[0];
                 }
                 const int n_ = L == 0 ? nl0 : (L == 1 ? nl1 : nl2);
@@ -332,16 +342,13 @@ __device__ __forceinline__ int lane_step(const IndexView &ix, const BatchOpt &O,
                 ++npu;
             }
         }
-        const bool exact = !err && base < 4 && sel4(base, kk[0], kk[1], kk[2], kk[3]) <= sel4(base, ll[0], ll[1], ll[2], ll[3]);
+        const bool exact = !err && base < 4 && rk[4] <= rl[4];
         if (err) {   // the read ends at this pop with BWTGAP_ERR_SCORE
             mt = df << 5; endc = 3;
         } else {
             mt = npu | (exact ? 16u : 0u) | df << 5;
             endc = exact ? -1 : 0;
-            if (exact) {
-                x.k = sel4(base, kk[0], kk[1], kk[2], kk[3]); x.l = sel4(base, ll[0], ll[1], ll[2], ll[3]);
-                x.i = i; x.isdiff = 0; x.state = kStM;
-            }
+            if (exact) { x.k = rk[4]; x.l = rl[4]; x.i = i; x.isdiff = 0; x.state = kStM; }
         }
     }
     if (endc == -2) return endc;
