@@ -220,7 +220,7 @@ def main():
     ap.add_argument("--data-dir", default=None)
     ap.add_argument("--trace", action="store_true", help="compute per-read trace hashes (verification mode)")
     ap.add_argument("--t0-cap", type=int, default=1024, help="first-tier stack entries per thread")
-    ap.add_argument("--warp-arena", type=int, default=16384, help="warp-tier stack chunks (32 entries) per warp")
+    ap.add_argument("--warp-arena", type=int, default=8192, help="warp-tier stack chunks (64 entries) per warp")
     ap.add_argument("--serve-requests", type=int, default=40, help="requests in the serving run (0: none)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--autotune-sample", type=int, default=262144)

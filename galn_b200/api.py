@@ -155,7 +155,7 @@ class Index:
         if rc:
             raise GalnError(f"bad tuning ({rc})")
 
-    def set_warp_tier(self, on: bool, arena_chunks: int = 1 << 14):
+    def set_warp_tier(self, on: bool, arena_chunks: int = 1 << 13):
         if lib().galn_index_set_warp_tier(self.h, int(on), arena_chunks):
             raise GalnError("bad warp tier setting")
 

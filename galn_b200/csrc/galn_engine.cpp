@@ -420,7 +420,9 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
         // reads still queued when pass 1 ended, with big arenas for every warp
         const int aln_cap_w = 4096;
         const int kBigWarps = 128;
-        const int64_t full = (max_entries_all + 16 + 3 * 32 * 128 + kWarpMaxStacks * 32) / 32 + kWarpMaxStacks + 1;
+        // the cut-off, one wave's staged pushes and a partly filled chunk per bucket
+        const int64_t full = (max_entries_all + 16 + 3 * 32 * 128 + kWarpMaxStacks * kWarpChunk) / kWarpChunk
+                             + kWarpMaxStacks + 1;
         const int big_chunks = (int)std::min<int64_t>(std::max<int64_t>(full, ix->warp_arena), 1 << 22);
         for (int pass = 0; pass < 2 && !elig.empty(); ++pass) {
             int ne = (int)elig.size();
@@ -714,7 +716,7 @@ extern "C" int galn_index_set_occ_layout(galn_index *ix, int stride)
 
 extern "C" int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks)
 {
-    if (!ix || arena_chunks < 64) return GALN_EINVAL;
+    if (!ix || arena_chunks < 32) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
     ix->use_warp = on != 0;
     ix->warp_arena = arena_chunks;

@@ -107,7 +107,7 @@ struct galn_index {
     int occ = 64;                       // occurrence layout when the autotuner has no choice (64 or 80)
     bool tune_active = false;           // the autotuner is timing a candidate: ignore the table
     bool use_graph = true;              // launch the persistent first tier through a CUDA graph
-    int warp_arena = 1 << 14;           // 32-entry chunks per warp
+    int warp_arena = 1 << 13;           // chunks (kWarpChunk entries) per warp
     bool l2_persist = true;             // the occurrence blocks in a persisting L2 window
     // suffix-array samples (<prefix>.sa) for positions; sample 0 is the $ row (-1)
     galn::Buf sa_samples, sa_k, sa_len, sa_pos, sa_strand;

@@ -95,6 +95,7 @@ int dev_resident_threads(const TierCfg &cfg, bool wide, int device);
 // ovf[]; reads still queued when it ends are read back through warp_queue(). ws_mem holds
 // warp_ws_bytes(cfg, n) bytes.
 constexpr int kWarpMaxLen = 256, kWarpMaxStacks = 256;
+constexpr int kWarpChunk = 64;        // stack entries per chunk of a warp's arena
 struct WarpCfg {
     int n_warps = 0, arena_chunks = 0, aln_cap = 0, n_big = 0, big_chunks = 0;
 };

@@ -25,13 +25,14 @@
 // are committed to their buckets in replay order (per bucket: entry order, then pop order), so every
 // bucket is the same LIFO as in the sequential search.
 //
-// Storage: each bucket is a chain of 32-entry chunks in the warp's arena (global memory), with its top
+// Storage: each bucket is a chain of 64-entry chunks in the warp's arena (global memory), with its top
 // chunk, fill and entry count in shared memory. Widths, the query, the wave's entries and records and the
 // per-pop data are in shared memory; staged pushes (and, in trace mode, popped entries) in a per-warp
 // global staging area. Reads the tier cannot take (length > 256, n_stacks > 256, a penalty <= 0, 32-byte
 // entries) or that outgrow the arena or the record buffer go to the thread tiers (the host routes them).
 #pragma once
 
+#include "galn_internal.h"
 #include "galn_search.cuh"
 
 namespace galn {
@@ -41,7 +42,7 @@ constexpr int kWMaxLen = 256;    // read length
 constexpr int kWE = 128;         // entries per wave
 constexpr int kWP = 48;          // pops per lane per wave
 constexpr int kWL = 128;         // staged pushes per lane and target list per wave
-constexpr int kWCH = 32;         // entries per chunk
+constexpr int kWCH = kWarpChunk;  // entries per chunk
 constexpr int kWNewC = (kWCH + 32 * kWL) / kWCH + 2;   // chunks one commit may allocate
 constexpr int kWGrabPops = 6;    // an idle lane takes an entry only with room for this many pops
 constexpr int kWChain = kWE / kWCH + 2;   // chunks of the current bucket kept walked

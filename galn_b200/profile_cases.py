@@ -41,7 +41,7 @@ def warp_steady(data_dir: str) -> None:
     sub = Reads.from_strings([bytes(full.seq[full.offset[i]:full.offset[i + 1]]) for i in sel])
     sub.batch = np.zeros(len(sel), np.int32)
     ix.set_tuning(t0_cap=1024, keep_stats=False)
-    ix.set_warp_tier(True, 2048)
+    ix.set_warp_tier(True, 1024)
     args = list(opts) + ["-m", "100000"]
     for _ in range(2):
         r = aln(ix, args, sub)

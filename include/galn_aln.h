@@ -264,8 +264,8 @@ int galn_gather_peak(int device, uint64_t bytes, int repeats, double *gbs);
  * whether to keep the per-read profile. Results never depend on these values. */
 int galn_index_set_tuning(galn_index *ix, int t0_cap, int t0_aln, int t0_block, int t1_cap, int t1_aln, int keep_stats);
 
-/* The heavy-read warp tier on or off, and its stack arena per warp in 32-entry chunks (no reference
- * counterpart; on by default with 16384 chunks). Results never depend on it. */
+/* The heavy-read warp tier on or off, and its stack arena per warp in 64-entry chunks (no reference
+ * counterpart; on by default with 8192 chunks, at least 32). Results never depend on it. */
 int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks);
 
 /* The occurrence blocks in a persisting L2 access-policy window on the index's streams (no reference

@@ -51,7 +51,7 @@ def test_golden_case(name, engine, occ):
 
 @pytest.mark.parametrize("occ", [64, 80])
 @pytest.mark.parametrize("trace", [True, False])
-@pytest.mark.parametrize("warp", [(True, 16384), (True, 64), (False, 64)])
+@pytest.mark.parametrize("warp", [(True, 8192), (True, 32), (False, 32)])
 @pytest.mark.parametrize("caps", [(16, 1, 64, 16, 1), (64, 2, 256, 128, 2), (300, 4, 128, 1000, 3)])
 def test_tier_migration_gives_same_bytes(caps, warp, trace, occ):
     """Tiny first- and second-tier capacities push many reads through every tier (the warp tier with a
