@@ -42,6 +42,12 @@ class _Results(C.Structure):
                 ("_priv", C.c_void_p)]
 
 
+class BuildStats(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("primary", C.c_uint64), ("rounds", C.c_int), ("sort_passes", C.c_int),
+                ("sorted_items", C.c_uint64), ("scatter_items", C.c_uint64), ("ms_device", C.c_double),
+                ("ms_scatter", C.c_double), ("ms_files", C.c_double)]
+
+
 def lib_path() -> str:
     return os.path.join(HERE, "libgalnb200.so")
 
@@ -101,6 +107,9 @@ def lib():
                                 C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.galn_autotune_clear.argtypes = [vp]
     L.galn_last_graph_launches.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.galn_index_build_text.argtypes = [vp, C.c_uint64, C.c_char_p, C.POINTER(BuildStats)]
+    L.galn_index_build_fasta.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(BuildStats)]
+    L.galn_fasta_to_pac.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_uint64)]
     L.galn_version.restype = C.c_char_p
     _lib = L
     return L
@@ -426,6 +435,40 @@ def aln(index: Index, args: list[str] | Options, reads: Reads | str,
 
 def write_sai(path: str, res: Results) -> int:
     return res.write_sai(path)
+
+
+def _stats_dict(st: BuildStats) -> dict:
+    return {f: getattr(st, f) for f, _ in BuildStats._fields_}
+
+
+def index_fasta(fasta: str, prefix: str) -> dict:
+    """`galn index -p prefix fasta` on the current CUDA device: the five bwa index files (galn_index_build_fasta).
+    Returns the builder's statistics."""
+    st = BuildStats()
+    rc = lib().galn_index_build_fasta(fasta.encode(), prefix.encode(), C.byref(st))
+    if rc:
+        raise GalnError(f"galn_index_build_fasta failed ({rc})")
+    return _stats_dict(st)
+
+
+def fasta_to_pac(fasta: str, prefix: str) -> int:
+    """The host step of `galn index`: <prefix>.pac/.ann/.amb from a FASTA file. Returns the reference length."""
+    n = C.c_uint64()
+    rc = lib().galn_fasta_to_pac(fasta.encode(), prefix.encode(), C.byref(n))
+    if rc:
+        raise GalnError(f"galn_fasta_to_pac failed ({rc})")
+    return n.value
+
+
+def index_text(fwd: np.ndarray, prefix: str) -> dict:
+    """<prefix>.bwt and <prefix>.sa for the forward sequence fwd (codes 0..3; the text is fwd . revcomp(fwd)),
+    built on the current CUDA device (galn_index_build_text)."""
+    f = np.ascontiguousarray(fwd, dtype=np.uint8)
+    st = BuildStats()
+    rc = lib().galn_index_build_text(f.ctypes.data, len(f), prefix.encode(), C.byref(st))
+    if rc:
+        raise GalnError(f"galn_index_build_text failed ({rc})")
+    return _stats_dict(st)
 
 
 class Server:

@@ -27,8 +27,8 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "
 CXXFLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall", "-I" + os.path.join(CUDA, "include"),
             "-I" + os.path.join(ROOT, "include")]
 
-CU_SOURCES = ["galn_kernels.cu", "galn_noalloc.cu"]
-CPP_SOURCES = ["galn_host.cpp", "galn_engine.cpp", "galn_serve.cpp", "galn_tune.cpp"]
+CU_SOURCES = ["galn_kernels.cu", "galn_noalloc.cu", "galn_build_index.cu"]
+CPP_SOURCES = ["galn_host.cpp", "galn_engine.cpp", "galn_serve.cpp", "galn_tune.cpp", "galn_index_files.cpp"]
 
 
 def _headers():

@@ -1,0 +1,617 @@
+// galn_build_index.cu -- `galn index` on the GPU: the .bwt and .sa files of bwa index 0.7.19 for the text
+// T = F . revcomp(F) of a forward sequence F (codes 0..3).
+//
+// The reference builds them in src/index/gpu_index.cu:1-20 (BWT of T$ by libcubwt or its rank-based sorter,
+// then pack + interleaved Occ on the GPU, SA samples by LF walks and list ranking). This builder:
+//   1. sorts the suffixes by prefix doubling, refining only the groups still unsorted (Larsson-Sadakane):
+//      the first round sorts 21-symbol prefixes (3 bits a symbol, 0 past the end); round r sorts the
+//      unsorted suffixes i by (rank of i, rank of i + h), h = 21 * 2^(r-1), where a rank is the suffix-array
+//      index of the first suffix of its group. Every sort is a stable LSD radix sort written here: 8-bit
+//      digits, per-tile histogram, scan, and a scatter that ranks each tile's items in shared memory so
+//      each digit's run leaves the tile as one contiguous write;
+//   2. takes the BWT from the suffix array kept on the device, packs it 2 bits a symbol with the Occ counts
+//      every 128 symbols (the .bwt layout of bwt_bwtupdate_core, src/index/idxcommon.c:72-112);
+//   3. gathers every 32nd suffix-array row (the .sa layout, src/index/idxcommon.c:137-153).
+// Positions are 32-bit: texts up to 2^32 - 64 symbols (references up to about 2.1 Gbp), about 38 bytes of
+// device memory per symbol at the peak. Everything but the file writes runs on the device.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "galn_internal.h"
+
+namespace galn {
+namespace ixb {
+
+constexpr int kRThreads = 512, kRItems = 8, kRTile = kRThreads * kRItems, kRWarps = kRThreads / 32;
+constexpr int kScanThreads = 256;
+constexpr int kPrefix = 21;            // symbols in a first-round key
+constexpr int kMaxRounds = 40;         // h = 21 * 2^39 exceeds any 32-bit text
+
+struct U4 {
+    uint64_t c[4];
+};
+__host__ __device__ inline U4 operator+(const U4 &a, const U4 &b)
+{
+    return U4{{a.c[0] + b.c[0], a.c[1] + b.c[1], a.c[2] + b.c[2], a.c[3] + b.c[3]}};
+}
+
+// items a scan thread holds: 8 of 4- or 8-byte types, 2 of the 32-byte per-block counts
+template <class T>
+constexpr int scan_items() { return sizeof(T) > 8 ? 2 : 8; }
+template <class T>
+constexpr int scan_tile_n() { return kScanThreads * scan_items<T>(); }
+
+template <class T>
+struct OpSum {
+    __device__ static T id() { return T{}; }
+    __device__ static T op(const T &a, const T &b) { return a + b; }
+};
+template <class T>
+struct OpMax {
+    __device__ static T id() { return T(0); }
+    __device__ static T op(const T &a, const T &b) { return a > b ? a : b; }
+};
+
+// ---- scans (reduce, scan of the tile sums, scan of each tile with its carry-in) ----
+
+template <class T, class Op>
+__global__ void __launch_bounds__(kScanThreads) scan_reduce(const T *__restrict__ x, uint64_t n, T *__restrict__ part)
+{
+    constexpr int kItems = scan_items<T>(), kTile = scan_tile_n<T>();
+    __shared__ T s[kScanThreads];
+    const int t = threadIdx.x;
+    const uint64_t base = (uint64_t)blockIdx.x * kTile;
+    T acc = Op::id();
+    for (int j = 0; j < kItems; ++j) {
+        const uint64_t i = base + (uint64_t)j * kScanThreads + t;
+        if (i < n) acc = Op::op(acc, x[i]);
+    }
+    s[t] = acc;
+    __syncthreads();
+    for (int w = kScanThreads / 2; w > 0; w >>= 1) {
+        if (t < w) s[t] = Op::op(s[t], s[t + w]);
+        __syncthreads();
+    }
+    if (t == 0) part[blockIdx.x] = s[0];
+}
+
+// In place: inclusive (INCL) or exclusive scan of one tile, offset by carry[tile] when carry is given.
+template <class T, class Op, bool INCL>
+__global__ void __launch_bounds__(kScanThreads) scan_tile(T *__restrict__ x, uint64_t n, const T *__restrict__ carry)
+{
+    constexpr int kItems = scan_items<T>(), kTile = scan_tile_n<T>();
+    __shared__ T s[kTile];
+    __shared__ T tsum[kScanThreads];
+    const int t = threadIdx.x;
+    const uint64_t base = (uint64_t)blockIdx.x * kTile;
+    for (int j = 0; j < kItems; ++j) {
+        const uint64_t i = base + (uint64_t)j * kScanThreads + t;
+        s[j * kScanThreads + t] = i < n ? x[i] : Op::id();
+    }
+    __syncthreads();
+    T v[kItems];
+    T acc = Op::id();
+    for (int j = 0; j < kItems; ++j) {
+        v[j] = s[t * kItems + j];
+        acc = Op::op(acc, v[j]);
+    }
+    tsum[t] = acc;
+    __syncthreads();
+    for (int off = 1; off < kScanThreads; off <<= 1) {   // inclusive scan of the thread sums
+        const T o = t >= off ? tsum[t - off] : Op::id();
+        __syncthreads();
+        if (t >= off) tsum[t] = Op::op(o, tsum[t]);
+        __syncthreads();
+    }
+    T run = t ? tsum[t - 1] : Op::id();
+    if (carry) run = Op::op(carry[blockIdx.x], run);
+    for (int j = 0; j < kItems; ++j) {
+        const T in = v[j];
+        if (INCL) run = Op::op(run, in);
+        s[t * kItems + j] = run;
+        if (!INCL) run = Op::op(run, in);
+    }
+    __syncthreads();
+    for (int j = 0; j < kItems; ++j) {
+        const uint64_t i = base + (uint64_t)j * kScanThreads + t;
+        if (i < n) x[i] = s[j * kScanThreads + t];
+    }
+}
+
+// Device scratch for the scans' per-tile sums, taken as a stack.
+struct Scratch {
+    unsigned char *p = nullptr;
+    size_t cap = 0, top = 0;
+};
+
+template <class T, class Op, bool INCL>
+int scan(T *x, uint64_t n, Scratch &scr, cudaStream_t st)
+{
+    if (n == 0) return 0;
+    const uint64_t tiles = (n + scan_tile_n<T>() - 1) / scan_tile_n<T>();
+    if (tiles == 1) {
+        scan_tile<T, Op, INCL><<<1, kScanThreads, 0, st>>>(x, n, nullptr);
+        return cudaGetLastError() == cudaSuccess ? 0 : GALN_ECUDA;
+    }
+    const size_t bytes = (tiles * sizeof(T) + 255) & ~(size_t)255;
+    if (scr.top + bytes > scr.cap) return GALN_ENOMEM;
+    T *part = reinterpret_cast<T *>(scr.p + scr.top);
+    scr.top += bytes;
+    scan_reduce<T, Op><<<(unsigned)tiles, kScanThreads, 0, st>>>(x, n, part);
+    int rc = scan<T, Op, false>(part, tiles, scr, st);
+    if (!rc) scan_tile<T, Op, INCL><<<(unsigned)tiles, kScanThreads, 0, st>>>(x, n, part);
+    scr.top -= bytes;
+    if (rc) return rc;
+    return cudaGetLastError() == cudaSuccess ? 0 : GALN_ECUDA;
+}
+
+// ---- stable LSD radix sort of (uint64 key, uint32 value) pairs ----
+
+// counts[d * tiles + tile] = items of digit d in the tile
+__global__ void __launch_bounds__(kRThreads) radix_hist(const uint64_t *__restrict__ keys, uint64_t n, int shift,
+                                                         uint32_t *__restrict__ counts, uint32_t tiles)
+{
+    __shared__ uint32_t h[256];
+    const int t = threadIdx.x, lane = t & 31;
+    if (t < 256) h[t] = 0;
+    __syncthreads();
+    const uint64_t base = (uint64_t)blockIdx.x * kRTile;
+    for (int j = 0; j < kRItems; ++j) {
+        const uint64_t i = base + (uint64_t)j * kRThreads + t;
+        const bool ok = i < n;
+        const uint32_t d = ok ? (uint32_t)(keys[i] >> shift) & 255u : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        if (ok && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    if (t < 256) counts[(uint64_t)t * tiles + blockIdx.x] = h[t];
+}
+
+struct ScatterSmem {
+    uint32_t wcnt[kRWarps][256];       // per warp: items of each digit, then their offset among the tile's
+    uint32_t tstart[256];              // start of each digit in the tile's sorted order
+    uint32_t gofs[256];                // the tile's first output index for each digit
+    uint32_t wsum[8];
+    uint64_t k[kRTile];
+    uint32_t v[kRTile];
+};
+
+// Items of a tile in input order: warp w holds [w * 32 * kRItems, (w + 1) * 32 * kRItems), its step j the
+// 32 items from j * 32 on, one per lane. A lane's rank among the warp's items of its digit comes from
+// __match_any_sync; warps are ordered by a per-digit prefix over warps; the tile's items are placed in
+// digit order in shared memory and leave it in runs.
+__global__ void __launch_bounds__(kRThreads) radix_scatter(const uint64_t *__restrict__ kin,
+                                                            const uint32_t *__restrict__ vin,
+                                                            uint64_t *__restrict__ kout, uint32_t *__restrict__ vout,
+                                                            uint64_t n, int shift, const uint32_t *__restrict__ offsets,
+                                                            uint32_t tiles)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(smem_raw);
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    for (int i = t; i < kRWarps * 256; i += kRThreads) (&S.wcnt[0][0])[i] = 0;
+    if (t < 256) S.gofs[t] = offsets[(uint64_t)t * tiles + blockIdx.x];
+    __syncthreads();
+
+    const uint64_t base = (uint64_t)blockIdx.x * kRTile;
+    const uint64_t wbase = base + (uint64_t)w * (32 * kRItems);
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint64_t key[kRItems];
+    uint32_t val[kRItems], rk[kRItems];
+#pragma unroll
+    for (int j = 0; j < kRItems; ++j) {
+        const uint64_t i = wbase + (uint64_t)j * 32 + lane;
+        const bool ok = i < n;
+        key[j] = ok ? kin[i] : 0;
+        val[j] = ok ? vin[i] : 0;
+        const uint32_t d = ok ? (uint32_t)(key[j] >> shift) & 255u : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t c = ok ? S.wcnt[w][d] : 0u;
+        rk[j] = c + (uint32_t)__popc(peers & lt_mask);
+        __syncwarp();
+        if (ok && (peers & lt_mask) == 0) S.wcnt[w][d] = c + (uint32_t)__popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    uint32_t tot = 0;
+    if (t < 256) {
+        for (int ww = 0; ww < kRWarps; ++ww) {
+            const uint32_t c = S.wcnt[ww][t];
+            S.wcnt[ww][t] = tot;
+            tot += c;
+        }
+    }
+    // exclusive scan of the 256 digit totals (threads 0..255 = warps 0..7)
+    uint32_t inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (t < 256 && lane == 31) S.wsum[w] = inc;
+    __syncthreads();
+    if (t < 256) {
+        uint32_t before = 0;
+        for (int ww = 0; ww < w; ++ww) before += S.wsum[ww];
+        S.tstart[t] = before + inc - tot;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kRItems; ++j) {
+        const uint64_t i = wbase + (uint64_t)j * 32 + lane;
+        if (i < n) {
+            const uint32_t d = (uint32_t)(key[j] >> shift) & 255u;
+            const uint32_t p = S.tstart[d] + S.wcnt[w][d] + rk[j];
+            S.k[p] = key[j];
+            S.v[p] = val[j];
+        }
+    }
+    __syncthreads();
+    const uint32_t tile_n = (uint32_t)min((uint64_t)kRTile, n - base);
+    for (uint32_t i = t; i < tile_n; i += kRThreads) {
+        const uint64_t kk = S.k[i];
+        const uint32_t d = (uint32_t)(kk >> shift) & 255u;
+        const uint64_t dst = (uint64_t)S.gofs[d] + (i - S.tstart[d]);
+        kout[dst] = kk;
+        vout[dst] = S.v[i];
+    }
+}
+
+struct Sorter {
+    uint64_t *k[2] = {nullptr, nullptr};
+    uint32_t *v[2] = {nullptr, nullptr};
+    uint32_t *counts = nullptr;
+    Scratch *scr = nullptr;
+    int passes = 0;
+    uint64_t scatter_items = 0;
+    std::vector<cudaEvent_t> ev;       // start/stop pairs around each scatter launch
+};
+
+// Sorts the n pairs in (k[cur], v[cur]) on key bits [0, bits); returns the buffer that holds them sorted.
+int radix_sort(Sorter &s, int cur, uint64_t n, int bits, cudaStream_t st, int &out)
+{
+    out = cur;
+    if (n <= 1) return 0;
+    const uint32_t tiles = (uint32_t)((n + kRTile - 1) / kRTile);
+    for (int shift = 0; shift < bits; shift += 8) {
+        radix_hist<<<tiles, kRThreads, 0, st>>>(s.k[cur], n, shift, s.counts, tiles);
+        int rc = scan<uint32_t, OpSum<uint32_t>, false>(s.counts, (uint64_t)tiles * 256, *s.scr, st);
+        if (rc) return rc;
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return GALN_ECUDA;
+        s.ev.push_back(a);
+        s.ev.push_back(b);
+        cudaEventRecord(a, st);
+        radix_scatter<<<tiles, kRThreads, sizeof(ScatterSmem), st>>>(s.k[cur], s.v[cur], s.k[cur ^ 1], s.v[cur ^ 1], n,
+                                                                     shift, s.counts, tiles);
+        cudaEventRecord(b, st);
+        if (cudaGetLastError() != cudaSuccess) return GALN_ECUDA;
+        cur ^= 1;
+        ++s.passes;
+        s.scatter_items += n;
+    }
+    out = cur;
+    return 0;
+}
+
+// ---- prefix doubling ----
+
+__global__ void pd_key0(const uint8_t *__restrict__ T, uint64_t N, uint64_t *__restrict__ key, uint32_t *__restrict__ pos)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    uint64_t k = 0;
+    for (int j = 0; j < kPrefix; ++j) {
+        const uint64_t p = i + j;
+        k = (k << 3) | (p < N ? (uint64_t)T[p] + 1 : 0);
+    }
+    key[i] = k;
+    pos[i] = (uint32_t)i;
+}
+
+// H[k] = the slot of item k if it starts a group of equal keys, else 0 (an inclusive max-scan then gives
+// every item its group's first slot). Slots rise with k; round 0's slot of item k is k.
+__global__ void pd_heads(const uint64_t *__restrict__ K, const uint32_t *__restrict__ slot, uint64_t M,
+                         uint32_t *__restrict__ H)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M) return;
+    const bool head = k == 0 || K[k] != K[k - 1];
+    H[k] = head ? (slot ? slot[k] : (uint32_t)k) : 0u;
+}
+
+// rank[position] = its group's first slot; C[k] = 1 when item k stays unsorted (its group has two or more)
+__global__ void pd_rank(const uint64_t *__restrict__ K, const uint32_t *__restrict__ P, const uint32_t *__restrict__ H,
+                        uint64_t M, uint32_t *__restrict__ rank, uint32_t *__restrict__ C)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M) return;
+    const bool head = k == 0 || K[k] != K[k - 1];
+    const bool last = k + 1 == M || K[k + 1] != K[k];
+    rank[P[k]] = H[k];
+    C[k] = (head && last) ? 0u : 1u;
+}
+
+// C: inclusive count of kept items. Kept item k goes to C[k] - 1 with its position and slot.
+__global__ void pd_compact(const uint32_t *__restrict__ P, const uint32_t *__restrict__ slot,
+                           const uint32_t *__restrict__ C, uint64_t M, uint32_t *__restrict__ P2,
+                           uint32_t *__restrict__ slot2)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M) return;
+    const uint32_t c = C[k], prev = k ? C[k - 1] : 0u;
+    if (c == prev) return;
+    P2[c - 1] = P[k];
+    slot2[c - 1] = slot ? slot[k] : (uint32_t)k;
+}
+
+// key of an unsorted suffix p: (rank of p, rank of p + h plus one; 0 when p + h is the end of the text)
+__global__ void pd_key(const uint32_t *__restrict__ P, const uint32_t *__restrict__ rank, uint64_t M, uint64_t N,
+                       uint64_t h, int lo_bits, uint64_t *__restrict__ K)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M) return;
+    const uint64_t p = P[k], q = p + h;
+    const uint64_t lo = q < N ? (uint64_t)rank[q] + 1 : 0;
+    K[k] = ((uint64_t)rank[p] << lo_bits) | lo;
+}
+
+__global__ void pd_sa(const uint32_t *__restrict__ rank, uint64_t N, uint32_t *__restrict__ sa)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) sa[(uint64_t)rank[i] + 1] = (uint32_t)i;
+    if (i == 0) sa[0] = (uint32_t)N;
+}
+
+// ---- BWT, .bwt body, .sa samples ----
+
+// L[s], s = 0..N-1: the BWT of T$ without the $ of row `primary`; row 0 (the $ suffix) gives T[N-1]
+__global__ void bwt_symbols(const uint8_t *__restrict__ T, const uint32_t *__restrict__ sa, uint64_t N, uint64_t primary,
+                            uint8_t *__restrict__ L)
+{
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= N) return;
+    const uint64_t row = s < primary ? s : s + 1;
+    L[s] = T[(uint64_t)sa[row] - 1];
+}
+
+__global__ void bwt_block_counts(const uint8_t *__restrict__ L, uint64_t N, uint64_t nb, U4 *__restrict__ cnt)
+{
+    const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const uint64_t s = b * 128, e = min(s + 128, N);
+    uint64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+    for (uint64_t i = s; i < e; ++i) {
+        const uint8_t x = L[i];
+        c0 += x == 0; c1 += x == 1; c2 += x == 2; c3 += x == 3;
+    }
+    cnt[b] = U4{{c0, c1, c2, c3}};
+}
+
+// 16 words per 128-symbol block: the four uint64 counts before it, then 8 words of 16 symbols, the first
+// symbol in the top two bits. incl = inclusive per-block counts. Words past the text are not written.
+__global__ void bwt_write(const uint8_t *__restrict__ L, uint64_t N, uint64_t nb, const U4 *__restrict__ incl,
+                          uint32_t *__restrict__ body)
+{
+    const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nb * 16) return;
+    const uint64_t b = idx >> 4;
+    const int j = (int)(idx & 15);
+    if (j < 8) {
+        const uint64_t v = b ? incl[b - 1].c[j >> 1] : 0;
+        body[idx] = (j & 1) ? (uint32_t)(v >> 32) : (uint32_t)v;
+        return;
+    }
+    const uint64_t s0 = b * 128 + (uint64_t)(j - 8) * 16;
+    if (s0 >= N) return;
+    uint32_t word = 0;
+    for (int t = 0; t < 16; ++t)
+        if (s0 + t < N) word |= (uint32_t)L[s0 + t] << (30 - 2 * t);
+    body[idx] = word;
+}
+
+__global__ void sa_samples(const uint32_t *__restrict__ sa, uint64_t ns, uint64_t *__restrict__ out)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < ns) out[k] = sa[(k + 1) * 32];
+}
+
+__global__ void text_from_forward(const uint8_t *__restrict__ F, uint64_t l_pac, uint8_t *__restrict__ T)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * l_pac) return;
+    T[i] = i < l_pac ? F[i] : (uint8_t)(3 - F[2 * l_pac - 1 - i]);
+}
+
+inline unsigned grid(uint64_t n, int b) { return (unsigned)((n + b - 1) / b); }
+inline int bitlen(uint64_t x) { return x ? 64 - __builtin_clzll(x) : 0; }
+
+struct DevMem {
+    std::vector<void *> ptrs;
+    ~DevMem()
+    {
+        for (void *p : ptrs) cudaFree(p);
+    }
+    template <class T>
+    T *get(size_t count)
+    {
+        void *p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(count * sizeof(T), 256)) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        ptrs.push_back(p);
+        return static_cast<T *>(p);
+    }
+};
+
+}  // namespace ixb
+
+// The whole device part: forward sequence (host) -> .bwt words, L2, primary, .sa samples (host).
+int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bwt, uint64_t L2[5], uint64_t &primary,
+                     std::vector<uint64_t> &samples, galn_build_stats *stats)
+{
+    using namespace ixb;
+    const uint64_t N = 2 * l_pac;
+    if (l_pac == 0 || N > 0xFFFFFFFFull - 64) return GALN_EINVAL;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return GALN_ECUDA;
+    const uint64_t tiles = (N + kRTile - 1) / kRTile;
+    const size_t need = (size_t)N * 38 + tiles * 1024 + (64ull << 20);
+    if (need > fr) {
+        fprintf(stderr, "[galn index] a text of %llu symbols needs about %.1f GB of device memory, %.1f GB free\n",
+                (unsigned long long)N, need / 1e9, fr / 1e9);
+        return GALN_ENOMEM;
+    }
+    cudaStream_t st;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return GALN_ECUDA;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ScatterSmem));
+        attr = true;
+    }
+    int rc = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    Sorter srt;
+    Scratch scr;
+    {
+        DevMem m;
+        uint8_t *F_d = m.get<uint8_t>(l_pac);
+        uint8_t *T = m.get<uint8_t>(N + 64);
+        uint32_t *rank = m.get<uint32_t>(N + 1);
+        srt.k[0] = m.get<uint64_t>(N);
+        srt.k[1] = m.get<uint64_t>(N);
+        srt.v[0] = m.get<uint32_t>(N);
+        srt.v[1] = m.get<uint32_t>(N);
+        uint32_t *slots[2] = {m.get<uint32_t>(N), m.get<uint32_t>(N)};
+        srt.counts = m.get<uint32_t>(tiles * 256);
+        scr.cap = (size_t)(N / 1000 + 4096) * 32;
+        scr.p = m.get<unsigned char>(scr.cap);
+        srt.scr = &scr;
+        if (!F_d || !T || !rank || !srt.k[0] || !srt.k[1] || !srt.v[0] || !srt.v[1] || !slots[0] || !slots[1] ||
+            !srt.counts || !scr.p) {
+            rc = GALN_ENOMEM;
+        }
+        if (!rc) {
+            cudaEventRecord(e0, st);
+            cudaMemcpyAsync(F_d, F, l_pac, cudaMemcpyHostToDevice, st);
+            text_from_forward<<<grid(N, 256), 256, 0, st>>>(F_d, l_pac, T);
+            cudaMemsetAsync(T + N, 0, 64, st);
+            pd_key0<<<grid(N, 256), 256, 0, st>>>(T, N, srt.k[0], srt.v[0]);
+        }
+        // round 0 over all N suffixes; later rounds over the unsorted ones (positions P, slots S)
+        int kb = 0, sbuf = 0;
+        uint64_t M = N, h = kPrefix;
+        const uint32_t *S = nullptr;
+        int bits = 3 * kPrefix;
+        int rounds = 0;
+        uint64_t sorted = 0;
+        while (!rc) {
+            rc = radix_sort(srt, kb, M, bits, st, kb);
+            if (rc) break;
+            sorted += M;
+            const uint64_t *K = srt.k[kb];
+            const uint32_t *P = srt.v[kb];
+            // the other key buffer is free: two uint32 arrays of M
+            uint32_t *H = reinterpret_cast<uint32_t *>(srt.k[kb ^ 1]);
+            uint32_t *C = H + M;
+            pd_heads<<<grid(M, 256), 256, 0, st>>>(K, S, M, H);
+            rc = scan<uint32_t, OpMax<uint32_t>, true>(H, M, scr, st);
+            if (rc) break;
+            pd_rank<<<grid(M, 256), 256, 0, st>>>(K, P, H, M, rank, C);
+            rc = scan<uint32_t, OpSum<uint32_t>, true>(C, M, scr, st);
+            if (rc) break;
+            uint32_t kept = 0;
+            if (cudaMemcpyAsync(&kept, C + M - 1, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess) {
+                rc = GALN_ECUDA;
+                break;
+            }
+            if (kept == 0) break;
+            if (++rounds > kMaxRounds) { rc = GALN_EINVAL; break; }
+            uint32_t *P2 = srt.v[kb ^ 1], *S2 = slots[sbuf];
+            pd_compact<<<grid(M, 256), 256, 0, st>>>(P, S, C, M, P2, S2);
+            S = S2;
+            sbuf ^= 1;
+            M = kept;
+            const int lo_bits = bitlen(N);
+            bits = lo_bits + bitlen(N - 1);
+            pd_key<<<grid(M, 256), 256, 0, st>>>(P2, rank, M, N, h, lo_bits, srt.k[kb ^ 1]);
+            kb ^= 1;
+            h *= 2;
+        }
+        if (!rc) {
+            uint32_t r0 = 0;
+            uint32_t *sa = reinterpret_cast<uint32_t *>(srt.k[0]);
+            pd_sa<<<grid(N, 256), 256, 0, st>>>(rank, N, sa);
+            if (cudaMemcpyAsync(&r0, rank, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                rc = GALN_ECUDA;
+            primary = (uint64_t)r0 + 1;
+            const uint64_t nb = (N + 127) / 128, nw = (N + 15) / 16;
+            uint8_t *L = reinterpret_cast<uint8_t *>(srt.k[1]);
+            U4 *cnt = reinterpret_cast<U4 *>(srt.v[0]);      // nb * 32 bytes <= 4N
+            uint32_t *body = srt.v[1];                       // nb * 64 bytes <= 4N + 64
+            uint64_t *smp = reinterpret_cast<uint64_t *>(slots[0]);
+            const uint64_t ns = (N + 32) / 32 - 1;
+            if (!rc) {
+                bwt_symbols<<<grid(N, 256), 256, 0, st>>>(T, sa, N, primary, L);
+                bwt_block_counts<<<grid(nb, 128), 128, 0, st>>>(L, N, nb, cnt);
+                rc = scan<U4, OpSum<U4>, true>(cnt, nb, scr, st);
+            }
+            if (!rc) {
+                bwt_write<<<grid(nb * 16, 256), 256, 0, st>>>(L, N, nb, cnt, body);
+                if (ns) sa_samples<<<grid(ns, 256), 256, 0, st>>>(sa, ns, smp);
+                const uint64_t last_words = nw - 8 * (nb - 1);
+                const uint64_t body_words = 16 * nb - (8 - last_words);
+                bwt.resize(body_words + 8);
+                samples.resize(ns);
+                U4 totals{};
+                cudaMemcpyAsync(bwt.data(), body, body_words * 4, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(&totals, cnt + nb - 1, sizeof(U4), cudaMemcpyDeviceToHost, st);
+                if (ns) cudaMemcpyAsync(samples.data(), smp, ns * 8, cudaMemcpyDeviceToHost, st);
+                cudaEventRecord(e1, st);
+                if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = GALN_ECUDA;
+                if (!rc) {
+                    memcpy(bwt.data() + body_words, totals.c, sizeof(totals.c));
+                    L2[0] = 0;
+                    for (int c = 0; c < 4; ++c) L2[c + 1] = L2[c] + totals.c[c];
+                }
+            }
+        }
+        if (stats && !rc) {
+            stats->n = N;
+            stats->primary = primary;
+            stats->rounds = rounds;
+            stats->sorted_items = sorted;
+            stats->sort_passes = srt.passes;
+            stats->scatter_items = srt.scatter_items;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            stats->ms_device = ms;
+            double sc = 0;
+            for (size_t i = 0; i + 1 < srt.ev.size(); i += 2) {
+                float x = 0;
+                cudaEventElapsedTime(&x, srt.ev[i], srt.ev[i + 1]);
+                sc += x;
+            }
+            stats->ms_scatter = sc;
+        }
+        if (rc) cudaStreamSynchronize(st);
+    }
+    for (cudaEvent_t e : srt.ev) cudaEventDestroy(e);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    if (rc == GALN_ECUDA) cudaGetLastError();
+    return rc;
+}
+
+}  // namespace galn

@@ -5,6 +5,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
+#include "galn_aln.h"
+
 namespace galn {
 
 constexpr int kBatchReads = 0x40000;   // bwa_read_seq batch (src/host_io.h:16)
@@ -89,7 +93,7 @@ int dev_search(const DevIndex &ix, DevJob &job, const TierCfg &cfg, const int32_
 // Occupancy: resident threads per SM for a tier's kernel at the given block size
 int dev_resident_threads(const TierCfg &cfg, bool wide, int device);
 
-// The warp tier: one warp per read over list[0..n). Warps 0..n_big-1 have arenas of big_chunks 32-entry
+// The warp tier: one warp per read over list[0..n). Warps 0..n_big-1 have arenas of big_chunks kWarpChunk-entry
 // chunks, the others arena_chunks; a read that outgrows a small arena is handed to a big warp in the same
 // launch through a queue in ws_mem. Every warp holds aln_cap records. Reads the launch cannot finish go to
 // ovf[]; reads still queued when it ends are read back through warp_queue(). ws_mem holds
@@ -115,5 +119,10 @@ int dev_order_results(const DevJob &job, int n, int64_t *rec_off, uint64_t *rec_
 size_t order_tile_bytes(int n);
 // the queue in ws_mem: control words (0 head, 1 tail, 2 small warps finished, 3 a slot was lost) and slots
 int32_t *warp_queue(const WarpCfg &c, int n, void *ws_mem, int32_t **slots);
+// The device part of `galn index` (galn_build_index.cu): the forward sequence F[0..l_pac) (host, codes
+// 0..3) -> the .bwt words after its header (the Occ-interleaved body and the four totals), L2, primary and
+// the .sa samples SA[32], SA[64], ...
+int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bwt, uint64_t L2[5], uint64_t &primary,
+                     std::vector<uint64_t> &samples, galn_build_stats *stats);
 
 }  // namespace galn

@@ -1,7 +1,12 @@
-// galn_main.cpp -- the `galn aln` command line on top of the C ABI (the reference's galn_aln,
-// src/galn.cu:436-1288, and its usage text, src/galn.cu:144-180).
+// galn_main.cpp -- the `galn aln` and `galn index` command lines on top of the C ABI (the reference's
+// galn_aln, src/galn.cu:436-1288, its usage text, src/galn.cu:144-180, and galn index,
+// src/index/galn_index.c:36-71).
 //
 //   galn aln [options] <prefix> <reads.fq[.gz]> [> out.sai]
+//   galn index [-a auto|gpu|gpu-lowmem] [-p prefix] [-t threads] [-v] [--device N] <in.fasta[.gz]>
+//
+// galn index writes the five files of bwa index 0.7.19; every builder choice runs the GPU builder (-a cpu
+// is refused: there is no CPU path), -t is accepted and ignored, bwa's -a is/bwtsw/rb2 mean auto.
 //
 // Every bwa aln option keeps its meaning and default; -dt only sets the thread count written into the .sai
 // header. Per-read trace hashes (the reference's --verify data) are computed only with --verify. Flags of the reference that pick CPU/GPU work sharing (--cpu-workers, --gpu-only, --cpu-interleave,
@@ -34,7 +39,8 @@ static int usage()
 {
     fprintf(stderr,
             "\nProgram: galn-b200 (bwa aln search on NVIDIA B200, sm_100a)\n\n"
-            "Usage:   galn aln [options] <prefix> <in.fq[.gz]>\n\n"
+            "Usage:   galn aln [options] <prefix> <in.fq[.gz]>\n"
+            "         galn index [-a auto|gpu|gpu-lowmem] [-p prefix] [-v] [--device N] <in.fasta[.gz]>\n\n"
             "bwa aln options (same meaning and defaults as BWA 0.7.19):\n"
             "         -n NUM    max #diff (int) or missing prob under 0.02 err rate (float) [0.04]\n"
             "         -o INT    maximum number of gap opens [1]\n"
@@ -363,12 +369,68 @@ static int run_pipelined(const galn_opts &opt, const char *const pos[2], const c
     return werr;
 }
 
+static int index_usage()
+{
+    fprintf(stderr,
+            "\nUsage:   galn index [-a STR] [-p prefix] [-v] [--device N] <in.fasta[.gz]>\n\n"
+            "Options: -a STR   auto, gpu or gpu-lowmem (one GPU builder; bwa's is, bwtsw and rb2 mean auto) [auto]\n"
+            "         -p STR   prefix of the index files [the FASTA file name]\n"
+            "         -t INT   accepted and ignored\n"
+            "         -v       the time of each step on stderr\n"
+            "         --device INT  CUDA device [0]\n\n");
+    return 1;
+}
+
+// galn index (src/index/galn_index.c:36-71): exit 1 usage, 2 the FASTA or the index files, 10 CUDA
+static int index_main(int argc, char **argv)
+{
+    const char *prefix = nullptr, *fa = nullptr;
+    int verbose = 0, device = 0;
+    for (int i = 0; i < argc; ++i) {
+        const char *a = argv[i], *v = i + 1 < argc ? argv[i + 1] : nullptr;
+        if (!strcmp(a, "-p") && v) { prefix = v; ++i; }
+        else if (!strcmp(a, "-t") && v) ++i;
+        else if (!strcmp(a, "--device") && v) { device = atoi(v); ++i; }
+        else if (!strcmp(a, "-v")) verbose = 1;
+        else if (!strcmp(a, "--cpu")) { fprintf(stderr, "[galn index] there is no CPU builder in this build\n"); return 1; }
+        else if (!strcmp(a, "-a") && v) {
+            ++i;
+            if (!strcmp(v, "cpu")) { fprintf(stderr, "[galn index] there is no CPU builder in this build\n"); return 1; }
+            if (strcmp(v, "auto") && strcmp(v, "gpu") && strcmp(v, "gpu-lowmem") && strcmp(v, "is") &&
+                strcmp(v, "bwtsw") && strcmp(v, "rb2")) {
+                fprintf(stderr, "[galn index] unknown builder -a %s\n", v);
+                return index_usage();
+            }
+        }
+        else if (a[0] == '-') { fprintf(stderr, "[galn index] unknown option %s\n", a); return index_usage(); }
+        else if (!fa) fa = a;
+        else return index_usage();
+    }
+    if (!fa) return index_usage();
+    if (!prefix) prefix = fa;
+    if (cudaSetDevice(device) != cudaSuccess) { fprintf(stderr, "[galn index] no CUDA device %d\n", device); return 10; }
+    galn_build_stats st{};
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = galn_index_build_fasta(fa, prefix, &st);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (rc) {
+        fprintf(stderr, "[galn index] failed (%d) for %s\n", rc, fa);
+        return rc == GALN_ECUDA ? 10 : 2;
+    }
+    if (verbose)
+        fprintf(stderr, "[galn index] %llu symbols, %d doubling rounds, %d radix passes: device %.1f ms "
+                "(scatter %.1f ms), files %.1f ms, %.2f s in all\n", (unsigned long long)st.n, st.rounds,
+                st.sort_passes, st.ms_device, st.ms_scatter, st.ms_files, secs);
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
     if (argc < 2) return usage();
     if (!strcmp(argv[1], "--version") || !strcmp(argv[1], "version")) { printf("%s\n", galn_version()); return 0; }
+    if (!strcmp(argv[1], "index")) return index_main(argc - 2, argv + 2);
     if (strcmp(argv[1], "aln")) {
-        fprintf(stderr, "[galn] unknown command '%s' (this build provides aln)\n", argv[1]);
+        fprintf(stderr, "[galn] unknown command '%s' (this build provides aln and index)\n", argv[1]);
         return usage();
     }
     std::vector<const char *> bwa_args;

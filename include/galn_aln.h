@@ -155,6 +155,38 @@ int galn_index_load_sa(galn_index *ix, const char *prefix);
 int galn_bwt_sa(galn_index *ix, const uint64_t *rows, int64_t n, uint64_t *sa);
 int galn_sa2pos(galn_index *ix, const uint64_t *rows, const int32_t *ref_len, int64_t n, uint64_t *pos, int8_t *strand);
 
+/* ---- index building (`galn index`) -----------------------------------------------------------------------
+ * The files of `bwa index` 0.7.19, byte for byte: <prefix>.pac/.ann/.amb from the FASTA records (the
+ * reference's src/index/fasta_pac.c, bwa's bns_fasta2bntseq) and <prefix>.bwt/.sa from the text
+ * F . revcomp(F), F the forward sequence with ambiguous bases replaced (the reference's GPU builder,
+ * src/index/gpu_index.cu:1-20). The suffix sort, BWT, Occ packing and SA sampling run on the GPU; texts
+ * up to 2^32 - 64 symbols (references up to about 2.1 Gbp), about 38 bytes of device memory per symbol. */
+typedef struct {
+    uint64_t n;                 /* text length, 2 x reference length */
+    uint64_t primary;           /* the BWT row of the whole text */
+    int rounds;                 /* prefix-doubling rounds after the first sort */
+    int sort_passes;            /* 8-bit radix passes, all rounds */
+    uint64_t sorted_items;      /* (key, position) pairs sorted, all rounds */
+    uint64_t scatter_items;     /* items moved by the radix scatter launches (sorted_items x passes) */
+    double ms_device;           /* device time from the text's upload to the last result copy */
+    double ms_scatter;          /* device time of the radix scatter launches */
+    double ms_files;            /* host time: FASTA to .pac/.ann/.amb, and writing .bwt/.sa */
+} galn_build_stats;
+
+/* The host step: <prefix>.pac/.ann/.amb from a FASTA file (plain or gzip), as the reference's
+ * galn_fasta_to_pac (src/index/fasta_pac.c:330) writes them; *l_pac = the reference length. FASTQ input is
+ * refused (GALN_EINVAL), as is an input without bases. */
+int galn_fasta_to_pac(const char *fasta, const char *prefix, uint64_t *l_pac);
+
+/* .bwt and .sa for the forward sequence fwd[0..l_pac) (codes 0..3) on the current device.
+ * Returns 0, GALN_EINVAL (empty or too long), GALN_ENOMEM (device memory), GALN_EIO or GALN_ECUDA.
+ * stats may be NULL. */
+int galn_index_build_text(const uint8_t *fwd, uint64_t l_pac, const char *prefix, galn_build_stats *stats);
+
+/* All five files for a FASTA file (plain or gzip) on the current device, as `galn index -a gpu
+ * -p <prefix> <fasta>` writes them (src/index/galn_index.c:36-71). */
+int galn_index_build_fasta(const char *fasta, const char *prefix, galn_build_stats *stats);
+
 /* ---- .sai ----------------------------------------------------------------------------------------------- */
 /* "SAI\1", the option block, then per read int32 n_aln and the records (src/sai_writer.h:9-21). A read
  * with an error code is written with 0 records and the call returns 4 (src/galn.cu:1250-1263); 5 on a

@@ -138,6 +138,8 @@ def lib():
         L.orc_bwt_sa.argtypes = [vp, vp, C.c_uint64, C.c_uint64]
         L.orc_sa2pos.restype = C.c_uint64
         L.orc_sa2pos.argtypes = [vp, vp, C.c_uint64, C.c_uint64, C.c_int, ip]
+        L.orc_suffix_array.argtypes = [vp, C.c_uint64, vp]
+        L.orc_index_files.argtypes = [vp, C.c_uint64, C.c_char_p]
         _lib = L
     return _lib
 
@@ -355,3 +357,32 @@ def read_sai(path: str) -> dict:
             pos += 24 * k
     return dict(opt=opt, n_aln=np.array(ns, np.int32),
                 records=np.concatenate(recs) if recs else np.zeros(0, REC_DTYPE))
+
+
+# ------------------------------------------------------------------------------------------------
+# index files (bwa index 0.7.19 .bwt / .sa; src/index/idxcommon.c:72-153)
+
+def suffix_array(T: np.ndarray) -> np.ndarray:
+    """SA of T$ (codes 0..3) over its n+1 rows; row 0 is the $ suffix (position n). Comparison sort."""
+    t = np.ascontiguousarray(T, dtype=np.uint8)
+    sa = np.zeros(len(t) + 1, dtype=np.uint64)
+    lib().orc_suffix_array(_ptr(t), len(t), _ptr(sa))
+    return sa
+
+
+def index_files(F: np.ndarray, prefix: str) -> None:
+    """<prefix>.bwt and <prefix>.sa for the forward sequence F (codes 0..3), as bwa index writes them."""
+    f = np.ascontiguousarray(F, dtype=np.uint8)
+    if lib().orc_index_files(_ptr(f), len(f), prefix.encode()):
+        raise RuntimeError("orc_index_files failed")
+
+
+def forward_from_pac(pac_path: str) -> np.ndarray:
+    """The forward sequence (codes 0..3) held in a .pac file: 4 bases a byte, the first in the top bits; the
+    last byte holds l_pac % 4 (after a 0 byte when that is 0)."""
+    b = np.fromfile(pac_path, dtype=np.uint8)
+    rem = int(b[-1])
+    nbytes = len(b) - (2 if rem == 0 else 1)
+    codes = np.stack([(b[:nbytes] >> s) & 3 for s in (6, 4, 2, 0)], axis=1).reshape(-1)
+    l_pac = nbytes * 4 if rem == 0 else (nbytes - 1) * 4 + rem
+    return codes[:l_pac].astype(np.uint8)

@@ -787,3 +787,90 @@ void orc_reads_free(void *p)
     if (!o) return;
     free(o->query); free(o->off); free(o->len); free(o->batch); free(o);
 }
+
+/* ---- index files (`bwa index` 0.7.19 .bwt and .sa; the reference's src/index/idxcommon.c:72-153) ----
+ * Test sizes only: the suffix array of T$ by a comparison sort over the suffixes (memcmp on one code per
+ * byte; a suffix that is a prefix of another sorts first, $ being the smallest symbol). */
+static const uint8_t *orc_sa_text;
+static uint64_t orc_sa_n;
+
+static int orc_suffix_cmp(const void *a, const void *b)
+{
+    const uint64_t i = *(const uint64_t*)a, j = *(const uint64_t*)b;
+    const uint64_t li = orc_sa_n - i, lj = orc_sa_n - j, l = li < lj ? li : lj;
+    const int c = memcmp(orc_sa_text + i, orc_sa_text + j, l);
+    if (c) return c;
+    return li < lj ? -1 : li > lj ? 1 : 0;
+}
+
+/* sa[0..n]: row 0 is the $ suffix (position n) */
+int orc_suffix_array(const uint8_t *T, uint64_t n, uint64_t *sa)
+{
+    orc_sa_text = T;
+    orc_sa_n = n;
+    sa[0] = n;
+    for (uint64_t i = 0; i < n; ++i) sa[i + 1] = i;
+    qsort(sa + 1, n, sizeof(uint64_t), orc_suffix_cmp);
+    return 0;
+}
+
+/* <prefix>.bwt and <prefix>.sa for the forward sequence F[0..l_pac) (codes 0..3): the text is
+ * T = F . revcomp(F); its BWT drops the $ of the row of suffix 0 (`primary`); the .bwt body holds, every 128
+ * symbols, the four 64-bit counts of the symbols before, and 16 symbols per 32-bit word, the first in the
+ * top two bits, then the four totals (idxcommon.c:72-112); the .sa holds every 32nd row from row 32 on
+ * (idxcommon.c:137-153). Both files start with primary and L2[1..4]; the .sa adds 32 and n. */
+int orc_index_files(const uint8_t *F, uint64_t l_pac, const char *prefix)
+{
+    const uint64_t n = 2 * l_pac;
+    uint8_t *T = (uint8_t*)malloc(n ? n : 1);
+    uint64_t *sa = (uint64_t*)malloc((n + 1) * sizeof(uint64_t));
+    uint8_t *L = (uint8_t*)malloc(n ? n : 1);
+    if (!T || !sa || !L) { free(T); free(sa); free(L); return -1; }
+    for (uint64_t i = 0; i < l_pac; ++i) { T[i] = F[i]; T[n - 1 - i] = (uint8_t)(3 - F[i]); }
+    orc_suffix_array(T, n, sa);
+    uint64_t primary = 0, m = 0, L2[5] = {0, 0, 0, 0, 0}, cnt[4] = {0, 0, 0, 0};
+    for (uint64_t r = 0; r <= n; ++r) {
+        if (sa[r] == 0) { primary = r; continue; }
+        L[m++] = T[sa[r] - 1];
+    }
+    for (uint64_t i = 0; i < n; ++i) ++cnt[T[i]];
+    for (int c = 0; c < 4; ++c) L2[c + 1] = L2[c] + cnt[c];
+    const uint64_t nw = (n + 15) / 16, nb = (n + 127) / 128;
+    uint32_t *body = (uint32_t*)calloc(nw + 8 * (nb + 1), sizeof(uint32_t));
+    uint64_t run[4] = {0, 0, 0, 0}, k = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if ((i & 127) == 0) { memcpy(body + k, run, sizeof run); k += 8; }
+        if ((i & 15) == 0) {
+            uint32_t w = 0;
+            for (uint64_t t = 0; t < 16 && i + t < n; ++t) w |= (uint32_t)L[i + t] << (30 - 2 * t);
+            body[k++] = w;
+        }
+        ++run[L[i]];
+    }
+    memcpy(body + k, run, sizeof run);
+    k += 8;
+    char path[4096];
+    int rc = 0;
+    snprintf(path, sizeof path, "%s.bwt", prefix);
+    FILE *f = fopen(path, "wb");
+    if (!f) rc = -1;
+    else {
+        fwrite(&primary, 8, 1, f);
+        fwrite(L2 + 1, 8, 4, f);
+        fwrite(body, 4, k, f);
+        fclose(f);
+    }
+    snprintf(path, sizeof path, "%s.sa", prefix);
+    f = rc ? NULL : fopen(path, "wb");
+    if (!f) rc = -1;
+    else {
+        const uint64_t head[3] = {primary, 32, n};
+        fwrite(head, 8, 1, f);
+        fwrite(L2 + 1, 8, 4, f);
+        fwrite(head + 1, 8, 2, f);
+        for (uint64_t r = 32; r <= n; r += 32) fwrite(sa + r, 8, 1, f);
+        fclose(f);
+    }
+    free(T); free(sa); free(L); free(body);
+    return rc;
+}

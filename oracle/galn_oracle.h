@@ -59,6 +59,10 @@ int   orc_result_fetch80(const void *res, uint64_t *fetch80);
 uint64_t orc_bwt_sa(const void *index, const uint64_t *samples, uint64_t intv, uint64_t k);
 uint64_t orc_sa2pos(const void *index, const uint64_t *samples, uint64_t intv, uint64_t k, int ref_len, int *strand);
 int   orc_result_write_sai(const void *res, const orc_gap_opt_t *opt, const char *path);
+/* index files: the suffix array of T$ (sa[0..n], row 0 = position n) by a comparison sort, and <prefix>.bwt
+ * / <prefix>.sa for the forward sequence F (codes 0..3) as bwa index writes them (test sizes only) */
+int   orc_suffix_array(const uint8_t *T, uint64_t n, uint64_t *sa);
+int   orc_index_files(const uint8_t *F, uint64_t l_pac, const char *prefix);
 void  orc_result_free(void *res);
 
 #ifdef __cplusplus

@@ -1,0 +1,89 @@
+"""`galn index` on the CPU side: the oracle's restatement of the .bwt/.sa files against the reference
+builder's own files (tests/golden/index, tests/golden/small, tests/golden/genome: the pin), the oracle's
+suffix sort against a plain sort, and the library's host step (FASTA -> .pac/.ann/.amb) against the
+reference's files for every golden FASTA (CRLF, lowercase, IUPAC codes, empty and '@' records, gzip)."""
+import filecmp
+import gzip
+import os
+
+import numpy as np
+import pytest
+
+import galn_b200
+import oracle
+from conftest import GOLDEN
+
+INDEX_CASES = sorted(os.listdir(os.path.join(GOLDEN, "index")))
+ALL = [("index", c) for c in INDEX_CASES] + [("", "small"), ("", "genome")]
+
+
+def _dir(group, name):
+    return os.path.join(GOLDEN, group, name) if group else os.path.join(GOLDEN, name)
+
+
+def _fasta(d):
+    return os.path.join(d, "ref.fa.gz") if os.path.exists(os.path.join(d, "ref.fa.gz")) else os.path.join(d, "ref.fa")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    oracle.build()
+
+
+def _same(a, b):
+    return filecmp.cmp(a, b, shallow=False)
+
+
+@pytest.mark.parametrize("group,name", ALL)
+def test_oracle_index_files_are_the_references(group, name, tmp_path):
+    d = _dir(group, name)
+    F = oracle.forward_from_pac(os.path.join(d, "ref.pac"))
+    pre = str(tmp_path / "o")
+    oracle.index_files(F, pre)
+    for ext in ("bwt", "sa"):
+        assert _same(pre + "." + ext, os.path.join(d, "ref." + ext)), ext
+
+
+def test_oracle_suffix_array_is_a_plain_sort():
+    rng = np.random.default_rng(5)
+    for n in (1, 2, 3, 7, 64, 300):
+        for kind in range(3):
+            T = (rng.integers(0, 4, n) if kind == 0 else np.zeros(n, np.int64) if kind == 1
+                 else np.tile([0, 1], n)[:n]).astype(np.uint8)
+            want = [n] + sorted(range(n), key=lambda i: T[i:].tobytes())
+            np.testing.assert_array_equal(oracle.suffix_array(T), np.array(want, dtype=np.uint64))
+
+
+@pytest.mark.parametrize("group,name", ALL)
+def test_host_step_files_are_the_references(group, name, tmp_path):
+    d = _dir(group, name)
+    pre = str(tmp_path / "h")
+    l_pac = galn_b200.fasta_to_pac(_fasta(d), pre)
+    assert l_pac == len(oracle.forward_from_pac(os.path.join(d, "ref.pac")))
+    for ext in ("pac", "ann", "amb"):
+        assert _same(pre + "." + ext, os.path.join(d, "ref." + ext)), ext
+
+
+def test_host_step_refuses_fastq_and_empty_input(tmp_path):
+    fq = tmp_path / "r.fq"
+    fq.write_text("@r1\nACGT\n+\nIIII\n")
+    with pytest.raises(galn_b200.GalnError):
+        galn_b200.fasta_to_pac(str(fq), str(tmp_path / "a"))
+    empty = tmp_path / "e.fa"
+    empty.write_text(">e\n\n")
+    with pytest.raises(galn_b200.GalnError):
+        galn_b200.fasta_to_pac(str(empty), str(tmp_path / "b"))
+    with pytest.raises(galn_b200.GalnError):
+        galn_b200.fasta_to_pac(str(tmp_path / "missing.fa"), str(tmp_path / "c"))
+
+
+def test_forward_from_pac_round_trip(tmp_path):
+    rng = np.random.default_rng(9)
+    for n in (1, 3, 4, 5, 8, 1001):
+        seq = "".join("ACGT"[i] for i in rng.integers(0, 4, n))
+        fa = tmp_path / f"s{n}.fa.gz"
+        with gzip.open(fa, "wt") as f:
+            f.write(f">s\n{seq}\n")
+        galn_b200.fasta_to_pac(str(fa), str(tmp_path / f"s{n}"))
+        F = oracle.forward_from_pac(str(tmp_path / f"s{n}.pac"))
+        assert "".join("ACGT"[c] for c in F) == seq
