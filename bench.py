@@ -18,6 +18,8 @@ table. The L2 cache is flushed (a 512 MB write) before each step, outside the ti
   cpu_baseline  the reference's own `galn aln --cpu-only` on a sample of the same reads, all host cores
 
 --impl reference times only the reference's CPU path (rank 0; other ranks exit at once).
+
+--index-build times `galn index` instead (the GPU index builder on the workload's reference; see index_bench).
 """
 from __future__ import annotations
 
@@ -62,9 +64,12 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def prepare(workload: str, scale: float, rank: int, device: int, data_dir: str | None, reads_scale=None):
-    """Reference + BWA index (built on this GPU) + this rank's reads, cached on disk."""
-    from galn_b200 import index_build, synth
+def prepare(workload: str, scale: float, rank: int, device: int, data_dir: str | None, reads_scale=None,
+            reference_builder: bool = False):
+    """Reference + BWA index + this rank's reads, cached on disk. The index is built on this GPU by `galn
+    index`, or by the reference's own CPU builder for the reference arm when that is built (the files are
+    the same bytes)."""
+    from galn_b200 import synth
     d = data_dir or os.path.join(tempfile.gettempdir(), f"galn_bench_{workload}_{scale}_r{rank}")
     os.makedirs(d, exist_ok=True)
     t = time.time()
@@ -73,7 +78,16 @@ def prepare(workload: str, scale: float, rank: int, device: int, data_dir: str |
         _, reads, _ = synth.workload(workload, scale, seed=1 + 7919 * rank, reads_scale=reads_scale)
     prefix = os.path.join(d, "ref")
     if not os.path.exists(prefix + ".bwt"):
-        index_build.build_from_reference(ref, prefix, device=f"cuda:{device}")
+        synth.write_fasta(prefix + ".fa", ref)
+        ref_builder = None
+        if reference_builder:
+            import oracle
+            ref_builder = oracle.INDEX_REF if os.path.exists(oracle.INDEX_REF) else None
+        if ref_builder:
+            subprocess.run([ref_builder, "-f", prefix + ".fa", prefix], check=True, capture_output=True)
+        else:
+            import galn_b200
+            galn_b200.index_fasta(prefix + ".fa", prefix, device)
     log(f"[bench] rank {rank}: data ready in {time.time() - t:.1f} s ({len(reads)} reads, ref {ref.total} bp)")
     return d, prefix, ref, reads, opts
 
@@ -157,6 +171,97 @@ def cpu_reference(prefix, reads, opts, sample, d, steps=1, warmup=0):
                        f" search time from its own timing line"), None
 
 
+def index_bench(args, rank: int, local: int) -> int:
+    """--index-build: `galn index` on the workload's reference (FASTA on disk to the five bwa index files).
+    value = reference bp / device span of the builder (text upload to the last result copy); e2e = reference
+    bp / wall time of galn_index_build_fasta (FASTA parse, device build, file writes); the roofline is the
+    radix scatter (24 B of keys and values read and written per item and pass); cpu_baseline = the reference's
+    own CPU builder (`galn index -a cpu`, oracle/_ref/galn_index_cpu) on the same FASTA, all host threads.
+    With --impl reference only the reference's builder runs. The files are compared with the reference
+    builder's when it ran."""
+    import filecmp
+    import oracle
+    from galn_b200 import synth
+    if rank != 0:
+        return 0
+    d = args.data_dir or os.path.join(tempfile.gettempdir(), f"galn_index_{args.workload}_{args.scale}")
+    os.makedirs(d, exist_ok=True)
+    ref, _, _ = synth.workload(args.workload, args.scale, seed=1, reads_scale=0.001)
+    fa = os.path.join(d, "ref.fa")
+    if not os.path.exists(fa):
+        synth.write_fasta(fa, ref)
+    cores = os.cpu_count() or 1
+    config = {"workload": f"bwa index of the {args.workload} reference ({ref.total} bp, {len(ref.names)} contigs)",
+              "scale": args.scale}
+
+    def run_reference():
+        if not os.path.exists(oracle.INDEX_REF):
+            return None
+        t = time.time()
+        p = subprocess.run([oracle.INDEX_REF, "-f", fa, os.path.join(d, "refix")], capture_output=True, text=True)
+        return time.time() - t if p.returncode == 0 else None
+
+    if args.impl == "reference":
+        walls = []
+        for i in range(args.warmup + args.steps):
+            w = run_reference()
+            if w is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference index builder not built"}))
+                return 0
+            if i >= args.warmup:
+                walls.append(w)
+        v = ref.total / statistics.mean(walls)
+        cb = dict(value=v, unit="bp/s", cores=cores, kind="reference",
+                  sample=f"the whole {ref.total} bp reference, `galn index -a cpu` with {cores} threads")
+        print(json.dumps({"impl": "reference", "metric": "bwa index: reference bp/s", "value": v, "unit": "bp/s",
+                          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * statistics.mean(walls), "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)", "config": config,
+                          "cpu_baseline": cb, "e2e": {"value": v, "unit": "bp/s", "h2d_bytes_per_step": 0,
+                                                      "d2h_bytes_per_step": 0}}))
+        return 0
+
+    import galn_b200
+    from galn_b200 import build as gbuild
+    gbuild.build()
+    hbm, hbm_kind = peaks()
+    sts, walls = [], []
+    for i in range(args.warmup + args.steps):
+        t = time.time()
+        st = galn_b200.index_fasta(fa, os.path.join(d, "gpu"), local)
+        if i >= args.warmup:
+            walls.append(time.time() - t)
+            sts.append(st)
+    ms_dev = statistics.mean(x["ms_device"] for x in sts)
+    ms_sc = statistics.mean(x["ms_scatter"] for x in sts)
+    sc_bytes = 24.0 * sts[0]["scatter_items"]
+    wref = run_reference()
+    same = None
+    if wref is not None:
+        same = all(filecmp.cmp(os.path.join(d, "gpu." + e), os.path.join(d, "refix." + e), shallow=False)
+                   for e in ("pac", "ann", "amb", "bwt", "sa"))
+    n = sts[0]["n"]
+    d2h = os.path.getsize(os.path.join(d, "gpu.bwt")) + os.path.getsize(os.path.join(d, "gpu.sa")) - 40 - 56
+    line = {"metric": "bwa index: reference bp/s (five files byte-identical to the reference builder's)",
+            "value": ref.total / (ms_dev / 1e3), "unit": "bp/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_dev, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)", "config": config,
+            "e2e": {"value": ref.total / statistics.mean(walls), "unit": "bp/s", "h2d_bytes_per_step": ref.total,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": "radix_scatter (all passes of all doubling rounds)",
+                         "achieved": sc_bytes / (ms_sc / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": sc_bytes / (ms_sc / 1e3) / 1e9 / hbm, "peak_kind": hbm_kind, "traffic": None},
+            "builder": {"text_symbols": n, "rounds": sts[0]["rounds"], "radix_passes": sts[0]["sort_passes"],
+                        "sorted_items": sts[0]["sorted_items"], "ms_scatter": ms_sc,
+                        "ms_host_files": statistics.mean(x["ms_files"] for x in sts)},
+            "identical_to_reference_builder": same}
+    if wref is not None:
+        line["cpu_baseline"] = dict(value=ref.total / wref, unit="bp/s", cores=cores, kind="reference",
+                                    sample=f"the whole {ref.total} bp reference, `galn index -a cpu` with {cores} threads")
+    print(json.dumps(line))
+    return 0
+
+
 def serving_run(ix, ref, n_requests: int, seed: int, rate_hz: float, scale: float):
     """The serving configuration on the resident index: Poisson arrivals, requests of 1k-500k reads
     (log-uniform, times `scale`), lengths 36-150 bp, half default and half aDNA options. Returns reads/s and
@@ -225,16 +330,19 @@ def main():
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--autotune-sample", type=int, default=262144)
     ap.add_argument("--serve-rate", type=float, default=16.0, help="request arrival rate (per second)")
+    ap.add_argument("--index-build", action="store_true", help="time `galn index` on the workload's reference")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.index_build:
+        return index_bench(args, rank, local)
     if args.impl == "reference":
         if rank != 0:
             return 0
-        import torch  # noqa: F401  (index build)
-        d, prefix, ref, reads, opts = prepare(args.workload, args.scale, 0, local, args.data_dir, args.reads_scale)
+        d, prefix, ref, reads, opts = prepare(args.workload, args.scale, 0, local, args.data_dir, args.reads_scale,
+                                              reference_builder=True)
         cb, why = cpu_reference(prefix, reads, opts, args.cpu_sample, d, steps=args.steps, warmup=args.warmup)
         if cb is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))

@@ -107,8 +107,8 @@ def lib():
                                 C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.galn_autotune_clear.argtypes = [vp]
     L.galn_last_graph_launches.argtypes = [vp, C.POINTER(C.c_int64)]
-    L.galn_index_build_text.argtypes = [vp, C.c_uint64, C.c_char_p, C.POINTER(BuildStats)]
-    L.galn_index_build_fasta.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(BuildStats)]
+    L.galn_index_build_text.argtypes = [vp, C.c_uint64, C.c_char_p, C.c_int, C.POINTER(BuildStats)]
+    L.galn_index_build_fasta.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(BuildStats)]
     L.galn_fasta_to_pac.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_uint64)]
     L.galn_version.restype = C.c_char_p
     _lib = L
@@ -441,11 +441,11 @@ def _stats_dict(st: BuildStats) -> dict:
     return {f: getattr(st, f) for f, _ in BuildStats._fields_}
 
 
-def index_fasta(fasta: str, prefix: str) -> dict:
-    """`galn index -p prefix fasta` on the current CUDA device: the five bwa index files (galn_index_build_fasta).
+def index_fasta(fasta: str, prefix: str, device: int = 0) -> dict:
+    """`galn index -p prefix fasta` on a CUDA device: the five bwa index files (galn_index_build_fasta).
     Returns the builder's statistics."""
     st = BuildStats()
-    rc = lib().galn_index_build_fasta(fasta.encode(), prefix.encode(), C.byref(st))
+    rc = lib().galn_index_build_fasta(fasta.encode(), prefix.encode(), device, C.byref(st))
     if rc:
         raise GalnError(f"galn_index_build_fasta failed ({rc})")
     return _stats_dict(st)
@@ -460,12 +460,12 @@ def fasta_to_pac(fasta: str, prefix: str) -> int:
     return n.value
 
 
-def index_text(fwd: np.ndarray, prefix: str) -> dict:
+def index_text(fwd: np.ndarray, prefix: str, device: int = 0) -> dict:
     """<prefix>.bwt and <prefix>.sa for the forward sequence fwd (codes 0..3; the text is fwd . revcomp(fwd)),
-    built on the current CUDA device (galn_index_build_text)."""
+    built on a CUDA device (galn_index_build_text)."""
     f = np.ascontiguousarray(fwd, dtype=np.uint8)
     st = BuildStats()
-    rc = lib().galn_index_build_text(f.ctypes.data, len(f), prefix.encode(), C.byref(st))
+    rc = lib().galn_index_build_text(f.ctypes.data, len(f), prefix.encode(), device, C.byref(st))
     if rc:
         raise GalnError(f"galn_index_build_text failed ({rc})")
     return _stats_dict(st)

@@ -161,12 +161,21 @@ __global__ void __launch_bounds__(kRThreads) radix_hist(const uint64_t *__restri
     if (t < 256) h[t] = 0;
     __syncthreads();
     const uint64_t base = (uint64_t)blockIdx.x * kRTile;
-    for (int j = 0; j < kRItems; ++j) {
+    uint32_t dg[kRItems];
+#pragma unroll
+    for (int j = 0; j < kRItems; ++j) {   // all loads first
         const uint64_t i = base + (uint64_t)j * kRThreads + t;
-        const bool ok = i < n;
-        const uint32_t d = ok ? (uint32_t)(keys[i] >> shift) & 255u : 256u;
+        dg[j] = i < n ? (uint32_t)(keys[i] >> shift) & 255u : 256u;
+    }
+#pragma unroll
+    for (int j = 0; j < kRItems; ++j) {
+        const uint32_t d = dg[j];
+        if (__all_sync(0xffffffffu, d == __shfl_sync(0xffffffffu, d, 0))) {   // one digit in the whole warp
+            if (lane == 0 && d < 256u) atomicAdd(&h[d], 32u);
+            continue;
+        }
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (ok && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+        if (d < 256u && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
     }
     __syncthreads();
     if (t < 256) counts[(uint64_t)t * tiles + blockIdx.x] = h[t];
@@ -194,23 +203,27 @@ __global__ void __launch_bounds__(kRThreads) radix_scatter(const uint64_t *__res
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    for (int i = t; i < kRWarps * 256; i += kRThreads) (&S.wcnt[0][0])[i] = 0;
-    if (t < 256) S.gofs[t] = offsets[(uint64_t)t * tiles + blockIdx.x];
-    __syncthreads();
-
     const uint64_t base = (uint64_t)blockIdx.x * kRTile;
     const uint64_t wbase = base + (uint64_t)w * (32 * kRItems);
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint64_t key[kRItems];
     uint32_t val[kRItems], rk[kRItems];
 #pragma unroll
-    for (int j = 0; j < kRItems; ++j) {
+    for (int j = 0; j < kRItems; ++j) {   // all loads in flight while the counters are cleared
         const uint64_t i = wbase + (uint64_t)j * 32 + lane;
         const bool ok = i < n;
         key[j] = ok ? kin[i] : 0;
         val[j] = ok ? vin[i] : 0;
+    }
+    for (int i = t; i < kRWarps * 256; i += kRThreads) (&S.wcnt[0][0])[i] = 0;
+    if (t < 256) S.gofs[t] = offsets[(uint64_t)t * tiles + blockIdx.x];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kRItems; ++j) {
+        const bool ok = wbase + (uint64_t)j * 32 + lane < n;
         const uint32_t d = ok ? (uint32_t)(key[j] >> shift) & 255u : 256u;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const bool uni = __all_sync(0xffffffffu, d == __shfl_sync(0xffffffffu, d, 0));
+        const uint32_t peers = uni ? 0xffffffffu : __match_any_sync(0xffffffffu, d);
         const uint32_t c = ok ? S.wcnt[w][d] : 0u;
         rk[j] = c + (uint32_t)__popc(peers & lt_mask);
         __syncwarp();

@@ -14,8 +14,10 @@
 #include <string.h>
 #include <zlib.h>
 
+#include <algorithm>
 #include <chrono>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "galn_aln.h"
@@ -32,6 +34,18 @@ inline bool is_space(int c) { return c == ' ' || (c >= '\t' && c <= '\r'); }
 
 int read_all(const char *path, std::vector<uint8_t> &B)
 {
+    if (FILE *f = fopen(path, "rb")) {            // a plain file: one read of its size
+        unsigned char magic[2] = {0, 0};
+        const size_t got = fread(magic, 1, 2, f);
+        if (!(got == 2 && magic[0] == 0x1f && magic[1] == 0x8b) && fseeko(f, 0, SEEK_END) == 0) {
+            const off_t n = ftello(f);
+            B.resize(n > 0 ? (size_t)n : 0);
+            const bool ok = n >= 0 && fseeko(f, 0, SEEK_SET) == 0 && fread(B.data(), 1, B.size(), f) == B.size();
+            fclose(f);
+            return ok ? 0 : GALN_EIO;
+        }
+        fclose(f);
+    }
     gzFile fp = gzopen(path, "rb");
     if (!fp) return GALN_EIO;
     gzbuffer(fp, 1 << 20);
@@ -68,7 +82,9 @@ int parse_records(const std::vector<uint8_t> &B, std::vector<Record> &recs)
     std::vector<int64_t> starts;       // the '>' or '@' of each record
     if (q < N) starts.push_back(q);
     for (int64_t p = q; p + 1 < N; ++p) {
-        if (B[p] != '\n') continue;
+        const uint8_t *nl = (const uint8_t *)memchr(B.data() + p, '\n', N - 1 - p);
+        if (!nl) break;
+        p = nl - B.data();
         if (B[p + 1] == '>' || B[p + 1] == '@') starts.push_back(p + 1);
         else if (B[p + 1] == '+') return GALN_EINVAL;   // FASTQ
     }
@@ -100,17 +116,16 @@ int parse_records(const std::vector<uint8_t> &B, std::vector<Record> &recs)
     return 0;
 }
 
-// one record's sequence bytes
-void record_seq(const std::vector<uint8_t> &B, const Record &r, std::string &out)
+// one record's sequence bytes, appended to out
+void record_seq(const std::vector<uint8_t> &B, const Record &r, std::vector<uint8_t> &out)
 {
-    out.clear();
     int64_t x = r.rs;
     while (x < r.re) {
         const uint8_t *nl = (const uint8_t *)memchr(B.data() + x, '\n', r.re - x);
         const int64_t e = nl ? nl - B.data() : r.re;
         int64_t f = e;
         if (e > x && B[e - 1] == '\r' && cr_dropped(B, e - 1, r.rs)) f = e - 1;
-        out.append((const char *)B.data() + x, f - x);
+        out.insert(out.end(), B.begin() + x, B.begin() + f);
         x = e + 1;
     }
 }
@@ -121,16 +136,16 @@ struct Hole {
     char amb;
 };
 
-int nt4(uint8_t c)
-{
-    switch (c) {
-    case 'A': case 'a': return 0;
-    case 'C': case 'c': return 1;
-    case 'G': case 'g': return 2;
-    case 'T': case 't': return 3;
-    default: return 4;
+struct Nt4Table {
+    uint8_t v[256];
+    Nt4Table()
+    {
+        memset(v, 4, sizeof v);
+        const char *b = "ACGT";
+        for (int c = 0; c < 4; ++c) v[(uint8_t)b[c]] = v[(uint8_t)b[c] + 32] = (uint8_t)c;
     }
-}
+};
+const Nt4Table kNt4;
 
 int write_bytes(const std::string &path, const void *p, size_t n)
 {
@@ -140,7 +155,22 @@ int write_bytes(const std::string &path, const void *p, size_t n)
     return (fclose(f) == 0 && ok) ? 0 : GALN_EIO;
 }
 
-// FASTA -> .pac/.ann/.amb; F = the forward sequence as codes 0..3
+// body(lo, hi) over [0, n) split among the host's threads
+template <class Fn>
+void parallel_range(uint64_t n, Fn body)
+{
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const uint64_t parts = std::min<uint64_t>(hw, std::max<uint64_t>(1, n >> 20));
+    if (parts <= 1) { body((uint64_t)0, n); return; }
+    std::vector<std::thread> th;
+    for (uint64_t t = 0; t < parts; ++t)
+        th.emplace_back(body, n * t / parts, n * (t + 1) / parts);
+    for (auto &x : th) x.join();
+}
+
+// FASTA -> .pac/.ann/.amb; F = the forward sequence as codes 0..3. The sequence bytes of all records are
+// gathered first; bases are coded by threads, ambiguous ones are then replaced in order (their lrand48 draws
+// and holes depend only on what came before them).
 int fasta_to_pac(const char *fasta, const std::string &prefix, std::vector<uint8_t> &F)
 {
     std::vector<uint8_t> B;
@@ -149,41 +179,65 @@ int fasta_to_pac(const char *fasta, const std::string &prefix, std::vector<uint8
     std::vector<Record> recs;
     rc = parse_records(B, recs);
     if (rc) return rc;
-    F.clear();
+    std::vector<uint8_t> S;                          // every record's sequence bytes, in order
+    S.reserve(B.size());
+    std::vector<int64_t> rec_off(recs.size() + 1);
+    for (size_t i = 0; i < recs.size(); ++i) {
+        rec_off[i] = (int64_t)S.size();
+        record_seq(B, recs[i], S);
+    }
+    rec_off[recs.size()] = (int64_t)S.size();
+    std::vector<uint8_t>().swap(B);
+    const uint64_t l_pac = S.size();
+    if (l_pac == 0) return GALN_EINVAL;
+    F.resize(l_pac);
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::vector<int64_t>> amb_at(hw);
+    {
+        const uint64_t parts = std::min<uint64_t>(hw, std::max<uint64_t>(1, l_pac >> 20));
+        std::vector<std::thread> th;
+        for (uint64_t t = 0; t < parts; ++t)
+            th.emplace_back([&, t] {
+                const uint64_t a = l_pac * t / parts, b = l_pac * (t + 1) / parts;
+                for (uint64_t i = a; i < b; ++i) {
+                    const uint8_t c = kNt4.v[S[i]];
+                    F[i] = c;
+                    if (c > 3) amb_at[t].push_back((int64_t)i);
+                }
+            });
+        for (auto &x : th) x.join();
+    }
     std::vector<Hole> holes;
-    std::vector<int64_t> rec_len(recs.size()), rec_off(recs.size());
     std::vector<int> rec_ambs(recs.size());
     uint64_t x = (11ull << 16) | 0x330Eull;          // srand48(11)
     const uint64_t a = 0x5DEECE66Dull, cst = 0xB, m48 = (1ull << 48) - 1;
-    std::string seq;
-    for (size_t i = 0; i < recs.size(); ++i) {
-        record_seq(B, recs[i], seq);
-        rec_off[i] = (int64_t)F.size();
-        rec_len[i] = (int64_t)seq.size();
-        int last = 0;
-        for (size_t j = 0; j < seq.size(); ++j) {
-            const uint8_t ch = (uint8_t)seq[j];
-            int c = nt4(ch);
-            if (c >= 4) {
-                if (last == ch) ++holes.back().len;
-                else {
-                    holes.push_back(Hole{rec_off[i] + (int64_t)j, 1, (char)ch});
-                    ++rec_ambs[i];
-                }
-                x = (a * x + cst) & m48;             // lrand48() & 3
-                c = (int)((x >> 17) & 3);
+    size_t r = 0;
+    for (const auto &v : amb_at)
+        for (const int64_t i : v) {
+            while (rec_off[r + 1] <= i) ++r;
+            if (i > rec_off[r] && S[i - 1] == S[i]) ++holes.back().len;   // the same ambiguous byte: one hole
+            else {
+                holes.push_back(Hole{i, 1, (char)S[i]});
+                ++rec_ambs[r];
             }
-            last = ch;
-            F.push_back((uint8_t)c);
+            x = (a * x + cst) & m48;                 // lrand48() & 3
+            F[i] = (uint8_t)((x >> 17) & 3);
         }
-    }
-    const uint64_t l_pac = F.size();
-    if (l_pac == 0) return GALN_EINVAL;
-    std::vector<uint8_t> pac((l_pac + 3) / 4, 0);
-    for (uint64_t i = 0; i < l_pac; ++i) pac[i >> 2] |= (uint8_t)(F[i] << ((~i & 3) << 1));
-    if (l_pac % 4 == 0) pac.push_back(0);
-    pac.push_back((uint8_t)(l_pac % 4));
-    rc = write_bytes(prefix + ".pac", pac.data(), pac.size());
+    std::vector<uint8_t> pac((l_pac + 3) / 4 + 2, 0);
+    parallel_range((l_pac + 3) / 4, [&](uint64_t lo, uint64_t hi) {
+        for (uint64_t j = lo; j < hi; ++j) {
+            uint8_t v = 0;
+            for (int k = 0; k < 4; ++k) {
+                const uint64_t i = 4 * j + k;
+                v |= (uint8_t)((i < l_pac ? F[i] : 0) << (6 - 2 * k));
+            }
+            pac[j] = v;
+        }
+    });
+    size_t np = (l_pac + 3) / 4;
+    if (l_pac % 4 == 0) pac[np++] = 0;
+    pac[np++] = (uint8_t)(l_pac % 4);
+    rc = write_bytes(prefix + ".pac", pac.data(), np);
     if (rc) return rc;
     std::string ann, amb;
     char line[256];
@@ -191,7 +245,8 @@ int fasta_to_pac(const char *fasta, const std::string &prefix, std::vector<uint8
     ann += line;
     for (size_t i = 0; i < recs.size(); ++i) {
         ann += "0 " + recs[i].name + " " + recs[i].anno + "\n";
-        snprintf(line, sizeof line, "%lld %d %d\n", (long long)rec_off[i], (int)rec_len[i], rec_ambs[i]);
+        snprintf(line, sizeof line, "%lld %d %d\n", (long long)rec_off[i], (int)(rec_off[i + 1] - rec_off[i]),
+                 rec_ambs[i]);
         ann += line;
     }
     snprintf(line, sizeof line, "%llu %d %u\n", (unsigned long long)l_pac, (int)recs.size(), (unsigned)holes.size());
@@ -225,7 +280,8 @@ double now_ms()
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-int build_text(const uint8_t *fwd, uint64_t l_pac, const std::string &prefix, galn_build_stats *stats, double ms_before)
+int build_text(const uint8_t *fwd, uint64_t l_pac, const std::string &prefix, int device, galn_build_stats *stats,
+               double ms_before)
 {
     for (uint64_t i = 0; i < l_pac; ++i)
         if (fwd[i] > 3) return GALN_EINVAL;
@@ -233,6 +289,7 @@ int build_text(const uint8_t *fwd, uint64_t l_pac, const std::string &prefix, ga
     std::vector<uint64_t> samples;
     uint64_t L2[5] = {0, 0, 0, 0, 0}, primary = 0;
     galn_build_stats st{};
+    if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return GALN_ECUDA; }
     int rc = galn::dev_build_bwt_sa(fwd, l_pac, bwt, L2, primary, samples, &st);
     if (rc) return rc;
     const double t0 = now_ms();
@@ -244,10 +301,11 @@ int build_text(const uint8_t *fwd, uint64_t l_pac, const std::string &prefix, ga
 
 }  // namespace
 
-extern "C" int galn_index_build_text(const uint8_t *fwd, uint64_t l_pac, const char *prefix, galn_build_stats *stats)
+extern "C" int galn_index_build_text(const uint8_t *fwd, uint64_t l_pac, const char *prefix, int device,
+                                     galn_build_stats *stats)
 {
     if (!fwd || !prefix || l_pac == 0) return GALN_EINVAL;
-    return build_text(fwd, l_pac, prefix, stats, 0.0);
+    return build_text(fwd, l_pac, prefix, device, stats, 0.0);
 }
 
 extern "C" int galn_fasta_to_pac(const char *fasta, const char *prefix, uint64_t *l_pac)
@@ -259,12 +317,12 @@ extern "C" int galn_fasta_to_pac(const char *fasta, const char *prefix, uint64_t
     return rc;
 }
 
-extern "C" int galn_index_build_fasta(const char *fasta, const char *prefix, galn_build_stats *stats)
+extern "C" int galn_index_build_fasta(const char *fasta, const char *prefix, int device, galn_build_stats *stats)
 {
     if (!fasta || !prefix) return GALN_EINVAL;
     const double t0 = now_ms();
     std::vector<uint8_t> F;
     int rc = fasta_to_pac(fasta, prefix, F);
     if (rc) return rc;
-    return build_text(F.data(), F.size(), prefix, stats, now_ms() - t0);
+    return build_text(F.data(), F.size(), prefix, device, stats, now_ms() - t0);
 }

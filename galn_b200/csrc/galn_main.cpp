@@ -408,10 +408,9 @@ static int index_main(int argc, char **argv)
     }
     if (!fa) return index_usage();
     if (!prefix) prefix = fa;
-    if (cudaSetDevice(device) != cudaSuccess) { fprintf(stderr, "[galn index] no CUDA device %d\n", device); return 10; }
     galn_build_stats st{};
     const auto t0 = std::chrono::steady_clock::now();
-    const int rc = galn_index_build_fasta(fa, prefix, &st);
+    const int rc = galn_index_build_fasta(fa, prefix, device, &st);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (rc) {
         fprintf(stderr, "[galn index] failed (%d) for %s\n", rc, fa);

@@ -178,14 +178,14 @@ typedef struct {
  * refused (GALN_EINVAL), as is an input without bases. */
 int galn_fasta_to_pac(const char *fasta, const char *prefix, uint64_t *l_pac);
 
-/* .bwt and .sa for the forward sequence fwd[0..l_pac) (codes 0..3) on the current device.
+/* .bwt and .sa for the forward sequence fwd[0..l_pac) (codes 0..3), built on `device`.
  * Returns 0, GALN_EINVAL (empty or too long), GALN_ENOMEM (device memory), GALN_EIO or GALN_ECUDA.
  * stats may be NULL. */
-int galn_index_build_text(const uint8_t *fwd, uint64_t l_pac, const char *prefix, galn_build_stats *stats);
+int galn_index_build_text(const uint8_t *fwd, uint64_t l_pac, const char *prefix, int device, galn_build_stats *stats);
 
-/* All five files for a FASTA file (plain or gzip) on the current device, as `galn index -a gpu
- * -p <prefix> <fasta>` writes them (src/index/galn_index.c:36-71). */
-int galn_index_build_fasta(const char *fasta, const char *prefix, galn_build_stats *stats);
+/* All five files for a FASTA file (plain or gzip), built on `device`, as `galn index -a gpu -p <prefix>
+ * <fasta>` writes them (src/index/galn_index.c:36-71). */
+int galn_index_build_fasta(const char *fasta, const char *prefix, int device, galn_build_stats *stats);
 
 /* ---- .sai ----------------------------------------------------------------------------------------------- */
 /* "SAI\1", the option block, then per read int32 n_aln and the records (src/sai_writer.h:9-21). A read
