@@ -87,3 +87,18 @@ def test_forward_from_pac_round_trip(tmp_path):
         galn_b200.fasta_to_pac(str(fa), str(tmp_path / f"s{n}"))
         F = oracle.forward_from_pac(str(tmp_path / f"s{n}.pac"))
         assert "".join("ACGT"[c] for c in F) == seq
+
+
+def test_command_line_options_without_a_gpu(tmp_path):
+    """`galn index` refuses the CPU builder, unknown builders and options, and a missing FASTA argument with
+    exit code 1 before touching a device."""
+    import subprocess
+    from galn_b200 import build
+    build.build()
+    fa = os.path.join(GOLDEN, "index", "tiny3", "ref.fa")
+    pre = ["-p", str(tmp_path / "x")]
+    for args in (pre, pre + ["-a", "cpu", fa], pre + ["--cpu", fa], pre + ["-a", "bogus", fa], pre + ["--bogus", fa],
+                 pre + [fa, fa]):
+        p = subprocess.run([build.CLI, "index", *args], capture_output=True, text=True)
+        assert p.returncode == 1, (args, p.stderr)
+        assert not os.path.exists(str(tmp_path / "x.pac"))
