@@ -173,7 +173,7 @@ def cpu_reference(prefix, reads, opts, sample, d, steps=1, warmup=0):
 
 def index_bench(args, rank: int, local: int) -> int:
     """--index-build: `galn index` on the workload's reference (FASTA on disk to the five bwa index files).
-    value = reference bp / device span of the builder (text upload to the last result copy); e2e = reference
+    value = reference bp / device span of the builder (text in HBM to results in HBM); e2e = reference
     bp / wall time of galn_index_build_fasta (FASTA parse, device build, file writes); the roofline is the
     radix scatter (24 B of keys and values read and written per item and pass); cpu_baseline = the reference's
     own CPU builder (`galn index -a cpu`, oracle/_ref/galn_index_cpu) on the same FASTA, all host threads.
@@ -253,6 +253,7 @@ def index_bench(args, rank: int, local: int) -> int:
                          "frac": sc_bytes / (ms_sc / 1e3) / 1e9 / hbm, "peak_kind": hbm_kind, "traffic": None},
             "builder": {"text_symbols": n, "rounds": sts[0]["rounds"], "radix_passes": sts[0]["sort_passes"],
                         "sorted_items": sts[0]["sorted_items"], "ms_scatter": ms_sc,
+                        "ms_copies": statistics.mean(x["ms_copies"] for x in sts),
                         "ms_host_files": statistics.mean(x["ms_files"] for x in sts)},
             "identical_to_reference_builder": same}
     if wref is not None:

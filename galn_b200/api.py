@@ -45,7 +45,7 @@ class _Results(C.Structure):
 class BuildStats(C.Structure):
     _fields_ = [("n", C.c_uint64), ("primary", C.c_uint64), ("rounds", C.c_int), ("sort_passes", C.c_int),
                 ("sorted_items", C.c_uint64), ("scatter_items", C.c_uint64), ("ms_device", C.c_double),
-                ("ms_scatter", C.c_double), ("ms_files", C.c_double)]
+                ("ms_copies", C.c_double), ("ms_scatter", C.c_double), ("ms_files", C.c_double)]
 
 
 def lib_path() -> str:

@@ -483,15 +483,21 @@ int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bw
     }
     cudaStream_t st;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return GALN_ECUDA;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ScatterSmem));
-        attr = true;
-    }
+    // per device: the attribute belongs to the current device's context
+    cudaFuncSetAttribute(radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ScatterSmem));
+    // the copies go straight from and to the caller's pageable arrays: page-locking them for one build costs
+    // more host time than the copies save
+    const uint64_t nb = (N + 127) / 128, nw = (N + 15) / 16;
+    const uint64_t body_words = 16 * nb - (8 - (nw - 8 * (nb - 1)));
+    const uint64_t ns = (N + 32) / 32 - 1;
+    bwt.resize(body_words + 8);
+    samples.resize(ns);
     int rc = 0;
-    cudaEvent_t e0, e1;
+    cudaEvent_t ea, e0, e1, eb;   // upload start, text in HBM, results in HBM, results on the host
+    cudaEventCreate(&ea);
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    cudaEventCreate(&eb);
     Sorter srt;
     Scratch scr;
     {
@@ -513,8 +519,9 @@ int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bw
             rc = GALN_ENOMEM;
         }
         if (!rc) {
-            cudaEventRecord(e0, st);
+            cudaEventRecord(ea, st);
             cudaMemcpyAsync(F_d, F, l_pac, cudaMemcpyHostToDevice, st);
+            cudaEventRecord(e0, st);
             text_from_forward<<<grid(N, 256), 256, 0, st>>>(F_d, l_pac, T);
             cudaMemsetAsync(T + N, 0, 64, st);
             pd_key0<<<grid(N, 256), 256, 0, st>>>(T, N, srt.k[0], srt.v[0]);
@@ -568,12 +575,10 @@ int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bw
                 cudaStreamSynchronize(st) != cudaSuccess)
                 rc = GALN_ECUDA;
             primary = (uint64_t)r0 + 1;
-            const uint64_t nb = (N + 127) / 128, nw = (N + 15) / 16;
             uint8_t *L = reinterpret_cast<uint8_t *>(srt.k[1]);
             U4 *cnt = reinterpret_cast<U4 *>(srt.v[0]);      // nb * 32 bytes <= 4N
             uint32_t *body = srt.v[1];                       // nb * 64 bytes <= 4N + 64
             uint64_t *smp = reinterpret_cast<uint64_t *>(slots[0]);
-            const uint64_t ns = (N + 32) / 32 - 1;
             if (!rc) {
                 bwt_symbols<<<grid(N, 256), 256, 0, st>>>(T, sa, N, primary, L);
                 bwt_block_counts<<<grid(nb, 128), 128, 0, st>>>(L, N, nb, cnt);
@@ -582,15 +587,12 @@ int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bw
             if (!rc) {
                 bwt_write<<<grid(nb * 16, 256), 256, 0, st>>>(L, N, nb, cnt, body);
                 if (ns) sa_samples<<<grid(ns, 256), 256, 0, st>>>(sa, ns, smp);
-                const uint64_t last_words = nw - 8 * (nb - 1);
-                const uint64_t body_words = 16 * nb - (8 - last_words);
-                bwt.resize(body_words + 8);
-                samples.resize(ns);
                 U4 totals{};
+                cudaEventRecord(e1, st);
                 cudaMemcpyAsync(bwt.data(), body, body_words * 4, cudaMemcpyDeviceToHost, st);
                 cudaMemcpyAsync(&totals, cnt + nb - 1, sizeof(U4), cudaMemcpyDeviceToHost, st);
                 if (ns) cudaMemcpyAsync(samples.data(), smp, ns * 8, cudaMemcpyDeviceToHost, st);
-                cudaEventRecord(e1, st);
+                cudaEventRecord(eb, st);
                 if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = GALN_ECUDA;
                 if (!rc) {
                     memcpy(bwt.data() + body_words, totals.c, sizeof(totals.c));
@@ -606,9 +608,12 @@ int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bw
             stats->sorted_items = sorted;
             stats->sort_passes = srt.passes;
             stats->scatter_items = srt.scatter_items;
-            float ms = 0;
+            float ms = 0, up = 0, down = 0;
             cudaEventElapsedTime(&ms, e0, e1);
+            cudaEventElapsedTime(&up, ea, e0);
+            cudaEventElapsedTime(&down, e1, eb);
             stats->ms_device = ms;
+            stats->ms_copies = up + down;
             double sc = 0;
             for (size_t i = 0; i + 1 < srt.ev.size(); i += 2) {
                 float x = 0;
@@ -620,8 +625,10 @@ int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bw
         if (rc) cudaStreamSynchronize(st);
     }
     for (cudaEvent_t e : srt.ev) cudaEventDestroy(e);
+    cudaEventDestroy(ea);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    cudaEventDestroy(eb);
     cudaStreamDestroy(st);
     if (rc == GALN_ECUDA) cudaGetLastError();
     return rc;

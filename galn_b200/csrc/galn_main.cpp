@@ -418,8 +418,8 @@ static int index_main(int argc, char **argv)
     }
     if (verbose)
         fprintf(stderr, "[galn index] %llu symbols, %d doubling rounds, %d radix passes: device %.1f ms "
-                "(scatter %.1f ms), files %.1f ms, %.2f s in all\n", (unsigned long long)st.n, st.rounds,
-                st.sort_passes, st.ms_device, st.ms_scatter, st.ms_files, secs);
+                "(scatter %.1f ms), copies %.1f ms, files %.1f ms, %.2f s in all\n", (unsigned long long)st.n,
+                st.rounds, st.sort_passes, st.ms_device, st.ms_scatter, st.ms_copies, st.ms_files, secs);
     return 0;
 }
 

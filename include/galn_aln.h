@@ -168,7 +168,8 @@ typedef struct {
     int sort_passes;            /* 8-bit radix passes, all rounds */
     uint64_t sorted_items;      /* (key, position) pairs sorted, all rounds */
     uint64_t scatter_items;     /* items moved by the radix scatter launches (sorted_items x passes) */
-    double ms_device;           /* device time from the text's upload to the last result copy */
+    double ms_device;           /* device time from the text in device memory to the results in device memory */
+    double ms_copies;           /* device time of the text's upload and the results' copy back */
     double ms_scatter;          /* device time of the radix scatter launches */
     double ms_files;            /* host time: FASTA to .pac/.ann/.amb, and writing .bwt/.sa */
 } galn_build_stats;
