@@ -102,3 +102,41 @@ def test_command_line_options_without_a_gpu(tmp_path):
         p = subprocess.run([build.CLI, "index", *args], capture_output=True, text=True)
         assert p.returncode == 1, (args, p.stderr)
         assert not os.path.exists(str(tmp_path / "x.pac"))
+
+
+def test_oracle_suffix_array_agrees_with_prefix_doubling():
+    """The oracle's comparison sort and the fixture builder's prefix doubling (torch on the CPU) are two
+    independent suffix sorts: they agree on random, repetitive and palindromic texts."""
+    from galn_b200 import index_build
+    rng = np.random.default_rng(31)
+    u = rng.integers(0, 4, 3000)
+    for T in (rng.integers(0, 4, 40_000), np.tile(u[:37], 300), np.concatenate([u, 3 - u[::-1], u, u[:1000]])):
+        T = T.astype(np.uint8)
+        np.testing.assert_array_equal(oracle.suffix_array(T).astype(np.int64), index_build.suffix_array(T, "cpu"))
+
+
+def test_host_step_random_fasta_against_fixture_writer(tmp_path):
+    """Random FASTA files (records of random length, lowercase, runs of IUPAC codes, wrapped at random widths)
+    give the same .pac/.ann/.amb from the library's host step as from the fixture builder's writer."""
+    from galn_b200 import index_build
+    rng = np.random.default_rng(8)
+    alphabet = np.frombuffer(b"ACGTACGTACGTacgtNNRYKMnSW", dtype=np.uint8)
+    for case in range(12):
+        parts = []
+        for r in range(int(rng.integers(1, 8))):
+            L = int(rng.integers(0 if r else 1, 3000))
+            seq = alphabet[rng.integers(0, len(alphabet), L)]
+            if L > 50:   # a long run of one ambiguous code
+                a = int(rng.integers(0, L - 40))
+                seq[a:a + 30] = ord("N")
+            w = int(rng.integers(10, 120))
+            body = b"".join(seq[i:i + w].tobytes() + b"\n" for i in range(0, L, w))
+            head = b">c%d" % r + (b" some comment %d" % case if r % 2 else b"")
+            parts.append(head + b"\n" + body)
+        fa = tmp_path / f"r{case}.fa"
+        fa.write_bytes(b"".join(parts))
+        galn_b200.fasta_to_pac(str(fa), str(tmp_path / f"h{case}"))
+        names, comments, seqs = index_build.read_fasta(str(fa))
+        index_build.write_pac_ann_amb(str(tmp_path / f"f{case}"), names, comments, seqs)
+        for ext in ("pac", "ann", "amb"):
+            assert _same(str(tmp_path / f"h{case}.{ext}"), str(tmp_path / f"f{case}.{ext}")), (case, ext)
