@@ -21,9 +21,12 @@
 #include <vector>
 
 #include "galn_aln.h"
+#include "galn_host_internal.h"
 #include "galn_internal.h"
 
 namespace {
+
+using galn::hvec;
 
 struct Record {
     std::string name, anno;
@@ -32,7 +35,7 @@ struct Record {
 
 inline bool is_space(int c) { return c == ' ' || (c >= '\t' && c <= '\r'); }
 
-int read_all(const char *path, std::vector<uint8_t> &B)
+int read_all(const char *path, hvec<uint8_t> &B)
 {
     if (FILE *f = fopen(path, "rb")) {            // a plain file: one read of its size
         unsigned char magic[2] = {0, 0};
@@ -50,12 +53,13 @@ int read_all(const char *path, std::vector<uint8_t> &B)
     if (!fp) return GALN_EIO;
     gzbuffer(fp, 1 << 20);
     B.clear();
-    std::vector<uint8_t> chunk(1 << 22);
     for (;;) {
-        const int n = gzread(fp, chunk.data(), (unsigned)chunk.size());
+        const size_t at = B.size();
+        B.resize(at + (4u << 20));
+        const int n = gzread(fp, B.data() + at, 4u << 20);
         if (n < 0) { gzclose(fp); return GALN_EIO; }
+        B.resize(at + (size_t)n);
         if (n == 0) break;
-        B.insert(B.end(), chunk.begin(), chunk.begin() + n);
     }
     return gzclose(fp) == Z_OK ? 0 : GALN_EIO;
 }
@@ -63,9 +67,8 @@ int read_all(const char *path, std::vector<uint8_t> &B)
 // whether kseq drops the '\r' at x of a sequence that starts at rs: it cuts one '\r' off the end of a line
 // when the sequence read so far is longer than one character; a one-character line at the very end of the
 // input is not cut
-bool cr_dropped(const std::vector<uint8_t> &B, int64_t x, int64_t rs)
+bool cr_dropped(const uint8_t *B, int64_t N, int64_t x, int64_t rs)
 {
-    const int64_t N = (int64_t)B.size();
     if (x + 1 < N && B[x + 1] != '\n') return false;
     if (x == 0 || B[x - 1] != '\n') return true;
     if (x + 1 == N) return false;
@@ -74,7 +77,7 @@ bool cr_dropped(const std::vector<uint8_t> &B, int64_t x, int64_t rs)
     return y >= rs;
 }
 
-int parse_records(const std::vector<uint8_t> &B, std::vector<Record> &recs)
+int parse_records(const hvec<uint8_t> &B, std::vector<Record> &recs)
 {
     const int64_t N = (int64_t)B.size();
     int64_t q = 0;
@@ -116,18 +119,30 @@ int parse_records(const std::vector<uint8_t> &B, std::vector<Record> &recs)
     return 0;
 }
 
-// one record's sequence bytes, appended to out
-void record_seq(const std::vector<uint8_t> &B, const Record &r, std::vector<uint8_t> &out)
+// A piece of one sequence line: input bytes [x, f) go to output offset out.
+struct Seg {
+    int64_t x, f, out;
+};
+
+// the pieces of one record's sequence lines (lines longer than 1 MiB are cut, so threads can share them);
+// returns the record's length
+int64_t record_segs(const hvec<uint8_t> &B, const Record &r, int64_t out, std::vector<Seg> &segs)
 {
+    const int64_t start = out, N = (int64_t)B.size();
     int64_t x = r.rs;
     while (x < r.re) {
         const uint8_t *nl = (const uint8_t *)memchr(B.data() + x, '\n', r.re - x);
         const int64_t e = nl ? nl - B.data() : r.re;
         int64_t f = e;
-        if (e > x && B[e - 1] == '\r' && cr_dropped(B, e - 1, r.rs)) f = e - 1;
-        out.insert(out.end(), B.begin() + x, B.begin() + f);
+        if (e > x && B[e - 1] == '\r' && cr_dropped(B.data(), N, e - 1, r.rs)) f = e - 1;
+        for (int64_t a = x; a < f; a += 1 << 20) {
+            const int64_t b = std::min<int64_t>(f, a + (1 << 20));
+            segs.push_back(Seg{a, b, out});
+            out += b - a;
+        }
         x = e + 1;
     }
+    return out - start;
 }
 
 struct Hole {
@@ -168,41 +183,45 @@ void parallel_range(uint64_t n, Fn body)
     for (auto &x : th) x.join();
 }
 
-// FASTA -> .pac/.ann/.amb; F = the forward sequence as codes 0..3. The sequence bytes of all records are
-// gathered first; bases are coded by threads, ambiguous ones are then replaced in order (their lrand48 draws
-// and holes depend only on what came before them).
-int fasta_to_pac(const char *fasta, const std::string &prefix, std::vector<uint8_t> &F)
+// FASTA -> .pac/.ann/.amb; F = the forward sequence as codes 0..3. The sequence lines of all records are
+// listed first; host threads code them, noting the ambiguous bases, which are then replaced in order (their
+// lrand48 draws and holes depend only on what came before them).
+int fasta_to_pac(const char *fasta, const std::string &prefix, hvec<uint8_t> &F)
 {
-    std::vector<uint8_t> B;
+    hvec<uint8_t> B;
     int rc = read_all(fasta, B);
     if (rc) return rc;
     std::vector<Record> recs;
     rc = parse_records(B, recs);
     if (rc) return rc;
-    std::vector<uint8_t> S;                          // every record's sequence bytes, in order
-    S.reserve(B.size());
+    std::vector<Seg> segs;
+    segs.reserve(B.size() / 48 + recs.size() + 16);
     std::vector<int64_t> rec_off(recs.size() + 1);
+    int64_t total = 0;
     for (size_t i = 0; i < recs.size(); ++i) {
-        rec_off[i] = (int64_t)S.size();
-        record_seq(B, recs[i], S);
+        rec_off[i] = total;
+        total += record_segs(B, recs[i], total, segs);
     }
-    rec_off[recs.size()] = (int64_t)S.size();
-    std::vector<uint8_t>().swap(B);
-    const uint64_t l_pac = S.size();
+    rec_off[recs.size()] = total;
+    const uint64_t l_pac = (uint64_t)total;
     if (l_pac == 0) return GALN_EINVAL;
     F.resize(l_pac);
     const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    std::vector<std::vector<int64_t>> amb_at(hw);
+    const size_t parts = std::min<size_t>(hw, std::max<size_t>(1, (size_t)(l_pac >> 20)));
+    std::vector<std::vector<int64_t>> amb_at(parts);   // position << 8 | the ambiguous byte
     {
-        const uint64_t parts = std::min<uint64_t>(hw, std::max<uint64_t>(1, l_pac >> 20));
         std::vector<std::thread> th;
-        for (uint64_t t = 0; t < parts; ++t)
+        for (size_t t = 0; t < parts; ++t)
             th.emplace_back([&, t] {
-                const uint64_t a = l_pac * t / parts, b = l_pac * (t + 1) / parts;
-                for (uint64_t i = a; i < b; ++i) {
-                    const uint8_t c = kNt4.v[S[i]];
-                    F[i] = c;
-                    if (c > 3) amb_at[t].push_back((int64_t)i);
+                const size_t a = segs.size() * t / parts, b = segs.size() * (t + 1) / parts;
+                for (size_t k = a; k < b; ++k) {
+                    const Seg &g = segs[k];
+                    uint8_t *o = F.data() + g.out;
+                    for (int64_t j = g.x; j < g.f; ++j) {
+                        const uint8_t ch = B[j], c = kNt4.v[ch];
+                        o[j - g.x] = c;
+                        if (c > 3) amb_at[t].push_back((g.out + (j - g.x)) << 8 | ch);
+                    }
                 }
             });
         for (auto &x : th) x.join();
@@ -212,18 +231,23 @@ int fasta_to_pac(const char *fasta, const std::string &prefix, std::vector<uint8
     uint64_t x = (11ull << 16) | 0x330Eull;          // srand48(11)
     const uint64_t a = 0x5DEECE66Dull, cst = 0xB, m48 = (1ull << 48) - 1;
     size_t r = 0;
+    int64_t prev = -2;                                // the last ambiguous base: position << 8 | byte
     for (const auto &v : amb_at)
-        for (const int64_t i : v) {
+        for (const int64_t pb : v) {
+            const int64_t i = pb >> 8;
+            const uint8_t ch = (uint8_t)(pb & 0xff);
             while (rec_off[r + 1] <= i) ++r;
-            if (i > rec_off[r] && S[i - 1] == S[i]) ++holes.back().len;   // the same ambiguous byte: one hole
+            // the byte before, in the same record, is the same ambiguous byte: the hole goes on
+            if (i > rec_off[r] && prev == (((i - 1) << 8) | ch)) ++holes.back().len;
             else {
-                holes.push_back(Hole{i, 1, (char)S[i]});
+                holes.push_back(Hole{i, 1, (char)ch});
                 ++rec_ambs[r];
             }
+            prev = pb;
             x = (a * x + cst) & m48;                 // lrand48() & 3
             F[i] = (uint8_t)((x >> 17) & 3);
         }
-    std::vector<uint8_t> pac((l_pac + 3) / 4 + 2, 0);
+    hvec<uint8_t> pac((l_pac + 3) / 4 + 2);
     parallel_range((l_pac + 3) / 4, [&](uint64_t lo, uint64_t hi) {
         for (uint64_t j = lo; j < hi; ++j) {
             uint8_t v = 0;
@@ -311,7 +335,7 @@ extern "C" int galn_index_build_text(const uint8_t *fwd, uint64_t l_pac, const c
 extern "C" int galn_fasta_to_pac(const char *fasta, const char *prefix, uint64_t *l_pac)
 {
     if (!fasta || !prefix) return GALN_EINVAL;
-    std::vector<uint8_t> F;
+    hvec<uint8_t> F;
     const int rc = fasta_to_pac(fasta, prefix, F);
     if (!rc && l_pac) *l_pac = F.size();
     return rc;
@@ -321,7 +345,7 @@ extern "C" int galn_index_build_fasta(const char *fasta, const char *prefix, int
 {
     if (!fasta || !prefix) return GALN_EINVAL;
     const double t0 = now_ms();
-    std::vector<uint8_t> F;
+    hvec<uint8_t> F;
     int rc = fasta_to_pac(fasta, prefix, F);
     if (rc) return rc;
     return build_text(F.data(), F.size(), prefix, device, stats, now_ms() - t0);
