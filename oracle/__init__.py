@@ -1,9 +1,11 @@
 """Test infrastructure: the CPU oracle for the `bwa aln` search, and the reference itself.
 
 Only tests/, __graft_entry__.smoke() and the cpu_baseline / reference legs of bench.py use this package,
-and only as the checker (or, for the reference leg, as the timed CPU baseline); the product never imports it.
+and only as the checker (or, for the reference legs, as the timed CPU baseline and the reference arm's index
+builder); the product never imports it.
 
-  * liboracle.so          this project's own C restatement of the reference's search (galn_oracle.c)
+  * liboracle.so          this project's own C restatement of the reference's search, of bwt_sa/bwa_sa2pos and
+                          of the .bwt/.sa index files over a comparison suffix sort (galn_oracle.c)
   * _ref/galn_ref         the reference's `galn aln` built from its own sources (oracle/Makefile)
   * _ref/galn_index_cpu   the reference's CPU index builder
   * _ref/libgalnref_dump.so  per-read dump around the reference's aln_search_host

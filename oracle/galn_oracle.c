@@ -1,4 +1,5 @@
-/* galn_oracle.c -- test infrastructure: the CPU restatement of the `bwa aln` search (parity oracle).
+/* galn_oracle.c -- test infrastructure: the CPU restatement of the `bwa aln` search, of samse's coordinate
+ * step and of the bwa index files (parity oracle).
  * See galn_oracle.h for what it covers and which reference lines each part follows. Compiled with
  * -ffp-contract=off so that bwa_cal_maxdiff rounds as the reference does (CMakeLists.txt:24-25).
  */
