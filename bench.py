@@ -56,6 +56,32 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+# DRAM bytes per pop of the warp tier, from one ncu capture of it on a steady-state aDNA case (60,000 heavy
+# reads, 534.5 M pops, every warp busy): 35.1 GB read + 33.0 GB written.
+WARP_DRAM_BYTES_PER_POP = (35.1e9 + 33.0e9) / 534.5e6
+
+
+# DRAM bytes per item and pass of the index builder's radix scatter, from one ncu capture of it on a 10 Mbp
+# reference (2 x 10^7 items in one pass): 245.1 MB read + 192.2 MB written.
+SCATTER_DRAM_BYTES_PER_ITEM = (245.1e6 + 192.2e6) / 2e7
+
+
+def scaled_traffic(dom: int, workload: str, tiers_info: dict):
+    """DRAM bytes of one launch of the dominant kernel, scaled from the ncu capture by the launch's pops (the
+    aDNA workload's warp tier only; None otherwise), and how it was obtained."""
+    try:
+        if dom != 1 or workload != "adna":
+            return None, None
+        pops = int((tiers_info.get("warp_counters") or {}).get("pops") or 0)
+        if pops <= 0:
+            return None, None
+        return (WARP_DRAM_BYTES_PER_POP * pops,
+                "ncu dram__bytes_read.sum + dram__bytes_write.sum of the warp tier on a steady-state aDNA case "
+                "(68.1 GB for 534.5 M pops), scaled by this launch's pops")
+    except (TypeError, ValueError, AttributeError):
+        return None, None
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -250,7 +276,11 @@ def index_bench(args, rank: int, local: int) -> int:
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "kernel": "radix_scatter (all passes of all doubling rounds)",
                          "achieved": sc_bytes / (ms_sc / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
-                         "frac": sc_bytes / (ms_sc / 1e3) / 1e9 / hbm, "peak_kind": hbm_kind, "traffic": None},
+                         "frac": sc_bytes / (ms_sc / 1e3) / 1e9 / hbm, "peak_kind": hbm_kind,
+                         "traffic": SCATTER_DRAM_BYTES_PER_ITEM * sts[0]["scatter_items"],
+                         "traffic_how": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one radix_scatter launch "
+                                        "on a 10 Mbp reference (437.3 MB for 2 x 10^7 items), scaled by the items of "
+                                        "all scatter launches of this build"},
             "builder": {"text_symbols": n, "rounds": sts[0]["rounds"], "radix_passes": sts[0]["sort_passes"],
                         "sorted_items": sts[0]["sorted_items"], "ms_scatter": ms_sc,
                         "ms_copies": statistics.mean(x["ms_copies"] for x in sts),
@@ -467,12 +497,7 @@ def main():
     ix_bytes = os.path.getsize(prefix + ".bwt")   # the occ64 index has the .bwt body's size
     ix_pow2 = 1 << max(20, (ix_bytes - 1).bit_length())
     gather_ix_gbs = gather_peak(ix_pow2)       # a buffer of the index's size (next power of two)
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        tj = json.load(open(tp)).get(args.workload)
-        if tj:
-            traffic = tj.get("dram_bytes_per_launch")
+    traffic, traffic_how = scaled_traffic(dom, args.workload, tiers_info)
 
     plain = None
     if not args.no_plain and engine != galn_b200.GALN_ENGINE_PLAIN:
@@ -509,7 +534,7 @@ def main():
                    "parallelism": f"{world} independent GPU shards (reads split, index replicated)"},
         "e2e": {"value": total_reads / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind,
+                     "traffic": traffic, "traffic_how": traffic_how, "peak_kind": peak_kind,
                      "kernel": TIER_NAMES[min(dom, 2)],
                      "algorithmic_bytes_per_launch": 32 * fetch_dom, "fetches_all_tiers": fetch_all,
                      "ms_per_launch": 1e3 * dom_s,
