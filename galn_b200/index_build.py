@@ -1,8 +1,8 @@
-"""BWA-format index files for a FASTA reference: <prefix>.pac/.ann/.amb/.bwt/.sa.
+"""BWA-format index files for a FASTA reference: <prefix>.pac/.ann/.amb/.bwt/.sa, in Python on torch.
 
-This is the data-preparation step that gives the aln search its input; building indexes is not the
-search itself. The files follow `bwa index` 0.7.19 byte for byte (the BWT of a text is unique, so any
-correct suffix sort gives the same .bwt):
+The library's own builder is `galn index` (galn_index_build_fasta: the suffix sort in CUDA kernels); this
+module is a second, independent implementation that the tests compare it with. The files follow `bwa
+index` 0.7.19 byte for byte (the BWT of a text is unique, so any correct suffix sort gives the same .bwt):
 
   * text T = F . revcomp(F), F the forward 2-bit sequence; an ambiguous base becomes lrand48() & 3 from
     a generator seeded with srand48(11), drawn in sequence order; runs of the same ambiguous character
