@@ -17,7 +17,10 @@
 #include <zlib.h>
 
 #include <algorithm>
+#include <condition_variable>
+#include <deque>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -120,23 +123,101 @@ extern "C" int galn_cal_maxdiff(int l, double err, double thres)
 
 namespace {
 
-// the input as a byte stream: decompressed in 4 MiB steps and parsed as it arrives; bytes already consumed
-// are dropped from the front of the buffer
+// the input as a byte stream, parsed as it arrives; bytes already consumed are dropped from the front of the
+// buffer. A gzip input is inflated ahead by a thread of its own (up to four 8 MiB blocks), so inflating and
+// parsing overlap; a plain input is read in the parsing thread.
 struct Src {
     gzFile fp = nullptr;
     std::vector<unsigned char> buf;
     size_t n = 0, i = 0;
     bool eof = false, err = false;
+    // read-ahead of a gzip input
+    bool ahead = false;
+    std::thread th;
+    std::mutex mu;
+    std::condition_variable cv_ready, cv_room;
+    std::deque<std::vector<unsigned char>> ready;
+    std::vector<std::vector<unsigned char>> spare;
+    bool done = false, stop = false, ahead_err = false;
+    static constexpr size_t kBlock = 8u << 20;
+    static constexpr size_t kAhead = 4;
+
+    void start()
+    {
+        if (!fp || gzdirect(fp)) return;
+        ahead = true;
+        th = std::thread([this] { inflate_ahead(); });
+    }
+    void inflate_ahead()
+    {
+        for (;;) {
+            std::vector<unsigned char> b;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_room.wait(lk, [&] { return stop || ready.size() < kAhead; });
+                if (stop) return;
+                if (!spare.empty()) { b.swap(spare.back()); spare.pop_back(); }
+            }
+            b.resize(kBlock);
+            const int r = gzread(fp, b.data(), (unsigned)b.size());
+            std::lock_guard<std::mutex> lk(mu);
+            if (r <= 0) {
+                ahead_err = r < 0;
+                done = true;
+                cv_ready.notify_all();
+                return;
+            }
+            b.resize((size_t)r);
+            ready.push_back(std::move(b));
+            cv_ready.notify_all();
+        }
+    }
+    // stops the read-ahead thread (before gzclose, or when the stream is dropped early)
+    void finish()
+    {
+        if (!ahead) return;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        cv_room.notify_all();
+        th.join();
+        ahead = false;
+    }
+    ~Src() { finish(); }
     bool fill()
     {
         if (eof) return false;
         if (i > 0 && i == n) { n = 0; i = 0; }
         else if (i > (size_t)(16 << 20)) { memmove(buf.data(), buf.data() + i, n - i); n -= i; i = 0; }
-        if (buf.size() - n < (size_t)(4 << 20)) buf.resize(std::max(buf.size() * 2, n + (size_t)(8 << 20)));
-        int r = gzread(fp, buf.data() + n, (unsigned)(buf.size() - n));
-        if (r < 0) { err = true; eof = true; return false; }
-        if (r == 0) { eof = true; return false; }
-        n += (size_t)r;
+        if (!ahead) {
+            if (buf.size() - n < (size_t)(4 << 20)) buf.resize(std::max(buf.size() * 2, n + (size_t)(8 << 20)));
+            int r = gzread(fp, buf.data() + n, (unsigned)(buf.size() - n));
+            if (r < 0) { err = true; eof = true; return false; }
+            if (r == 0) { eof = true; return false; }
+            n += (size_t)r;
+            return true;
+        }
+        std::vector<unsigned char> b;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_ready.wait(lk, [&] { return !ready.empty() || done; });
+            if (ready.empty()) {
+                err = ahead_err;
+                eof = true;
+                return false;
+            }
+            b = std::move(ready.front());
+            ready.pop_front();
+        }
+        cv_room.notify_all();
+        if (buf.size() - n < b.size()) buf.resize(std::max(buf.size() * 2, n + b.size()));
+        memcpy(buf.data() + n, b.data(), b.size());
+        n += b.size();
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            spare.push_back(std::move(b));
+        }
         return true;
     }
     int getc_() { return (i < n || fill()) ? buf[i++] : -1; }
@@ -259,6 +340,7 @@ extern "C" galn_fastq_stream *galn_fastq_open(const char *path, int *err)
     gzbuffer(fp, 1 << 20);
     auto *st = new galn_fastq_stream();
     st->src.fp = fp;
+    st->src.start();
     if (err) *err = 0;
     return st;
 }
@@ -278,6 +360,7 @@ extern "C" int galn_fastq_next(galn_fastq_stream *st, galn_read_set *out)
 extern "C" int galn_fastq_close(galn_fastq_stream *st)
 {
     if (!st) return GALN_EINVAL;
+    st->src.finish();
     int rc = st->src.fp && gzclose(st->src.fp) != Z_OK ? GALN_EIO : 0;
     delete st;
     return rc;

@@ -210,3 +210,45 @@ def test_cli_usage_and_errors(tmp_path):
     assert p.returncode == 1
     p = subprocess.run([cli, "aln", "--cpu-only", "a", "b"], capture_output=True, text=True)
     assert p.returncode == 1
+
+
+@pytest.mark.parametrize("malformed", [None, 1234])
+def test_gzip_input_read_ahead(malformed, tmp_path):
+    """A gzip input is inflated ahead in a thread of its own: the whole-file and batch readers give the same
+    reads as from the plain file, over several 8 MiB blocks and a batch boundary."""
+    path = str(tmp_path / "b.fq")
+    _big_fastq(path, 0x40000 + 3000, malformed_at=malformed)
+    gz = path + ".gz"
+    with open(path, "rb") as f, gzip.open(gz, "wb", compresslevel=1) as g:
+        g.write(f.read())
+    plain = galn_b200.read_fastq(path)
+    whole = galn_b200.read_fastq(gz)
+    np.testing.assert_array_equal(whole.seq, plain.seq)
+    np.testing.assert_array_equal(whole.offset, plain.offset)
+    np.testing.assert_array_equal(whole.batch, plain.batch)
+    parts = list(galn_b200.read_fastq_batches(gz))
+    np.testing.assert_array_equal(np.concatenate([p.seq for p in parts]), plain.seq)
+    np.testing.assert_array_equal(np.concatenate([p.batch for p in parts]), plain.batch)
+
+
+def test_gzip_input_closed_early_or_truncated(tmp_path):
+    """Closing a gzip stream before its end stops the read-ahead; a truncated gzip file is an I/O error."""
+    import ctypes as C
+    path = str(tmp_path / "b.fq")
+    _big_fastq(path, 0x40000 + 3000)
+    gz = path + ".gz"
+    with open(path, "rb") as f, gzip.open(gz, "wb", compresslevel=1) as g:
+        g.write(f.read())
+    it = galn_b200.read_fastq_batches(gz)
+    assert len(next(it)) == 0x40000
+    it.close()
+    L = galn_b200.lib()
+    err = C.c_int(0)
+    st = L.galn_fastq_open(gz.encode(), C.byref(err))
+    assert st and L.galn_fastq_close(st) == 0
+    data = open(gz, "rb").read()
+    cut = str(tmp_path / "cut.fq.gz")
+    with open(cut, "wb") as f:
+        f.write(data[: len(data) // 2])
+    with pytest.raises(galn_b200.GalnError):
+        galn_b200.read_fastq(cut)
