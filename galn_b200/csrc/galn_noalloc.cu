@@ -4,9 +4,10 @@
 // GPU's memory through its own pool and forbids outside cudaMalloc/cudaFree, code running inside a
 // memory budget that must not grow, or a pipeline stage that must not synchronise the device (cudaFree
 // does). For them this entry point takes every input and output as the caller's own device buffers and
-// keeps all of its scratch (per-thread stacks, bucket heads, width arrays, the encoded reads, the work
-// counter and the per-length max_diff table) in one file-scope __device__ array of kScratchBytes. That
-// array belongs to the library: every GPU that loads the library holds it until the process exits.
+// keeps all of its scratch (per-thread stacks, bucket heads, width arrays, the encoded reads and the work
+// counter) in one file-scope __device__ array of kScratchBytes. That array belongs to the library: every
+// GPU that loads the library holds it until the process exits. The per-length max_diff table travels in the
+// kernel's parameters, so the only stream operations of a call are one memset of the counter and the launch.
 //
 // Host code never passes g_scratch itself to a kernel: in host code the name is only a stand-in for the
 // symbol, not a device address. The device address is looked up once per device with
@@ -33,13 +34,11 @@ constexpr int kNaMaxStacks = 512;                      // most score buckets
 constexpr int kNaMaxRec = 256;                         // most records per read
 constexpr int kNaCap = 2048;                           // stack entries per thread (bump-allocated)
 constexpr size_t kHdr = 256;                           // work counter
-constexpr size_t kTable = (size_t)(kNaMaxLen + 1) * 4; // max_diff by read length
 
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 std::mutex g_mu;
 void *g_addr[64];
-int g_table[kNaMaxLen + 1];                            // host staging of the max_diff table
 
 __host__ __device__ inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -54,7 +53,9 @@ struct NaArgs {
     unsigned char *scratch;           // device address of g_scratch
     size_t slot_bytes;
     Workspace ws;                     // arrays inside the scratch (strided by slot)
-    size_t q_off;                     // offset of the per-slot query buffer inside a slot's region
+    size_t q_off;                     // offset of the per-slot query buffers inside the scratch
+    size_t q_stride;                  // bytes per slot's query buffer
+    int16_t md[kNaMaxLen + 1];        // max_diff by read length (bwa_cal_maxdiff, computed on the host)
 };
 
 __global__ void __launch_bounds__(128) noalloc_kernel(const __grid_constant__ NaArgs a)
@@ -62,14 +63,13 @@ __global__ void __launch_bounds__(128) noalloc_kernel(const __grid_constant__ Na
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= a.n_slots) return;
     int32_t *claim = (int32_t *)a.scratch;
-    const int32_t *table = (const int32_t *)(a.scratch + kHdr);
-    uint8_t *q = a.scratch + a.q_off + (size_t)slot * a256(kNaMaxLen);
+    uint8_t *q = a.scratch + a.q_off + (size_t)slot * a.q_stride;
     for (;;) {
         int r = atomicAdd(claim, 1);
         if (r >= a.n) break;
         const int64_t s = a.off[r];
         const int64_t len64 = a.off[r + 1] - s;
-        if (len64 < 0 || len64 > a.max_len) { a.n_aln[r] = -20; continue; }
+        if (len64 < 0 || len64 > a.max_len) { a.n_aln[r] = -20; continue; }   // GALN_EINVAL for this read
         const int len = (int)len64;
         for (int j = 0; j < len; ++j) {   // reverse, complement; anything but ACGT is ambiguous
             uint8_t b;
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(128) noalloc_kernel(const __grid_constant__ Na
         uint32_t fetches = 0;
         cal_width(a.ix, len, q, W, fetches);
         if (use_seed) cal_width(a.ix, a.seed_len, q + (len - a.seed_len), SW, fetches);
-        SearchResult R = match_gap<false, false, false>(a.ix, a.bo, table[len], len, q, W, SW, use_seed, a.ws, slot,
+        SearchResult R = match_gap<false, false, false>(a.ix, a.bo, (int)a.md[len], len, q, W, SW, use_seed, a.ws, slot,
                                                         fetches);
         if (R.ret > 0) {
             const uint64_t *src = a.ws.aln + (size_t)slot * a.ws.aln_cap * 3;
@@ -130,9 +130,9 @@ extern "C" int galn_aln_run_noalloc(galn_index *ix, const galn_opts *o, int32_t 
     const int hcap = bo.n_stacks > 0 ? bo.n_stacks : 1;
     // per-slot strides exactly as match_gap indexes them (cap, hcap, wcap, aln_cap elements)
     const size_t st_ent = (size_t)kNaCap * 16, st_link = (size_t)kNaCap * 4, st_heads = (size_t)hcap * 4,
-                 st_wid = (size_t)wcap * 8, st_aln = (size_t)rec_per_read * 24, st_q = a256(kNaMaxLen);
+                 st_wid = (size_t)wcap * 8, st_aln = (size_t)rec_per_read * 24, st_q = a256((size_t)max_len + 1);
     const size_t slot_bytes = st_ent + st_link + st_heads + st_wid + st_aln + st_q + 6 * 256;
-    const size_t fixed = kHdr + a256(kTable);
+    const size_t fixed = kHdr;
     const int n_slots = (int)std::min<size_t>((size_t)n_reads, (kScratchBytes - fixed) / slot_bytes);
     if (n_slots < 1) return GALN_EINVAL;
 
@@ -151,19 +151,15 @@ extern "C" int galn_aln_run_noalloc(galn_index *ix, const galn_opts *o, int32_t 
             g_addr[dev] = p;
         }
         unsigned char *base = (unsigned char *)g_addr[dev];
-        for (int L = 0; L <= max_len; ++L)
-            g_table[L] = o->fnr > 0.0 ? galn_cal_maxdiff(L, 0.02, o->fnr) : bo.max_diff;
-        for (int L = 0; L <= max_len; ++L)
-            if (g_table[L] > 125) { rc = GALN_EINVAL; break; }
-        if (rc) break;
-        // pageable source: staged before the call returns, so g_table may be rewritten afterwards
-        if (cudaMemsetAsync(base, 0, kHdr, st) != cudaSuccess ||
-            cudaMemcpyAsync(base + kHdr, g_table, (size_t)(max_len + 1) * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) {
-            rc = GALN_ECUDA;
-            break;
-        }
         NaArgs a;
         memset(&a, 0, sizeof(a));
+        for (int L = 0; L <= max_len && !rc; ++L) {
+            const int md = o->fnr > 0.0 ? galn_cal_maxdiff(L, 0.02, o->fnr) : bo.max_diff;
+            if (md < -32768 || md > 125) rc = GALN_EINVAL;
+            else a.md[L] = (int16_t)md;
+        }
+        if (rc) break;
+        if (cudaMemsetAsync(base, 0, kHdr, st) != cudaSuccess) { rc = GALN_ECUDA; break; }
         a.ix.blk = (const uint4 *)ix->dev.blocks;
         a.ix.primary = ix->dev.primary;
         a.ix.seq_len = ix->dev.seq_len;
@@ -181,6 +177,7 @@ extern "C" int galn_aln_run_noalloc(galn_index *ix, const galn_opts *o, int32_t 
         a.ws.wid = (uint64_t *)(base + off);      off += a256(ns * st_wid);
         a.ws.aln = (uint64_t *)(base + off);      off += a256(ns * st_aln);
         a.q_off = off;                            off += a256(ns * st_q);
+        a.q_stride = st_q;
         if (off > kScratchBytes) { rc = GALN_EINVAL; break; }
         a.ws.cap = kNaCap; a.ws.hcap = hcap; a.ws.wcap = wcap; a.ws.aln_cap = rec_per_read;
         noalloc_kernel<<<(n_slots + 127) / 128, 128, 0, st>>>(a);

@@ -12,7 +12,8 @@ import pytest
 import galn_b200
 import oracle
 from conftest import GOLDEN, case_paths, golden_cases
-from galn_b200 import build, index_build, synth
+import fixture_index as index_build
+from galn_b200 import build, synth
 
 pytestmark = pytest.mark.gpu
 INDEX_CASES = sorted(os.listdir(os.path.join(GOLDEN, "index")))

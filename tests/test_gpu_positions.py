@@ -9,7 +9,8 @@ import pytest
 import galn_b200
 import oracle
 from conftest import GOLDEN, case_paths, golden_cases
-from galn_b200 import build, index_build, synth
+import fixture_index as index_build
+from galn_b200 import build, synth
 
 pytestmark = pytest.mark.gpu
 PREFIX = os.path.join(GOLDEN, "small", "ref")

@@ -7,7 +7,7 @@ import pytest
 
 import oracle
 from conftest import GOLDEN, case_paths, golden_cases
-from galn_b200 import index_build
+import fixture_index as index_build
 
 CASES = golden_cases()
 
