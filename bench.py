@@ -14,17 +14,23 @@ table. The L2 cache is flushed (a 512 MB write) before each step, outside the ti
           already in HBM
   e2e     reads / wall time of the whole call (H2D + device + D2H + result assembly)
   roofline  the dominant kernel (the tier with the most device time): 32 B x the algorithmic block fetches
-          of the reads it finished / its time; also against the device's random 32-B gather peak
-  cpu_baseline  the reference's own `galn aln --cpu-only` on a sample of the same reads, all host cores
+          of the reads it finished / its time; also against the device's random 32-B gather peak, swept over
+          buffer sizes and loads in flight
+  cpu_baseline  the reference's own `galn aln --cpu-only` on all reads of the same workload, all host cores;
+          its .sai is compared byte for byte (md5) with this build's (sai_md5_vs_reference)
+  divergent  the high-divergence configuration (the same reference, 100 bp reads at 4% substitutions +
+          0.5% indels, -n 6 -o 2 -e 6 -k 3 -N) at a stated fraction of its 1 M reads: persistent and plain
+          engines, and the reference's .sai on a prefix
+  serving  continuous batching of Poisson-arriving requests on the resident index, p50/p99 latency, every
+          request's .sai against the plain launch and against the reference's own run of that request
 
 --impl reference times only the reference's CPU path (rank 0; other ranks exit at once).
-
 --index-build times `galn index` instead (the GPU index builder on the workload's reference; see index_bench).
+--profile-case warp_steady runs the fixed warp-tier case that ncu captures (see profile_warp_steady).
 """
 from __future__ import annotations
 
 import argparse
-import ctypes
 import datetime
 import hashlib
 import json
@@ -50,6 +56,7 @@ WORKLOAD_DESC = {
                  "substitutions + 0.5% indels; -n 6 -o 2 -e 6 -k 3 -N",
     "genome": "genome-scale shape (scaled): repeat-rich reference with N runs, 150 bp reads; default options",
 }
+L2_NOTE = "flushed before every step (512 MB device write, outside the timed region)"
 
 
 def log(*a):
@@ -88,6 +95,13 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def workload_config(args, world: int, n_reads: int, opts: list[str]) -> dict:
+    """The workload as both arms name it (the same keys and values in the reference arm's line)."""
+    return {"workload": WORKLOAD_DESC[args.workload], "scale": args.scale, "reads_scale": args.reads_scale,
+            "reads_per_gpu": n_reads, "options": " ".join(opts), "l2": L2_NOTE,
+            "parallelism": f"{world} independent GPU shards (reads split, index replicated)"}
 
 
 def prepare(workload: str, scale: float, rank: int, device: int, data_dir: str | None, reads_scale=None,
@@ -158,44 +172,75 @@ def clock_sampler_stop(proc, f, path):
     return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference(prefix, reads, opts, sample, d, steps=1, warmup=0):
-    """The reference's `galn aln --cpu-only` on the first `sample` reads, all host cores."""
-    import oracle
-    from galn_b200 import synth
-    if not os.path.exists(oracle.GALN_REF):
-        return None, "reference binary oracle/_ref/galn_ref not built"
-    cores = os.cpu_count() or 1
+# ------------------------------------------------------------------------------------------------------------
+# the reference's CPU path
 
-    def sample_fastq(m):
+def sample_fastq(reads, m: int, d: str, tag: str) -> str:
+    """The first m reads as a FASTQ file in d (cached)."""
+    from galn_b200 import synth
+    fq = os.path.join(d, f"{tag}_{m}.fq")
+    if not os.path.exists(fq):
         sub = synth.Reads(reads.names[:m], reads.seq[:int(reads.off[m])], reads.off[:m + 1].copy(),
                           reads.qual[:int(reads.off[m])] if reads.qual is not None else None)
-        fq = os.path.join(d, f"sample_{m}.fq")
-        if not os.path.exists(fq):
-            synth.write_fastq(fq, sub)
-        return fq
+        synth.write_fastq(fq + ".part", sub)
+        os.replace(fq + ".part", fq)
+    return fq
 
-    # grow the sample until the reference's search takes a few seconds (its timer has 10 ms resolution)
+
+def reference_run(prefix: str, fq: str, opts: list[str], out_sai: str, cores: int) -> dict:
+    """One `galn aln --cpu-only` run of the reference: its search seconds and the md5 of the .sai it wrote."""
+    import oracle
+    if not os.path.exists(oracle.GALN_REF):
+        return {"error": "reference binary oracle/_ref/galn_ref not built"}
+    info = oracle.run_galn_ref(prefix, fq, opts, out_sai, workers=cores)
+    if info["rc"] not in (0, 4) or "search_s" not in info:
+        return {"error": "reference run failed: " + info["stderr"][-200:]}
+    with open(out_sai, "rb") as f:
+        md5 = hashlib.md5(f.read()).hexdigest()
+    return {"search_s": info["search_s"], "n_reads": info.get("n_reads"), "md5": md5}
+
+
+def cpu_reference_full(prefix, reads, opts, d, cores):
+    """The reference's CPU path on every read of the workload (one run, a few tens of seconds): the
+    cpu_baseline figure and the .sai the GPU arm is compared with."""
+    n = len(reads)
+    fq = sample_fastq(reads, n, d, "all")
+    r = reference_run(prefix, fq, opts, os.path.join(d, "ref_all.sai"), cores)
+    if "error" in r:
+        return None, r["error"]
+    cb = dict(value=n / max(r["search_s"], 1e-3), unit="reads/s", cores=cores, kind="reference",
+              sample=f"all {n} reads of the same workload, reference `galn aln --cpu-only --cpu-workers {cores}`, "
+                     f"search time from its own timing line")
+    return (cb, r), None
+
+
+def cpu_reference_sampled(prefix, reads, opts, sample, d, steps, warmup, cores):
+    """The reference arm: the reference's CPU path on a prefix of the reads grown until one run searches
+    for a few seconds (its timer has 10 ms resolution), run warmup + steps times."""
     n = min(sample, len(reads))
     while True:
-        fq = sample_fastq(n)
-        info = oracle.run_galn_ref(prefix, fq, opts, os.path.join(d, "ref_sample.sai"), workers=cores)
-        if info["rc"] not in (0, 4) or "search_s" not in info:
-            return None, "reference run failed: " + info["stderr"][-200:]
-        if info["search_s"] >= 3.0 or n >= len(reads):
+        fq = sample_fastq(reads, n, d, "sample")
+        r = reference_run(prefix, fq, opts, os.path.join(d, "ref_sample.sai"), cores)
+        if "error" in r:
+            return None, r["error"]
+        if r["search_s"] >= 3.0 or n >= len(reads):
             break
-        n = min(len(reads), int(n * min(8.0, 4.0 / max(info["search_s"], 0.05))))
+        n = min(len(reads), int(n * min(8.0, 4.0 / max(r["search_s"], 0.05))))
     vals = []
     for i in range(warmup + steps):
         if i > 0:
-            info = oracle.run_galn_ref(prefix, fq, opts, os.path.join(d, "ref_sample.sai"), workers=cores)
-            if info["rc"] not in (0, 4) or "search_s" not in info:
-                return None, "reference run failed: " + info["stderr"][-200:]
+            r = reference_run(prefix, fq, opts, os.path.join(d, "ref_sample.sai"), cores)
+            if "error" in r:
+                return None, r["error"]
         if i >= warmup:
-            vals.append(n / max(info["search_s"], 1e-3))
+            vals.append(n / max(r["search_s"], 1e-3))
     return dict(value=statistics.mean(vals), unit="reads/s", cores=cores, kind="reference",
-                sample=f"first {n} reads of the same workload, reference `galn aln --cpu-only --cpu-workers {cores}`,"
-                       f" search time from its own timing line"), None
+                sample=f"first {n} reads of the same workload per step, reference `galn aln --cpu-only "
+                       f"--cpu-workers {cores}`, search time from its own timing line"), None
 
+
+# ------------------------------------------------------------------------------------------------------------
+# --index-build
 
 def index_bench(args, rank: int, local: int) -> int:
     """--index-build: `galn index` on the workload's reference (FASTA on disk to the five bwa index files).
@@ -212,7 +257,7 @@ def index_bench(args, rank: int, local: int) -> int:
         return 0
     d = args.data_dir or os.path.join(tempfile.gettempdir(), f"galn_index_{args.workload}_{args.scale}")
     os.makedirs(d, exist_ok=True)
-    ref, _, _ = synth.workload(args.workload, args.scale, seed=1, reads_scale=0.001)
+    ref = synth.workload_reference(args.workload, args.scale, seed=1)
     fa = os.path.join(d, "ref.fa")
     if not os.path.exists(fa):
         synth.write_fasta(fa, ref)
@@ -293,11 +338,83 @@ def index_bench(args, rank: int, local: int) -> int:
     return 0
 
 
-def serving_run(ix, ref, n_requests: int, seed: int, rate_hz: float, scale: float):
+# ------------------------------------------------------------------------------------------------------------
+# sub-records of the default run
+
+def gather_sweep(device: int, ix_bytes: int) -> dict:
+    """The device's random 32-byte sector read rate over buffer sizes (from a quarter of L2 to 32x it) and
+    loads in flight per thread (galn_gather_peak_ex, best of 5 launches each)."""
+    import galn_b200
+    spans = [32 << 20, 128 << 20, 1 << 30, 2 << 30, 4 << 30]
+    table = []
+    for span in spans:
+        for inf in (2, 4, 8, 16):
+            g = galn_b200.gather_peak(device, span, inf, 5)
+            table.append({"bytes": span, "in_flight": inf, "gbs": g})
+    ix_pow2 = 1 << max(20, (ix_bytes - 1).bit_length())
+    best = lambda rows: max((r for r in rows if r["gbs"]), key=lambda r: r["gbs"], default=None)  # noqa: E731
+    hbm = best([r for r in table if r["bytes"] >= (1 << 30)])
+    l2 = best([r for r in table if r["bytes"] == (32 << 20)])
+    ixr = best([{"bytes": ix_pow2, "in_flight": inf, "gbs": galn_b200.gather_peak(device, ix_pow2, inf, 5)}
+                for inf in (4, 8, 16)])
+    return {"table": table, "hbm_best": hbm, "l2_best": l2, "index_size_best": ixr}
+
+
+def divergent_run(ix, ref, d: str, args, cores: int, prefix: str) -> dict:
+    """The high-divergence configuration on the resident aDNA index: `div_reads_scale` of its 1 M reads
+    with the persistent engine (autotuned for these options), the plain per-batch engine and the persistent
+    engine on the first `div_plain_reads` of them, and the reference's own .sai of the first
+    `div_ref_reads` against this build's."""
+    import galn_b200
+    from galn_b200 import synth
+    t = time.time()
+    n = max(1, int(synth.FULL_READS["divergent"] * args.div_reads_scale))
+    reads, opts = synth.workload_reads("divergent", ref, n, seed=1)
+    R = galn_b200.Reads(reads.ascii(), reads.off.copy())
+    log(f"[bench] divergent: {n} reads generated in {time.time() - t:.1f} s")
+    tune = ix.autotune(opts, R, max_sample=min(n, 16384))
+
+    def timed(eng, rr, k, w):
+        dev, e2e = [], []
+        res = None
+        for i in range(w + k):
+            t1 = time.perf_counter()
+            res = galn_b200.aln(ix, opts, rr, eng)
+            dt = time.perf_counter() - t1
+            if i >= w:
+                e2e.append(dt)
+                dev.append(ix.last_profile()["ms_device"] / 1e3)
+        return len(rr) / statistics.mean(dev), len(rr) / statistics.mean(e2e), res
+
+    pv, pe, pres = timed(galn_b200.GALN_ENGINE_PERSISTENT, R, 2, 1)
+    m = min(n, args.div_plain_reads)
+    Rm = galn_b200.Reads(R.seq[:int(R.offset[m])], R.offset[:m + 1].copy())
+    sv, se, sres = timed(galn_b200.GALN_ENGINE_PERSISTENT, Rm, 1, 0)
+    qv, qe, qres = timed(galn_b200.GALN_ENGINE_PLAIN, Rm, 1, 0)
+    out = {"reads": n, "reads_fraction": args.div_reads_scale, "options": " ".join(opts), "autotuned": tune,
+           "persistent": {"value": pv, "e2e": pe},
+           "same_reads": {"reads": m, "persistent": sv, "plain": qv, "ratio": sv / qv,
+                          "sai_identical": sres.sai_bytes() == qres.sai_bytes()},
+           "pops_per_read": float(pres.pops.astype("float64").mean())}
+    k = min(n, args.div_ref_reads)
+    if k > 0 and args.cpu_sample > 0:
+        fq = sample_fastq(reads, k, d, "div")
+        rr = reference_run(prefix, fq, opts, os.path.join(d, "ref_div.sai"), cores)
+        Rk = galn_b200.Reads(R.seq[:int(R.offset[k])], R.offset[:k + 1].copy())
+        mine = hashlib.md5(galn_b200.aln(ix, opts, Rk).sai_bytes()).hexdigest()
+        out["reference"] = {"reads": k, "error": rr["error"]} if "error" in rr else {
+            "reads": k, "reads_per_s": k / max(rr["search_s"], 1e-3), "cores": cores,
+            "sai_md5": rr["md5"], "sai_md5_vs_reference": rr["md5"] == mine}
+    return out
+
+
+def serving_run(ix, ref, n_requests: int, seed: int, rate_hz: float, scale: float, d: str, prefix: str,
+                check_reference: bool, cores: int):
     """The serving configuration on the resident index: Poisson arrivals, requests of 1k-500k reads
     (log-uniform, times `scale`), lengths 36-150 bp, half default and half aDNA options. Returns reads/s and
     submit-to-result latency percentiles, next to the same requests as plain per-request launches in
-    arrival order (one at a time), and whether every request's .sai is the same both ways."""
+    arrival order (one at a time), whether every request's .sai is the same both ways, and (check_reference)
+    whether every request's .sai equals the reference's own run of that request."""
     import numpy as np
 
     import galn_b200
@@ -332,14 +449,70 @@ def serving_run(ix, ref, n_requests: int, seed: int, rate_hz: float, scale: floa
         t_free = start + sv
         lat.append(t_free - t_arr)
     lat = np.array(lat) * 1e3
-    return {"requests": len(items), "reads": total, "arrival_rate_hz": rate_hz,
-            "reads_per_s": total / max(t_end - t_sub[0], 1e-9), "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "steps": st["steps"], "device_busy_s": st["busy_ms"] / 1e3,
-            "plain_per_request": {"reads_per_s": total / sum(service), "p50_ms": float(np.percentile(lat, 50)),
-                                  "p99_ms": float(np.percentile(lat, 99)),
-                                  "latency": "FIFO queue of one-at-a-time launches with the same arrivals"},
-            "sai_identical_served_vs_plain": bool(same)}
+    out = {"requests": len(items), "reads": total, "arrival_rate_hz": rate_hz,
+           "reads_per_s": total / max(t_end - t_sub[0], 1e-9), "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+           "steps": st["steps"], "device_busy_s": st["busy_ms"] / 1e3,
+           "plain_per_request": {"reads_per_s": total / sum(service), "p50_ms": float(np.percentile(lat, 50)),
+                                 "p99_ms": float(np.percentile(lat, 99)),
+                                 "latency": "FIFO queue of one-at-a-time launches with the same arrivals"},
+           "sai_identical_served_vs_plain": bool(same)}
+    if check_reference:
+        t = time.time()
+        ok, checked, errs = True, 0, []
+        for i, (req, o) in enumerate(zip(reqs, outs)):
+            fq = os.path.join(d, f"serve_req{i}.fq")
+            if not os.path.exists(fq):
+                synth.write_fastq(fq + ".part", req["reads"])
+                os.replace(fq + ".part", fq)
+            rr = reference_run(prefix, fq, req["opts"], os.path.join(d, f"serve_req{i}.sai"), cores)
+            if "error" in rr:
+                errs.append(rr["error"])
+                continue
+            checked += 1
+            ok = ok and rr["md5"] == hashlib.md5(o.sai_bytes()).hexdigest()
+        out["sai_md5_vs_reference"] = {"requests_checked": checked, "all_identical": bool(ok and checked == len(reqs)),
+                                       "errors": errs[:3], "seconds": round(time.time() - t, 1)}
+    return out
 
+
+def profile_warp_steady(args, local: int) -> int:
+    """--profile-case warp_steady: the warp tier in its steady state, for ncu captures. From the aDNA workload
+    (100 Mbp reference, 2,000,000 reads, -l 1024 -n 0.01 -o 2) it takes the first 60,000 reads that the first
+    tier hands to the warp tier and that need 2,000-50,000 pops: no read long enough to run alone at the end of
+    the launch, so counters describe the kernel while all warps are busy. They are searched as one bwa batch
+    with -m 100000 (none of them comes near that cut-off, so their results are those of the full workload)
+    and a 1024-chunk arena per warp (64 Ki entries), which keeps the device footprint near 4 GB. The search
+    runs twice: the second launch of warp_kernel is the one to capture (ncu -k regex:warp_kernel -s 1 -c 1).
+    Each run prints its tier times."""
+    import numpy as np
+
+    import galn_b200
+    d, prefix, ref, reads, opts = prepare("adna", 1.0, 0, local, args.data_dir, None)
+    full = galn_b200.Reads(reads.ascii(), reads.off.copy())
+    ix = galn_b200.Index(prefix, device=local)
+    ix.set_trace(False)
+    sel_path = os.path.join(d, "warp_steady_reads.npy")
+    if not os.path.exists(sel_path):
+        ix.set_tuning(t0_cap=1024, keep_stats=True)
+        r = galn_b200.aln(ix, opts, full)
+        prof = ix.last_profile(len(full))
+        sel = np.nonzero((prof["tier"] == 1) & (r.pops >= 2000) & (r.pops <= 50000))[0][:60000]
+        np.save(sel_path, sel)
+    sel = np.load(sel_path)
+    sub = galn_b200.Reads.from_strings([bytes(full.seq[full.offset[i]:full.offset[i + 1]]) for i in sel])
+    sub.batch = np.zeros(len(sel), np.int32)
+    ix.set_tuning(t0_cap=1024, keep_stats=False)
+    ix.set_warp_tier(True, 1024)
+    a = list(opts) + ["-m", "100000"]
+    for _ in range(2):
+        r = galn_b200.aln(ix, a, sub)
+        p = ix.last_profile()
+        print(json.dumps(dict(case="warp_steady", reads=len(sub), ms_tier=[round(x, 3) for x in p["ms_tier"][:2]],
+                              pops=int(r.pops.sum()))), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------------------
 
 def main():
     ap = argparse.ArgumentParser()
@@ -352,36 +525,54 @@ def main():
     ap.add_argument("--reads-scale", type=float, default=None, help="reads at this fraction of the workload's")
     ap.add_argument("--engine", default="persistent", choices=["persistent", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-engine comparison")
-    ap.add_argument("--cpu-sample", type=int, default=200_000)
+    ap.add_argument("--cpu-sample", type=int, default=200_000,
+                    help="first reads of the reference arm's sample (0: no reference runs in the GPU arm)")
     ap.add_argument("--data-dir", default=None)
     ap.add_argument("--trace", action="store_true", help="compute per-read trace hashes (verification mode)")
     ap.add_argument("--t0-cap", type=int, default=1024, help="first-tier stack entries per thread")
     ap.add_argument("--warp-arena", type=int, default=8192, help="warp-tier stack chunks (64 entries) per warp")
     ap.add_argument("--serve-requests", type=int, default=40, help="requests in the serving run (0: none)")
+    ap.add_argument("--no-serve-reference", dest="serve_reference", action="store_false",
+                    help="skip the reference runs of the served requests")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--autotune-sample", type=int, default=262144)
     ap.add_argument("--serve-rate", type=float, default=16.0, help="request arrival rate (per second)")
+    ap.add_argument("--div-reads-scale", type=float, default=0.1,
+                    help="fraction of the high-divergence configuration's 1 M reads (0: skip it)")
+    ap.add_argument("--div-plain-reads", type=int, default=20_000,
+                    help="high-divergence reads timed with both engines")
+    ap.add_argument("--div-ref-reads", type=int, default=3_000,
+                    help="high-divergence reads compared with the reference's .sai")
+    ap.add_argument("--no-gather-sweep", dest="gather_sweep", action="store_false")
     ap.add_argument("--index-build", action="store_true", help="time `galn index` on the workload's reference")
+    ap.add_argument("--profile-case", choices=["warp_steady"], default=None)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    cores = os.cpu_count() or 1
 
     if args.index_build:
         return index_bench(args, rank, local)
+    if args.profile_case:
+        return profile_warp_steady(args, local)
     if args.impl == "reference":
         if rank != 0:
             return 0
         d, prefix, ref, reads, opts = prepare(args.workload, args.scale, 0, local, args.data_dir, args.reads_scale,
                                               reference_builder=True)
-        cb, why = cpu_reference(prefix, reads, opts, args.cpu_sample, d, steps=args.steps, warmup=args.warmup)
+        cb, why = cpu_reference_sampled(prefix, reads, opts, args.cpu_sample, d, args.steps, args.warmup, cores)
         if cb is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return 0
+        n = len(reads)
         line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "reads/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * min(args.cpu_sample, len(reads)) / cb["value"],
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * n / cb["value"],
+                "ms_per_step_how": f"the {n} reads of one step of the GPU arm at the sample's rate",
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-                "data": "synthetic (seeded)", "config": {"workload": WORKLOAD_DESC[args.workload], "scale": args.scale},
+                "data": "synthetic: seeded reference and reads with the workload's shapes (no public dataset here)",
+                "config": workload_config(args, args.gpus, n, opts),
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "reads/s", "h2d_bytes_per_step": 0,
                                             "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -421,6 +612,7 @@ def main():
     def run_steps(eng, k, w, keep_tiers=False):
         md5 = set()
         e2e, dev, tier0, launches = [], [], [], 0
+        res = None
         for i in range(w + k):
             flush.fill_(i & 255)
             torch.cuda.synchronize()
@@ -464,7 +656,6 @@ def main():
 
     e2e_s = max_over_ranks(statistics.mean(e2e))
     dev_s = max_over_ranks(statistics.mean(dev))
-    t0_s = statistics.mean(tier0)
     total_reads = n * world
 
     # roofline of the dominant kernel: algorithmic block fetches of the reads the first tier finished
@@ -478,6 +669,7 @@ def main():
                   "threads": prof["tier_threads"],
                   "fetches_finished": [int(prof["fetch"][prof["tier"] == t].astype(np.int64).sum()) for t in range(8)]}
     tiers_info["warp_counters"] = ix.warp_counters()
+    tiers_info["warp_queue"] = ix.last_warp_queue()
     fetch_all = int(prof["fetch"].astype(np.int64).sum())
     ix.set_tuning(t0_cap=args.t0_cap, keep_stats=False)
     peak, peak_kind = peaks()
@@ -488,32 +680,32 @@ def main():
     dom_s = tier_ms[dom] / 1e3
     fetch_dom = tiers_info["fetches_finished"][dom]
     achieved = 32.0 * fetch_dom / dom_s / 1e9
-    def gather_peak(nbytes):
-        g = ctypes.c_double(0)
-        rc_ = galn_b200.lib().galn_gather_peak(local, ctypes.c_uint64(nbytes), 5, ctypes.byref(g))
-        return g.value if rc_ == 0 else None
-    gather_gbs = gather_peak(4 << 30)          # HBM: a buffer 32x the L2
-    gather_l2_gbs = gather_peak(32 << 20)      # L2: a buffer a quarter of it
     ix_bytes = os.path.getsize(prefix + ".bwt")   # the occ64 index has the .bwt body's size
-    ix_pow2 = 1 << max(20, (ix_bytes - 1).bit_length())
-    gather_ix_gbs = gather_peak(ix_pow2)       # a buffer of the index's size (next power of two)
+    sweep = gather_sweep(local, ix_bytes) if args.gather_sweep else None
     traffic, traffic_how = scaled_traffic(dom, args.workload, tiers_info)
 
     plain = None
     if not args.no_plain and engine != galn_b200.GALN_ENGINE_PLAIN:
-        pe2e, pdev, _, _, pmd5, _ = run_steps(galn_b200.GALN_ENGINE_PLAIN, max(1, args.steps // 2), 1)
+        pe2e, pdev, _, _, pmd5, _ = run_steps(galn_b200.GALN_ENGINE_PLAIN, min(3, max(1, args.steps // 2)), 1)
         plain = {"value": total_reads / max_over_ranks(statistics.mean(pdev)),
                  "e2e": total_reads / max_over_ranks(statistics.mean(pe2e)), "sai_md5_same": pmd5 == md5}
 
+    divergent = None
+    if args.workload == "adna" and args.div_reads_scale > 0 and rank == 0 and world == 1:
+        divergent = divergent_run(ix, ref, d, args, cores, prefix)
+
     serving = None
     if args.serve_requests > 0 and args.workload == "adna":
-        serving = serving_run(ix, ref, args.serve_requests, 1000 + rank, args.serve_rate, args.scale)
+        serving = serving_run(ix, ref, args.serve_requests, 1000 + rank, args.serve_rate, args.scale, d, prefix,
+                              args.serve_reference and args.cpu_sample > 0 and world == 1, cores)
 
-    cpu = None
+    cpu, ref_full = None, None
     if rank == 0 and world == 1 and args.cpu_sample > 0:
-        cpu, why = cpu_reference(prefix, reads, opts, args.cpu_sample, d)
-        if cpu is None:
+        got, why = cpu_reference_full(prefix, reads, opts, d, cores)
+        if got is None:
             log("[bench] cpu baseline unavailable:", why)
+        else:
+            cpu, ref_full = got
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -521,31 +713,33 @@ def main():
         return 0
     h2d = int(len(reads.seq) + 8 * (n + 1))
     d2h = int(4 * n + 8 * (n + 1) + 16 * n + 24 * int(res.rec_offset[-1]))
+    hbm_g = sweep["hbm_best"] if sweep else None
+    l2_g = sweep["l2_best"] if sweep else None
+    ix_g = sweep["index_size_best"] if sweep else None
+    frac_of = lambda g: achieved / g["gbs"] if g and g.get("gbs") else None  # noqa: E731
     line = {
         "metric": METRIC, "value": total_reads / dev_s, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * e2e_s, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int64",
         "data": "synthetic: seeded reference and reads with the workload's shapes (no public dataset here)",
-        "config": {"workload": WORKLOAD_DESC[args.workload], "scale": args.scale, "reads_scale": args.reads_scale,
-                   "reads_per_gpu": n,
-                   "options": " ".join(opts), "engine": args.engine, "trace_hashes": bool(args.trace),
-                   "autotuned": tune,
-                   "l2": "flushed before every step (512 MB device write, outside the timed region)",
-                   "parallelism": f"{world} independent GPU shards (reads split, index replicated)"},
+        "config": workload_config(args, world, n, opts),
+        "search": {"engine": args.engine, "trace_hashes": bool(args.trace), "autotuned": tune},
         "e2e": {"value": total_reads / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_how": traffic_how, "peak_kind": peak_kind,
                      "kernel": TIER_NAMES[min(dom, 2)],
                      "algorithmic_bytes_per_launch": 32 * fetch_dom, "fetches_all_tiers": fetch_all,
                      "ms_per_launch": 1e3 * dom_s,
-                     "gather_peak_gbs": gather_gbs,
-                     "frac_of_gather_peak": achieved / gather_gbs if gather_gbs else None,
-                     "gather_l2_peak_gbs": gather_l2_gbs,
-                     "frac_of_gather_l2_peak": achieved / gather_l2_gbs if gather_l2_gbs else None,
-                     "gather_index_size_peak_gbs": gather_ix_gbs, "gather_index_size_bytes": ix_pow2,
-                     "frac_of_gather_index_size_peak": achieved / gather_ix_gbs if gather_ix_gbs else None,
-                     "gather_peak_how": "galn_gather_peak: random 32-B sectors of a 4 GiB buffer (HBM), a 32 MiB "
-                                        "buffer (L2) and a buffer of the index's size, best of 5 launches each"},
+                     "gather_peak_gbs": hbm_g["gbs"] if hbm_g else None,
+                     "frac_of_gather_peak": frac_of(hbm_g),
+                     "gather_l2_peak_gbs": l2_g["gbs"] if l2_g else None,
+                     "frac_of_gather_l2_peak": frac_of(l2_g),
+                     "gather_index_size_peak_gbs": ix_g["gbs"] if ix_g else None,
+                     "frac_of_gather_index_size_peak": frac_of(ix_g),
+                     "gather_peak_how": "galn_gather_peak_ex: random 32-B sectors, best over buffers of 1-4 GiB "
+                                        "(HBM), of 32 MiB (L2) and of the index's size (next power of two), each "
+                                        "over 2-16 sectors in flight per thread, best of 5 launches",
+                     "gather_sweep": sweep["table"] if sweep else None},
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
@@ -554,8 +748,14 @@ def main():
         "ms_device_per_step": 1e3 * dev_s,
         "tiers": tiers_info,
     }
+    if ref_full:
+        line["sai_md5_reference"] = ref_full["md5"]
+        line["sai_md5_vs_reference"] = len(md5) == 1 and ref_full["md5"] in md5
+        line["sai_md5_vs_reference_reads"] = n
     if plain:
         line["plain_engine"] = plain
+    if divergent:
+        line["divergent"] = divergent
     if serving:
         line["serving"] = serving
     print(json.dumps(line))

@@ -13,5 +13,6 @@ There is no CPU fallback: if the library is missing or no sm_100 device is prese
 from __future__ import annotations
 
 from .api import (GALN_ENGINE_PERSISTENT, GALN_ENGINE_PLAIN, GalnError, Index, Options, Reads, Results,  # noqa: F401
-                  Server, aln, cal_maxdiff, fasta_to_pac, index_fasta, index_text, lib, lib_path, parse_options, read_fastq,
+                  Server, aln, cal_maxdiff, fasta_to_pac, gather_peak, index_fasta, index_text, lib, lib_path, parse_options,
+                  read_fastq,
                   read_fastq_batches, write_sai)

@@ -110,6 +110,11 @@ def lib():
     L.galn_index_build_text.argtypes = [vp, C.c_uint64, C.c_char_p, C.c_int, C.POINTER(BuildStats)]
     L.galn_index_build_fasta.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(BuildStats)]
     L.galn_fasta_to_pac.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_uint64)]
+    L.galn_gather_peak.argtypes = [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_double)]
+    L.galn_index_set_warp_wait.argtypes = [vp, C.c_int64]
+    L.galn_index_occ.argtypes = [vp, C.c_int, vp, C.c_int64, vp, vp]
+    L.galn_last_warp_queue.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
+    L.galn_gather_peak_ex.argtypes = [C.c_int, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.galn_version.restype = C.c_char_p
     _lib = L
     return L
@@ -138,9 +143,13 @@ def cal_maxdiff(length: int, err: float, thres: float) -> int:
 class Index:
     """<prefix>.bwt resident on one GPU in the device occurrence layout."""
 
-    def __init__(self, prefix: str | None = None, device: int = 0, bwt_bytes: bytes | None = None):
+    def __init__(self, prefix: str | None = None, device: int = 0, bwt_bytes: bytes | np.ndarray | None = None):
+        """<prefix>.bwt, or a .bwt file's image in memory (bytes, or a numpy array used without a copy)."""
         err = C.c_int(0)
-        if bwt_bytes is not None:
+        if isinstance(bwt_bytes, np.ndarray):
+            a = np.ascontiguousarray(bwt_bytes)
+            self.h = lib().galn_index_open_mem(a.ctypes.data, a.nbytes, device, C.byref(err))
+        elif bwt_bytes is not None:
             buf = C.create_string_buffer(bwt_bytes, len(bwt_bytes))
             self.h = lib().galn_index_open_mem(buf, len(bwt_bytes), device, C.byref(err))
         else:
@@ -168,6 +177,17 @@ class Index:
         if lib().galn_index_set_warp_tier(self.h, int(on), arena_chunks):
             raise GalnError("bad warp tier setting")
 
+    def set_warp_wait(self, wait_ns: int):
+        """How long a big-arena warp waits for queued reads (galn_index_set_warp_wait; default 2 s)."""
+        if lib().galn_index_set_warp_wait(self.h, int(wait_ns)):
+            raise GalnError("bad warp wait")
+
+    def last_warp_queue(self) -> dict:
+        """Reads the last run's warp tier queued for its big-arena warps, and whether a wait ran out."""
+        q, g = C.c_int64(), C.c_int()
+        lib().galn_last_warp_queue(self.h, C.byref(q), C.byref(g))
+        return dict(queued=q.value, gave_up=bool(g.value))
+
     def load_sa(self, prefix: str):
         """Put <prefix>.sa (the suffix-array samples of this index) on the device for positions."""
         rc = lib().galn_index_load_sa(self.h, prefix.encode())
@@ -193,6 +213,20 @@ class Index:
         if rc:
             raise GalnError(f"galn_sa2pos failed ({rc})")
         return pos[:len(k)], strand[:len(k)]
+
+    def occ(self, rows, layout: int = 64) -> np.ndarray:
+        """Occ of the four bases at each BWT row (galn_index_occ): an (n, 4) uint64 array."""
+        k = np.ascontiguousarray(rows, np.uint64)
+        out = np.zeros((max(1, len(k)), 4), np.uint64)
+        rc = lib().galn_index_occ(self.h, layout, k.ctypes.data, len(k), out.ctypes.data, None)
+        if rc:
+            raise GalnError(f"galn_index_occ failed ({rc})")
+        return out[:len(k)]
+
+    def info(self) -> dict:
+        n, p, b = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        lib().galn_index_info(self.h, C.byref(n), C.byref(p), C.byref(b))
+        return dict(seq_len=n.value, primary=p.value, device_bytes=b.value)
 
     def set_l2_persist(self, on: bool):
         """Keep the occurrence blocks in a persisting L2 window (on by default)."""
@@ -435,6 +469,13 @@ def aln(index: Index, args: list[str] | Options, reads: Reads | str,
 
 def write_sai(path: str, res: Results) -> int:
     return res.write_sai(path)
+
+
+def gather_peak(device: int, nbytes: int, in_flight: int = 8, repeats: int = 5) -> float | None:
+    """Random 32-byte sector read rate (GB/s) over a buffer of nbytes (galn_gather_peak_ex), or None."""
+    g = C.c_double(0)
+    rc = lib().galn_gather_peak_ex(device, nbytes, in_flight, repeats, C.byref(g))
+    return g.value if rc == 0 else None
 
 
 def _stats_dict(st: BuildStats) -> dict:

@@ -433,6 +433,7 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
             wc.n_warps = std::min(ne, res_w);
             wc.arena_chunks = ix->warp_arena;
             wc.big_chunks = big_chunks;
+            wc.q_wait_ns = ix->warp_wait_ns;
             if (pass == 0) {
                 wc.n_big = std::min(kBigWarps, wc.n_warps / 8);
                 if (big_chunks <= wc.arena_chunks) wc.n_big = 0;
@@ -491,6 +492,11 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
             if (got || n_q) ECK(cudaStreamSynchronize(st));
             for (int32_t r : wov)
                 if (r < 0 || r >= n) return GALN_ECUDA;   // a slot written by no warp
+            if (q_lost) {   // every queued read again: one may also be in the overflow list
+                std::sort(wov.begin(), wov.end());
+                wov.erase(std::unique(wov.begin(), wov.end()), wov.end());
+            }
+            if (pass == 0) { S.warp_queued = q_tail; S.warp_gave_up = q_lost ? 1 : 0; }
             if (pass == 1) S.overflow_reads[1] = (int64_t)wov.size();
             elig.swap(wov);
         }
@@ -720,6 +726,23 @@ extern "C" int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks
     std::lock_guard<std::mutex> lk(ix->mu);
     ix->use_warp = on != 0;
     ix->warp_arena = arena_chunks;
+    return 0;
+}
+
+extern "C" int galn_index_set_warp_wait(galn_index *ix, int64_t wait_ns)
+{
+    if (!ix || wait_ns < 0) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    ix->warp_wait_ns = (uint64_t)wait_ns;
+    return 0;
+}
+
+extern "C" int galn_last_warp_queue(galn_index *ix, int64_t *queued, int *gave_up)
+{
+    if (!ix) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    if (queued) *queued = ix->main.last.warp_queued;
+    if (gave_up) *gave_up = ix->main.last.warp_gave_up;
     return 0;
 }
 

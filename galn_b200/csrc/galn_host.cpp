@@ -594,6 +594,31 @@ extern "C" int galn_sa2pos(galn_index *ix, const uint64_t *rows, const int32_t *
     return sa_query(ix, rows, ref_len, n, pos, strand);
 }
 
+extern "C" int galn_index_occ(galn_index *ix, int layout, const uint64_t *rows, int64_t n, uint64_t *occ, uint32_t *fetch)
+{
+    if (!ix || n < 0 || (layout != 64 && layout != 80) || (n > 0 && (!rows || !occ))) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    if (n == 0) return 0;
+    for (int64_t i = 0; i < n; ++i)
+        if (rows[i] != ~0ull && rows[i] > ix->dev.seq_len) return GALN_EINVAL;
+    if (cudaSetDevice(ix->dev.device) != cudaSuccess) return GALN_ECUDA;
+    const size_t nn = (size_t)n;
+    void *d = nullptr;
+    const size_t o_occ = (nn * 8 + 255) & ~(size_t)255, o_f = o_occ + nn * 32;
+    if (cudaMalloc(&d, o_f + nn * 4) != cudaSuccess) { cudaGetLastError(); return GALN_ENOMEM; }
+    cudaStream_t st = ix->stream;
+    char *b = (char *)d;
+    int rc = 0;
+    if (cudaMemcpyAsync(b, rows, nn * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) rc = GALN_ECUDA;
+    if (!rc) rc = galn::dev_occ_probe(ix->dev, layout, (const uint64_t *)b, n, (uint64_t *)(b + o_occ),
+                                      (uint32_t *)(b + o_f), st);
+    if (!rc && cudaMemcpyAsync(occ, b + o_occ, nn * 32, cudaMemcpyDeviceToHost, st) != cudaSuccess) rc = GALN_ECUDA;
+    if (!rc && fetch && cudaMemcpyAsync(fetch, b + o_f, nn * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) rc = GALN_ECUDA;
+    if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = GALN_ECUDA;
+    cudaFree(d);
+    return rc;
+}
+
 extern "C" int galn_index_info(const galn_index *ix, uint64_t *seq_len, uint64_t *primary, uint64_t *device_bytes)
 {
     if (!ix) return GALN_EINVAL;

@@ -67,6 +67,8 @@ struct RunStats {
     int64_t kernel_launches = 0;
     int64_t graph_launches = 0;      // of those, launched through a CUDA graph
     uint64_t warp_dbg[16] = {};      // warp-tier counters (keep_stats runs)
+    int64_t warp_queued = 0;         // reads the warp tier's first pass queued for its big-arena warps
+    int warp_gave_up = 0;            // a big warp's bounded wait ran out in the first pass
     std::vector<uint32_t> fetch;     // per read, of the last run
     std::vector<int8_t> tier_of;     // per read, of the last run
 };
@@ -108,6 +110,7 @@ struct galn_index {
     bool tune_active = false;           // the autotuner is timing a candidate: ignore the table
     bool use_graph = true;              // launch the persistent first tier through a CUDA graph
     int warp_arena = 1 << 13;           // chunks (kWarpChunk entries) per warp
+    uint64_t warp_wait_ns = 2000000000ull;   // a big warp's bounded wait for queued work
     bool l2_persist = true;             // the occurrence blocks in a persisting L2 window
     // suffix-array samples (<prefix>.sa) for positions; sample 0 is the $ row (-1)
     galn::Buf sa_samples, sa_k, sa_len, sa_pos, sa_strand;

@@ -102,6 +102,7 @@ constexpr int kWarpMaxLen = 256, kWarpMaxStacks = 256;
 constexpr int kWarpChunk = 64;        // stack entries per chunk of a warp's arena
 struct WarpCfg {
     int n_warps = 0, arena_chunks = 0, aln_cap = 0, n_big = 0, big_chunks = 0;
+    unsigned long long q_wait_ns = 2000000000ull;   // how long a big warp waits for queued work
 };
 size_t warp_smem_bytes();
 int warp_resident(int device);
@@ -113,6 +114,9 @@ int dev_search_warp(const DevIndex &ix, DevJob &job, const WarpCfg &c, int tier,
 // d_ref_len: position and strand, ~0 for a hit across the forward/reverse boundary)
 int dev_sa_walk(const DevIndex &ix, const uint64_t *d_samples, uint64_t intv, const uint64_t *d_k, int64_t n,
                 const int32_t *d_ref_len, uint64_t *d_pos, int8_t *d_strand, cudaStream_t st);
+// Occ(c, row) of the four bases at n BWT rows (occ: 4 per row) in layout `occ`, and the blocks read per row
+int dev_occ_probe(const DevIndex &ix, int occ, const uint64_t *d_rows, int64_t n, uint64_t *d_occ, uint32_t *d_fetch,
+                  cudaStream_t st);
 // Results in read order: rec_off[0..n] (exclusive scan of max(out_n, 0)) and the records gathered from
 // out_rec into rec_ord; tile_sum holds order_tile_bytes(n) bytes of scratch. Three kernels on st.
 int dev_order_results(const DevJob &job, int n, int64_t *rec_off, uint64_t *rec_ord, int64_t *tile_sum, cudaStream_t st);

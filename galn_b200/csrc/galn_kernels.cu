@@ -491,10 +491,39 @@ int dev_sa_walk(const DevIndex &ix, const uint64_t *d_samples, uint64_t intv, co
     return 0;
 }
 
+// ---- the occurrence layer on its own: Occ of the four bases at BWT rows, for checks ----
+template <int S>
+__global__ void occ_probe_kernel(IndexView ix, const uint64_t *__restrict__ rows, int64_t n, uint64_t *__restrict__ occ,
+                                 uint32_t *__restrict__ fetch)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    uint64_t ok[4], ol[4];
+    uint32_t f = 0;
+    occ4_pair_u<S>(ix, rows[t], rows[t], ok, ol, f);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) occ[4 * t + c] = ok[c];
+    if (fetch) fetch[t] = f;
+}
+
+int dev_occ_probe(const DevIndex &ix, int occ, const uint64_t *d_rows, int64_t n, uint64_t *d_occ, uint32_t *d_fetch,
+                  cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    IndexView v;
+    if (index_view(ix, occ, v)) return -20;
+    const unsigned grid = (unsigned)((n + 255) / 256);
+    if (occ == kOcc80) occ_probe_kernel<kOcc80><<<grid, 256, 0, st>>>(v, d_rows, n, d_occ, d_fetch);
+    else occ_probe_kernel<kOcc64><<<grid, 256, 0, st>>>(v, d_rows, n, d_occ, d_fetch);
+    GALN_CUDA(cudaGetLastError());
+    return 0;
+}
+
 // ---- random 32-byte gather peak (a measurement, not part of the search) ----
 // Every thread reads `per_thread` 32-byte sectors at pseudo-random sector indices of a power-of-two buffer
-// (a splitmix64 sequence per thread; independent loads, several in flight), and folds them into one word so
-// the loads are not dead. Bytes read / time is the device's random-sector read rate for that buffer size.
+// (a splitmix64 sequence per thread; IF independent sectors in flight per thread, each read as the search
+// reads an index block: two 16-byte loads), and folds them into one word so the loads are not dead. Bytes
+// read / time is the device's random-sector read rate for that buffer size and depth of loads in flight.
 __device__ __forceinline__ uint64_t mix64(uint64_t z)
 {
     z += 0x9e3779b97f4a7c15ull;
@@ -503,28 +532,29 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z)
     return z ^ (z >> 31);
 }
 
+template <int IF>
 __global__ void __launch_bounds__(256) gather_kernel(const uint4 *buf, uint64_t sector_mask, int per_thread, uint32_t *sink)
 {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t acc = 0;
-    constexpr int kInFlight = 8;
-    for (int i = 0; i < per_thread; i += kInFlight) {
-        uint4 a[kInFlight], b[kInFlight];
+    for (int i = 0; i < per_thread; i += IF) {
+        uint4 a[IF], b[IF];
 #pragma unroll
-        for (int u = 0; u < kInFlight; ++u) {
+        for (int u = 0; u < IF; ++u) {
             const uint64_t sct = mix64(tid * 0x100000001b3ull + (uint64_t)(i + u)) & sector_mask;
             a[u] = __ldcg(buf + 2 * sct);
             b[u] = __ldcg(buf + 2 * sct + 1);
         }
 #pragma unroll
-        for (int u = 0; u < kInFlight; ++u) acc ^= a[u].x ^ a[u].w ^ b[u].y ^ b[u].z;
+        for (int u = 0; u < IF; ++u) acc ^= a[u].x ^ a[u].w ^ b[u].y ^ b[u].z;
     }
     if (acc == 0x9e3779b9u) sink[0] = acc;   // practically never; keeps the loads
 }
 
-extern "C" int galn_gather_peak(int device, uint64_t bytes, int repeats, double *gbs)
+extern "C" int galn_gather_peak_ex(int device, uint64_t bytes, int in_flight, int repeats, double *gbs)
 {
     if (!gbs || bytes < (1u << 20) || repeats < 1) return -20;
+    if (in_flight != 2 && in_flight != 4 && in_flight != 8 && in_flight != 16) return -20;
     while (bytes & (bytes - 1)) bytes &= bytes - 1;      // the largest power of two not above it
     if (cudaSetDevice(device) != cudaSuccess) return -22;
     void *buf = nullptr, *sink = nullptr;
@@ -535,14 +565,24 @@ extern "C" int galn_gather_peak(int device, uint64_t bytes, int repeats, double 
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const int blocks = sms * 8, per_thread = 256;
     const uint64_t sector_mask = bytes / 32 - 1;
+    auto launch = [&]() {
+        const uint4 *b = (const uint4 *)buf;
+        uint32_t *k = (uint32_t *)sink;
+        switch (in_flight) {
+        case 2: gather_kernel<2><<<blocks, 256>>>(b, sector_mask, per_thread, k); break;
+        case 4: gather_kernel<4><<<blocks, 256>>>(b, sector_mask, per_thread, k); break;
+        case 8: gather_kernel<8><<<blocks, 256>>>(b, sector_mask, per_thread, k); break;
+        default: gather_kernel<16><<<blocks, 256>>>(b, sector_mask, per_thread, k); break;
+        }
+    };
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    gather_kernel<<<blocks, 256>>>((const uint4 *)buf, sector_mask, per_thread, (uint32_t *)sink);   // warm-up
+    launch();   // warm-up
     double best = 0;
     for (int r = 0; r < repeats; ++r) {
         cudaEventRecord(e0);
-        gather_kernel<<<blocks, 256>>>((const uint4 *)buf, sector_mask, per_thread, (uint32_t *)sink);
+        launch();
         cudaEventRecord(e1);
         cudaEventSynchronize(e1);
         float ms = 0;
@@ -558,6 +598,11 @@ extern "C" int galn_gather_peak(int device, uint64_t bytes, int repeats, double 
     if (ce != cudaSuccess) return -22;
     *gbs = best;
     return 0;
+}
+
+extern "C" int galn_gather_peak(int device, uint64_t bytes, int repeats, double *gbs)
+{
+    return galn_gather_peak_ex(device, bytes, 8, repeats, gbs);
 }
 
 // ---- results in read order ----
@@ -719,7 +764,7 @@ int dev_search_warp(const DevIndex &ix, DevJob &job, const WarpCfg &c, int tier,
     a.side = (WSide *)(base + L.side);
     a.q_ctl = (int32_t *)(base + L.q_ctl);
     a.ovq = (int32_t *)(base + L.ovq);
-    a.n_big = c.n_big; a.big_chunks = c.big_chunks;
+    a.n_big = c.n_big; a.big_chunks = c.big_chunks; a.q_wait_ns = c.q_wait_ns;
     GALN_CUDA(cudaMemsetAsync(a.q_ctl, 0, 16, st));
     GALN_CUDA(cudaMemsetAsync(a.ovq, 0xff, (size_t)n * 4, st));
     const int arena_chunks = c.arena_chunks, aln_cap = c.aln_cap, n_warps = c.n_warps;

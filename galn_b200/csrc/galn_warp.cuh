@@ -122,6 +122,7 @@ struct WArgs {
     int n_big, big_chunks;
     int32_t *ovq;
     int32_t *q_ctl;
+    uint64_t q_wait_ns;       // a big warp gives up waiting for queued work after this long
     unsigned long long *dbg;  // optional counters (kWDbg entries), or NULL
 };
 
@@ -915,17 +916,20 @@ __device__ __forceinline__ uint64_t gtimer_ns()
 }
 
 // A big warp's next read (lane 0): a queued one first, else one from the list; -1 when the list is done, every
-// small warp has finished and the queue is empty, or after kQWaitNs of waiting (the reads still queued then
-// go to the next pass; if the wait was for a claimed slot, q_ctl[3] is set and the host re-runs every queued
-// read).
-constexpr uint64_t kQWaitNs = 2000000000ull;
+// small warp has finished and the queue is empty, or after a.q_wait_ns of waiting: the reads still queued
+// then go to the next pass. If the wait was for a claimed slot whose read id had not arrived, q_ctl[3] is set
+// and the host re-runs every read that was ever queued (a read a big warp finished is searched again with the
+// same result). A wait of 0 sets q_ctl[3] whenever it gives up, so that path can be exercised on purpose.
 __device__ __noinline__ int big_next(const WArgs &a)
 {
     volatile int32_t *qc = a.q_ctl;
     const int n_small = a.n_warps - a.n_big;
     const uint64_t t0 = gtimer_ns();
     for (;;) {
-        if (gtimer_ns() - t0 > kQWaitNs) return -1;    // the reads left in the queue go to the next pass
+        if (gtimer_ns() - t0 > a.q_wait_ns) {
+            if (a.q_wait_ns == 0) atomicExch(a.q_ctl + 3, 1);
+            return -1;
+        }
         const int h = qc[0], t = qc[1];
         if (h < t) {
             if (atomicCAS(a.q_ctl, h, h + 1) == h) {
@@ -933,7 +937,7 @@ __device__ __noinline__ int big_next(const WArgs &a)
                 for (;;) {
                     const int r = atomicAdd(a.ovq + h, 0);
                     if (r >= 0) { __threadfence(); return r; }
-                    if (gtimer_ns() - t0 > kQWaitNs) { atomicExch(a.q_ctl + 3, 1); return -1; }
+                    if (gtimer_ns() - t0 > a.q_wait_ns) { atomicExch(a.q_ctl + 3, 1); return -1; }
                     __nanosleep(100);
                 }
             }

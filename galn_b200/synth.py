@@ -301,31 +301,45 @@ def write_fastq(path: str, reads: Reads) -> None:
 # ---------------------------------------------------------------------------------------------
 # the named workloads
 
+FULL_READS = {"plain_small": 20_000, "adna": 2_000_000, "divergent": 1_000_000, "genome": 10_000_000}
+
+
+def workload_reference(name: str, scale: float = 1.0, seed: int = 1) -> Reference:
+    """The reference of a named workload at `scale` of its full size (divergent shares adna's)."""
+    if name == "plain_small":
+        return reference_uniform(max(10_000, int(1_000_000 * scale)), seed)
+    if name in ("adna", "divergent"):
+        return reference_adna(max(20_000, int(100_000_000 * scale)), seed)
+    if name == "genome":
+        return reference_genome(max(200_000, int(3_100_000_000 * scale)), seed)
+    raise KeyError(name)
+
+
+def workload_reads(name: str, ref: Reference, n: int, seed: int = 1) -> tuple[Reads, list[str]]:
+    """n reads of a named workload drawn from `ref` (the reads workload() returns for the same seed), and
+    the workload's aln options."""
+    if name == "plain_small":
+        return (simulate_reads(ref, n, seed + 1, 100, sub_rate=0.01, indel_rate=0.001, random_frac=0.02,
+                               prefix="ps"), list(DEFAULT_OPTS))
+    if name == "adna":
+        return (simulate_reads(ref, n, seed + 1, adna_lengths, sub_rate=0.005, random_frac=0.03, deaminate=0.3,
+                               prefix="ad"), list(ADNA_OPTS))
+    if name == "divergent":
+        return (simulate_reads(ref, n, seed + 2, 100, sub_rate=0.04, indel_rate=0.005, prefix="dv"),
+                list(DIVERGENT_OPTS))
+    if name == "genome":
+        return (simulate_reads(ref, n, seed + 3, 150, sub_rate=lambda x: 0.001 + 0.014 * x, indel_rate=0.0005,
+                               prefix="gn"), list(DEFAULT_OPTS))
+    raise KeyError(name)
+
+
 def workload(name: str, scale: float = 1.0, seed: int = 1, reads_scale: float | None = None):
     """(reference, reads, options) for a named workload at `scale` of its full size (the reads at
     `reads_scale` of theirs when given)."""
     rs = scale if reads_scale is None else reads_scale
-    if name == "plain_small":
-        ref = reference_uniform(max(10_000, int(1_000_000 * scale)), seed)
-        reads = simulate_reads(ref, max(1, int(20_000 * rs)), seed + 1, 100, sub_rate=0.01,
-                               indel_rate=0.001, random_frac=0.02, prefix="ps")
-        return ref, reads, list(DEFAULT_OPTS)
-    if name == "adna":
-        ref = reference_adna(max(20_000, int(100_000_000 * scale)), seed)
-        reads = simulate_reads(ref, max(1, int(2_000_000 * rs)), seed + 1, adna_lengths, sub_rate=0.005,
-                               random_frac=0.03, deaminate=0.3, prefix="ad")
-        return ref, reads, list(ADNA_OPTS)
-    if name == "divergent":
-        ref = reference_adna(max(20_000, int(100_000_000 * scale)), seed)
-        reads = simulate_reads(ref, max(1, int(1_000_000 * rs)), seed + 2, 100, sub_rate=0.04,
-                               indel_rate=0.005, prefix="dv")
-        return ref, reads, list(DIVERGENT_OPTS)
-    if name == "genome":
-        ref = reference_genome(max(200_000, int(3_100_000_000 * scale)), seed)
-        reads = simulate_reads(ref, max(1, int(10_000_000 * rs)), seed + 3, 150,
-                               sub_rate=lambda x: 0.001 + 0.014 * x, indel_rate=0.0005, prefix="gn")
-        return ref, reads, list(DEFAULT_OPTS)
-    raise KeyError(name)
+    ref = workload_reference(name, scale, seed)
+    reads, opts = workload_reads(name, ref, max(1, int(FULL_READS[name] * rs)), seed)
+    return ref, reads, opts
 
 
 def serving_requests(n_requests: int, seed: int, ref: Reference, scale: float = 1.0,

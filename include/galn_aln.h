@@ -78,6 +78,12 @@ galn_index *galn_index_open_mem(const void *bwt_file_bytes, size_t n_bytes, int 
 int galn_index_close(galn_index *ix);
 /* seq_len (= L2[4]), primary, and the device bytes the occurrence layout takes */
 int galn_index_info(const galn_index *ix, uint64_t *seq_len, uint64_t *primary, uint64_t *device_bytes);
+/* The occurrence layer on its own: for each of n BWT rows (in [0, seq_len], or ~0 for -1), Occ of the four
+ * bases, occ[4 i + c] = bwt_occ4's count (src/bwtgap_hd.h:135-160, src/bwtsearch.h:46-76: the $ row skipped),
+ * read from the device layout `layout` (64 or 80 symbols per 32-byte block) by the search's own device code;
+ * fetch[i] (may be NULL) the blocks it read. A check of the occurrence layer (no reference counterpart as an
+ * entry point); host arrays. */
+int galn_index_occ(galn_index *ix, int layout, const uint64_t *rows, int64_t n, uint64_t *occ, uint32_t *fetch);
 
 /* ---- reads ------------------------------------------------------------------------------------------- */
 /* A batch of reads as the search takes them: the bases as read (ASCII, any case; A/C/G/T, everything
@@ -240,12 +246,17 @@ int galn_server_stats(galn_server *s, double *p50_ms, double *p99_ms, int64_t *n
  *                     0x40000 reads) whose longest read is max_len (<= 1024 bases)
  *   d_n_aln           device, n_reads: n_aln, GALN_ERR_SCORE, or GALN_ERR_STACK / GALN_ERR_ALN when the read
  *                     needed more than the fixed per-thread stack (2048 entries) or more than rec_per_read
- *                     records (<= 256); such reads can be searched again with galn_aln_run_batch
+ *                     records (<= 256); such reads can be searched again with galn_aln_run_batch. A read
+ *                     longer than max_len (or with offsets out of order) gets GALN_EINVAL and is not searched.
  *   d_rec             device, n_reads * rec_per_read records; read r's at d_rec[r * rec_per_read]
- * Runs asynchronously on `stream` (a cudaStream_t; NULL for the default stream). The first call on a device
- * looks up the array's device address and should come before any stream capture. All calls share the
- * array: calls that overlap on the GPU race and must be serialised by the caller. Sizes past the limits
- * above return GALN_EINVAL; options that need more than 512 score buckets or negative penalties too. */
+ * Runs asynchronously on `stream` (a cudaStream_t; NULL for the default stream): a memset of the array's
+ * work counter and one kernel launch, nothing copied from the host. The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) and should come before any stream capture. All calls
+ * share the array and it keeps the last call's contents: calls that overlap on the GPU (other streams,
+ * other host threads) race on it and must be serialised by the caller. The array holds a few hundred
+ * per-thread stacks (about 700 for 100-base reads), so this runs far below galn_aln_run_batch's rate.
+ * Sizes past the limits above return GALN_EINVAL; options that need more than 512 score buckets or
+ * negative penalties too. */
 int galn_aln_run_noalloc(galn_index *ix, const galn_opts *o, int32_t n_reads, int32_t max_len, const char *d_seq,
                          const int64_t *d_offset, int32_t *d_n_aln, galn_aln1 *d_rec, int32_t rec_per_read,
                          void *stream);
@@ -291,6 +302,9 @@ int galn_last_run_phases(galn_index *ix, double *ms, int n);
  * largest power of two <= `bytes` (>= 1 MiB; larger than L2 for the HBM figure, smaller for L2), in GB/s
  * of sectors read. */
 int galn_gather_peak(int device, uint64_t bytes, int repeats, double *gbs);
+/* The same with in_flight (2, 4, 8 or 16) independent sectors in flight per thread (galn_gather_peak uses 8);
+ * 256 sectors per thread, 8 blocks of 256 threads per SM. */
+int galn_gather_peak_ex(int device, uint64_t bytes, int in_flight, int repeats, double *gbs);
 
 /* Tier capacities (no reference counterpart; set by the autotuner): entries and records per thread in the
  * first tier, its block size (64/128/256/512), live entries and records per thread in the second tier, and
@@ -300,6 +314,16 @@ int galn_index_set_tuning(galn_index *ix, int t0_cap, int t0_aln, int t0_block, 
 /* The heavy-read warp tier on or off, and its stack arena per warp in 64-entry chunks (no reference
  * counterpart; on by default with 8192 chunks, at least 32). Results never depend on it. */
 int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks);
+
+/* How long (ns) a big-arena warp of the warp tier waits for queued reads before it gives up (no reference
+ * counterpart; default 2 s). Reads still queued when the warps give up are searched in a second launch, and
+ * when a warp gave up on a read id that had not yet arrived in its claimed slot, every read that was ever
+ * queued is searched again; results never depend on it. 0 makes every wait run out at once and takes the
+ * second of those paths (a way to test it). */
+int galn_index_set_warp_wait(galn_index *ix, int64_t wait_ns);
+/* The last run's warp-tier queue (no reference counterpart): reads its first launch queued for the big-arena
+ * warps, and whether a bounded wait ran out (then all of them were searched again). */
+int galn_last_warp_queue(galn_index *ix, int64_t *queued, int *gave_up);
 
 /* The occurrence blocks in a persisting L2 access-policy window on the index's streams (no reference
  * counterpart; on by default; results never depend on it). */

@@ -42,7 +42,9 @@ def build(ref: bool = False) -> None:
 
 
 def reference_sources_present() -> bool:
-    return os.path.isdir("/root/reference/src")
+    """Whether the reference's sources are where oracle/Makefile looks for them (GALN_REFERENCE)."""
+    p = subprocess.run(["make", "-s", "-C", HERE, "ref-present"], capture_output=True)
+    return p.returncode == 0
 
 
 def ref_available() -> bool:
@@ -122,6 +124,9 @@ def lib():
         L.orc_index_load.argtypes = [C.c_char_p, ip]
         L.orc_index_free.argtypes = [vp]
         L.orc_index_meta.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.orc_occ4.argtypes = [vp, vp, C.c_int64, vp]
+        L.orc_index_borrow.restype = vp
+        L.orc_index_borrow.argtypes = [vp, C.c_uint64, ip]
         L.orc_reads_load.restype = vp
         L.orc_reads_load.argtypes = [C.c_char_p, ip, i64p, ip]
         L.orc_reads_get.argtypes = [vp, vp, vp, vp, vp]
@@ -151,15 +156,27 @@ def _ptr(a: np.ndarray):
 
 
 class Index:
-    def __init__(self, bwt_path: str):
+    def __init__(self, bwt_path: str | None = None, file_words: np.ndarray | None = None):
+        """A .bwt file, or its image in memory as uint32 words (kept alive here, not copied)."""
         err = C.c_int(0)
-        self.h = lib().orc_index_load(bwt_path.encode(), C.byref(err))
+        if file_words is not None:
+            self._words = np.ascontiguousarray(file_words, np.uint32)
+            self.h = lib().orc_index_borrow(_ptr(self._words), len(self._words), C.byref(err))
+        else:
+            self.h = lib().orc_index_load(bwt_path.encode(), C.byref(err))
         if not self.h:
-            raise IOError(f"cannot load {bwt_path} ({err.value})")
+            raise IOError(f"cannot load {bwt_path or 'the .bwt image'} ({err.value})")
         prim, words = C.c_uint64(), C.c_uint64()
         L2 = (C.c_uint64 * 5)()
         lib().orc_index_meta(self.h, C.byref(prim), L2, C.byref(words))
         self.primary, self.L2, self.words = prim.value, list(L2), words.value
+
+    def occ4(self, rows) -> np.ndarray:
+        """Occ of the four bases at each row (the $ row not counted; ~0 = row -1): (n, 4) uint64."""
+        k = np.ascontiguousarray(rows, np.uint64)
+        out = np.zeros((max(1, len(k)), 4), np.uint64)
+        lib().orc_occ4(self.h, _ptr(k), len(k), _ptr(out))
+        return out[:len(k)]
 
     def __del__(self):
         if getattr(self, "h", None):

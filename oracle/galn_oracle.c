@@ -28,7 +28,27 @@ enum { ERR_SCORE = -3 };
 typedef struct {
     uint64_t primary, L2[5], seq_len, words;
     uint32_t *body;
+    int borrowed;                  /* body is the caller's memory (orc_index_borrow) */
 } oindex_t;
+
+/* the index over a .bwt file image already in memory (header words first), without a copy: the memory
+ * must outlive the index and end with the four totals (as every .bwt does) */
+void *orc_index_borrow(const uint32_t *file_words, uint64_t n_words, int *err)
+{
+    if (n_words < 10 + 8) { *err = -2; return NULL; }
+    uint64_t hdr[5];
+    memcpy(hdr, file_words, 40);
+    oindex_t *x = (oindex_t*)calloc(1, sizeof(oindex_t));
+    x->primary = hdr[0];
+    x->L2[0] = 0;
+    for (int c = 0; c < 4; ++c) x->L2[c + 1] = hdr[c + 1];
+    x->seq_len = x->L2[4];
+    x->words = n_words - 10;
+    x->body = (uint32_t*)(file_words + 10);
+    x->borrowed = 1;
+    *err = 0;
+    return x;
+}
 
 void *orc_index_load(const char *path, int *err)
 {
@@ -56,7 +76,7 @@ void *orc_index_load(const char *path, int *err)
 void orc_index_free(void *p)
 {
     oindex_t *x = (oindex_t*)p;
-    if (x) { free(x->body); free(x); }
+    if (x) { if (!x->borrowed) free(x->body); free(x); }
 }
 
 int orc_index_meta(const void *p, uint64_t *primary, uint64_t L2[5], uint64_t *words)
@@ -89,6 +109,13 @@ static uint64_t occ(const oindex_t *x, uint64_t k, int c)
     for (int w = 0; upto > 0; ++w, upto -= 16)
         n += count_in_word(blk[8 + w], c, upto < 16 ? upto : 16);
     return n;
+}
+
+void orc_occ4(const void *index, const uint64_t *rows, int64_t n, uint64_t *out)
+{
+    const oindex_t *x = (const oindex_t*)index;
+    for (int64_t i = 0; i < n; ++i)
+        for (int c = 0; c < 4; ++c) out[4 * i + c] = occ(x, rows[i], c);
 }
 
 /* ------------------------------------------------------------------------------------------------ */

@@ -36,8 +36,12 @@ typedef struct {
 } orc_gap_opt_t;
 
 void *orc_index_load(const char *bwt_path, int *err);
+/* the same over a .bwt file image in the caller's memory (not copied; it must outlive the index) */
+void *orc_index_borrow(const uint32_t *file_words, uint64_t n_words, int *err);
 void  orc_index_free(void *index);
 int   orc_index_meta(const void *index, uint64_t *primary, uint64_t L2[5], uint64_t *bwt_words);
+/* Occ(c, k) of the four bases at n rows (out[4 i + c]; rows in [0, seq_len] or ~0 for -1) */
+void  orc_occ4(const void *index, const uint64_t *rows, int64_t n, uint64_t *out);
 
 void *orc_reads_load(const char *fastq_path, int *n_reads, int64_t *total_bases, int *err);
 int   orc_reads_get(const void *reads, uint8_t *query, int64_t *off, int32_t *len, int32_t *batch);

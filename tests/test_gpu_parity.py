@@ -9,7 +9,8 @@ import pytest
 import galn_b200
 import oracle
 from conftest import GOLDEN, case_paths, golden_cases
-from galn_b200 import build, index_build, synth
+import fixture_index as index_build
+from galn_b200 import build, synth
 
 pytestmark = pytest.mark.gpu
 CASES = golden_cases()
@@ -81,6 +82,32 @@ def test_tier_migration_gives_same_bytes(caps, warp, trace, occ):
             np.testing.assert_array_equal(prof["fetch"].astype(np.uint64), o.fetch64 if occ == 64 else o.fetch80)
         st = ix.last_stats()
         assert st["tiers"] >= 2 or name in ("edge_nonstop", "tiny_queue")
+
+
+@pytest.mark.parametrize("wait_ns", [0, 20_000])
+def test_warp_wait_running_out_gives_same_bytes(wait_ns):
+    """The big-arena warps' bounded wait for queued reads, made to run out: at 0 every wait gives up at
+    once and the host searches every queued read again in a second launch; at 20 us some waits run out and
+    the reads left in the queue go to the second launch. Bytes, pops and traces stay the reference's."""
+    ix = galn_b200.Index(os.path.join(GOLDEN, "small", "ref"))
+    ix.set_tuning(16, 1, 64, 16, 1)
+    ix.set_warp_tier(True, 32)          # a tiny arena: heavy reads outgrow it and are queued
+    ix.set_warp_wait(wait_ns)
+    queued, gave_up = 0, 0
+    for name in ("adna", "divergent", "edge_nonstop", "tiny_queue"):
+        meta = CASES[name]
+        p = case_paths(name, meta)
+        res = galn_b200.aln(ix, meta["opts"], p["fq"], galn_b200.GALN_ENGINE_PERSISTENT)
+        assert res.sai_bytes() == open(p["sai"], "rb").read(), name
+        pr = np.load(p["per_read"])
+        np.testing.assert_array_equal(res.pops, pr["pops"])
+        np.testing.assert_array_equal(res.trace, pr["trace"])
+        q = ix.last_warp_queue()
+        queued += q["queued"]
+        gave_up += int(q["gave_up"])
+    assert queued > 0, "no read was queued for a big-arena warp"
+    if wait_ns == 0:
+        assert gave_up > 0, "no wait ran out"
 
 
 @pytest.mark.parametrize("occ", [64, 80])

@@ -107,7 +107,7 @@ def test_command_line_options_without_a_gpu(tmp_path):
 def test_oracle_suffix_array_agrees_with_prefix_doubling():
     """The oracle's comparison sort and the fixture builder's prefix doubling (torch on the CPU) are two
     independent suffix sorts: they agree on random, repetitive and palindromic texts."""
-    from galn_b200 import index_build
+    import fixture_index as index_build
     rng = np.random.default_rng(31)
     u = rng.integers(0, 4, 3000)
     for T in (rng.integers(0, 4, 40_000), np.tile(u[:37], 300), np.concatenate([u, 3 - u[::-1], u, u[:1000]])):
@@ -118,7 +118,7 @@ def test_oracle_suffix_array_agrees_with_prefix_doubling():
 def test_host_step_random_fasta_against_fixture_writer(tmp_path):
     """Random FASTA files (records of random length, lowercase, runs of IUPAC codes, wrapped at random widths)
     give the same .pac/.ann/.amb from the library's host step as from the fixture builder's writer."""
-    from galn_b200 import index_build
+    import fixture_index as index_build
     rng = np.random.default_rng(8)
     alphabet = np.frombuffer(b"ACGTACGTACGTacgtNNRYKMnSW", dtype=np.uint8)
     for case in range(12):
@@ -140,3 +140,20 @@ def test_host_step_random_fasta_against_fixture_writer(tmp_path):
         index_build.write_pac_ann_amb(str(tmp_path / f"f{case}"), names, comments, seqs)
         for ext in ("pac", "ann", "amb"):
             assert _same(str(tmp_path / f"h{case}.{ext}"), str(tmp_path / f"f{case}.{ext}")), (case, ext)
+
+
+@pytest.mark.parametrize("n", [1, 15, 16, 17, 127, 128, 129, 255, 1000, 5077])
+def test_random_bwt_helper_matches_brute_force(n, tmp_path):
+    """The random .bwt files of the superblock test: the oracle's Occ over them equals a count over their
+    symbols at every row, also when the file is assembled in several chunks."""
+    import bwt_synth
+    rng = np.random.default_rng(n)
+    primary = int(rng.integers(1, n + 1))
+    for chunk in (1 << 22, 3):
+        words = bwt_synth.random_bwt(n, primary, seed=n, chunk_blocks=chunk)
+        path = str(tmp_path / f"r{chunk}.bwt")
+        words.tofile(path)
+        sym = bwt_synth.symbols(words)
+        rows = np.concatenate([np.arange(n + 1, dtype=np.uint64), np.array([(1 << 64) - 1], np.uint64)])
+        got = oracle.Index(path).occ4(rows)
+        np.testing.assert_array_equal(got, bwt_synth.occ_brute(sym, primary, rows))
