@@ -200,17 +200,19 @@ def reference_run(prefix: str, fq: str, opts: list[str], out_sai: str, cores: in
     return {"search_s": info["search_s"], "n_reads": info.get("n_reads"), "md5": md5}
 
 
-def cpu_reference_full(prefix, reads, opts, d, cores):
-    """The reference's CPU path on every read of the workload (one run, a few tens of seconds): the
-    cpu_baseline figure and the .sai the GPU arm is compared with."""
-    n = len(reads)
+def cpu_reference_full(prefix, reads, opts, d, cores, m):
+    """The reference's CPU path on the first m reads of the workload (all of them for the aDNA workload: one
+    run, a few tens of seconds): the cpu_baseline figure and the .sai the GPU arm is compared with."""
+    n = min(m, len(reads))
     fq = sample_fastq(reads, n, d, "all")
     r = reference_run(prefix, fq, opts, os.path.join(d, "ref_all.sai"), cores)
     if "error" in r:
         return None, r["error"]
+    what = f"all {n} reads" if n == len(reads) else f"the first {n} reads"
     cb = dict(value=n / max(r["search_s"], 1e-3), unit="reads/s", cores=cores, kind="reference",
-              sample=f"all {n} reads of the same workload, reference `galn aln --cpu-only --cpu-workers {cores}`, "
+              sample=f"{what} of the same workload, reference `galn aln --cpu-only --cpu-workers {cores}`, "
                      f"search time from its own timing line")
+    r["n"] = n
     return (cb, r), None
 
 
@@ -527,6 +529,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-engine comparison")
     ap.add_argument("--cpu-sample", type=int, default=200_000,
                     help="first reads of the reference arm's sample (0: no reference runs in the GPU arm)")
+    ap.add_argument("--ref-reads", type=int, default=2_000_000,
+                    help="reads of the GPU arm's reference run (its cpu_baseline and .sai md5 check)")
     ap.add_argument("--data-dir", default=None)
     ap.add_argument("--trace", action="store_true", help="compute per-read trace hashes (verification mode)")
     ap.add_argument("--t0-cap", type=int, default=1024, help="first-tier stack entries per thread")
@@ -545,7 +549,7 @@ def main():
                     help="high-divergence reads compared with the reference's .sai")
     ap.add_argument("--no-gather-sweep", dest="gather_sweep", action="store_false")
     ap.add_argument("--index-build", action="store_true", help="time `galn index` on the workload's reference")
-    ap.add_argument("--profile-case", choices=["warp_steady"], default=None)
+    ap.add_argument("--profile-case", choices=["warp_steady", "gather"], default=None)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -554,6 +558,15 @@ def main():
 
     if args.index_build:
         return index_bench(args, rank, local)
+    if args.profile_case == "gather":
+        # the random 32-byte gather probe alone, for a capture of its DRAM sectors: a 1 GiB buffer, 8 sectors in
+        # flight per thread, one warm-up and two timed launches
+        import galn_b200
+        from galn_b200 import build as gbuild
+        gbuild.build()
+        print(json.dumps({"case": "gather", "bytes": 1 << 30, "in_flight": 8,
+                          "gbs": galn_b200.gather_peak(local, 1 << 30, 8, 2)}))
+        return 0
     if args.profile_case:
         return profile_warp_steady(args, local)
     if args.impl == "reference":
@@ -701,11 +714,15 @@ def main():
 
     cpu, ref_full = None, None
     if rank == 0 and world == 1 and args.cpu_sample > 0:
-        got, why = cpu_reference_full(prefix, reads, opts, d, cores)
+        got, why = cpu_reference_full(prefix, reads, opts, d, cores, args.ref_reads)
         if got is None:
             log("[bench] cpu baseline unavailable:", why)
         else:
             cpu, ref_full = got
+            if ref_full["n"] < n:   # this build's .sai of the same prefix
+                k = ref_full["n"]
+                Rk = galn_b200.Reads(R.seq[:int(R.offset[k])], R.offset[:k + 1].copy())
+                ref_full["gpu_md5"] = hashlib.md5(galn_b200.aln(ix, opts, Rk, engine).sai_bytes()).hexdigest()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -750,8 +767,11 @@ def main():
     }
     if ref_full:
         line["sai_md5_reference"] = ref_full["md5"]
-        line["sai_md5_vs_reference"] = len(md5) == 1 and ref_full["md5"] in md5
-        line["sai_md5_vs_reference_reads"] = n
+        if "gpu_md5" in ref_full:
+            line["sai_md5_vs_reference"] = ref_full["md5"] == ref_full["gpu_md5"]
+        else:
+            line["sai_md5_vs_reference"] = len(md5) == 1 and ref_full["md5"] in md5
+        line["sai_md5_vs_reference_reads"] = ref_full["n"]
     if plain:
         line["plain_engine"] = plain
     if divergent:

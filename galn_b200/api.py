@@ -108,11 +108,16 @@ def lib():
     L.galn_autotune_clear.argtypes = [vp]
     L.galn_last_graph_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     L.galn_index_build_text.argtypes = [vp, C.c_uint64, C.c_char_p, C.c_int, C.POINTER(BuildStats)]
+    L.galn_index_build_text_ex.argtypes = [vp, C.c_uint64, C.c_char_p, C.c_int, C.c_int64, C.POINTER(BuildStats)]
     L.galn_index_build_fasta.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(BuildStats)]
     L.galn_fasta_to_pac.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_uint64)]
     L.galn_gather_peak.argtypes = [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_double)]
     L.galn_index_set_warp_wait.argtypes = [vp, C.c_int64]
     L.galn_index_occ.argtypes = [vp, C.c_int, vp, C.c_int64, vp, vp]
+    L.galn_stack_need.argtypes = [vp, C.POINTER(Options), C.POINTER(_Reads), C.POINTER(C.c_uint64)]
+    L.galn_server_memory.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                     C.POINTER(C.c_int64)]
+    L.galn_server_admissions.argtypes = [vp, vp, C.c_int]
     L.galn_last_warp_queue.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
     L.galn_gather_peak_ex.argtypes = [C.c_int, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.galn_version.restype = C.c_char_p
@@ -501,12 +506,13 @@ def fasta_to_pac(fasta: str, prefix: str) -> int:
     return n.value
 
 
-def index_text(fwd: np.ndarray, prefix: str, device: int = 0) -> dict:
+def index_text(fwd: np.ndarray, prefix: str, device: int = 0, sort_chunk: int = 0) -> dict:
     """<prefix>.bwt and <prefix>.sa for the forward sequence fwd (codes 0..3; the text is fwd . revcomp(fwd)),
-    built on a CUDA device (galn_index_build_text)."""
+    built on a CUDA device (galn_index_build_text_ex; sort_chunk > 0 takes the 64-bit path with at most that
+    many suffixes sorted at once)."""
     f = np.ascontiguousarray(fwd, dtype=np.uint8)
     st = BuildStats()
-    rc = lib().galn_index_build_text(f.ctypes.data, len(f), prefix.encode(), device, C.byref(st))
+    rc = lib().galn_index_build_text_ex(f.ctypes.data, len(f), prefix.encode(), device, sort_chunk, C.byref(st))
     if rc:
         raise GalnError(f"galn_index_build_text failed ({rc})")
     return _stats_dict(st)
@@ -552,6 +558,26 @@ class Server:
                                 C.byref(steps))
         return dict(p50_ms=p50.value, p99_ms=p99.value, requests=nr.value, reads=nreads.value, busy_ms=busy.value,
                     steps=steps.value)
+
+    def stack_need(self, args: list[str] | Options, reads: Reads) -> int:
+        """Device memory the server reserves for this request's search stacks (galn_stack_need)."""
+        opts = args if isinstance(args, Options) else parse_options(list(args))
+        cr, keep = reads.c_struct()
+        v = C.c_uint64()
+        if lib().galn_stack_need(self.h, C.byref(opts), C.byref(cr), C.byref(v)):
+            raise GalnError("galn_stack_need failed")
+        return v.value
+
+    def memory(self) -> dict:
+        b, u, p, h = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_int64()
+        lib().galn_server_memory(self.h, C.byref(b), C.byref(u), C.byref(p), C.byref(h))
+        return dict(budget=b.value, in_use=u.value, peak=p.value, held_back=h.value)
+
+    def admissions(self, n: int = 1 << 16) -> list[int]:
+        """Request ids in the order they were admitted."""
+        ids = np.zeros(max(1, n), np.int64)
+        k = lib().galn_server_admissions(self.h, ids.ctypes.data, n)
+        return ids[:max(0, k)].tolist()
 
     def close(self):
         if getattr(self, "h", None):

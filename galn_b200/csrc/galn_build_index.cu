@@ -150,7 +150,7 @@ int scan(T *x, uint64_t n, Scratch &scr, cudaStream_t st)
     return cudaGetLastError() == cudaSuccess ? 0 : GALN_ECUDA;
 }
 
-// ---- stable LSD radix sort of (uint64 key, uint32 value) pairs ----
+// ---- stable LSD radix sort of (uint64 key, V value) pairs, V = uint32 or uint64 positions ----
 
 // counts[d * tiles + tile] = items of digit d in the tile
 __global__ void __launch_bounds__(kRThreads) radix_hist(const uint64_t *__restrict__ keys, uint64_t n, int shift,
@@ -181,33 +181,36 @@ __global__ void __launch_bounds__(kRThreads) radix_hist(const uint64_t *__restri
     if (t < 256) counts[(uint64_t)t * tiles + blockIdx.x] = h[t];
 }
 
+template <class V>
 struct ScatterSmem {
     uint32_t wcnt[kRWarps][256];       // per warp: items of each digit, then their offset among the tile's
     uint32_t tstart[256];              // start of each digit in the tile's sorted order
     uint32_t gofs[256];                // the tile's first output index for each digit
     uint32_t wsum[8];
     uint64_t k[kRTile];
-    uint32_t v[kRTile];
+    V v[kRTile];
 };
 
 // Items of a tile in input order: warp w holds [w * 32 * kRItems, (w + 1) * 32 * kRItems), its step j the
 // 32 items from j * 32 on, one per lane. A lane's rank among the warp's items of its digit comes from
 // __match_any_sync; warps are ordered by a per-digit prefix over warps; the tile's items are placed in
 // digit order in shared memory and leave it in runs.
+template <class V>
 __global__ void __launch_bounds__(kRThreads) radix_scatter(const uint64_t *__restrict__ kin,
-                                                            const uint32_t *__restrict__ vin,
-                                                            uint64_t *__restrict__ kout, uint32_t *__restrict__ vout,
+                                                            const V *__restrict__ vin,
+                                                            uint64_t *__restrict__ kout, V *__restrict__ vout,
                                                             uint64_t n, int shift, const uint32_t *__restrict__ offsets,
                                                             uint32_t tiles)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(smem_raw);
+    ScatterSmem<V> &S = *reinterpret_cast<ScatterSmem<V> *>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const uint64_t base = (uint64_t)blockIdx.x * kRTile;
     const uint64_t wbase = base + (uint64_t)w * (32 * kRItems);
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint64_t key[kRItems];
-    uint32_t val[kRItems], rk[kRItems];
+    V val[kRItems];
+    uint32_t rk[kRItems];
 #pragma unroll
     for (int j = 0; j < kRItems; ++j) {   // all loads in flight while the counters are cleared
         const uint64_t i = wbase + (uint64_t)j * 32 + lane;
@@ -275,9 +278,10 @@ __global__ void __launch_bounds__(kRThreads) radix_scatter(const uint64_t *__res
     }
 }
 
+template <class V>
 struct Sorter {
     uint64_t *k[2] = {nullptr, nullptr};
-    uint32_t *v[2] = {nullptr, nullptr};
+    V *v[2] = {nullptr, nullptr};
     uint32_t *counts = nullptr;
     Scratch *scr = nullptr;
     int passes = 0;
@@ -286,7 +290,8 @@ struct Sorter {
 };
 
 // Sorts the n pairs in (k[cur], v[cur]) on key bits [0, bits); returns the buffer that holds them sorted.
-int radix_sort(Sorter &s, int cur, uint64_t n, int bits, cudaStream_t st, int &out)
+template <class V>
+int radix_sort(Sorter<V> &s, int cur, uint64_t n, int bits, cudaStream_t st, int &out)
 {
     out = cur;
     if (n <= 1) return 0;
@@ -300,8 +305,8 @@ int radix_sort(Sorter &s, int cur, uint64_t n, int bits, cudaStream_t st, int &o
         s.ev.push_back(a);
         s.ev.push_back(b);
         cudaEventRecord(a, st);
-        radix_scatter<<<tiles, kRThreads, sizeof(ScatterSmem), st>>>(s.k[cur], s.v[cur], s.k[cur ^ 1], s.v[cur ^ 1], n,
-                                                                     shift, s.counts, tiles);
+        radix_scatter<V><<<tiles, kRThreads, sizeof(ScatterSmem<V>), st>>>(s.k[cur], s.v[cur], s.k[cur ^ 1],
+                                                                           s.v[cur ^ 1], n, shift, s.counts, tiles);
         cudaEventRecord(b, st);
         if (cudaGetLastError() != cudaSuccess) return GALN_ECUDA;
         cur ^= 1;
@@ -444,6 +449,203 @@ __global__ void text_from_forward(const uint8_t *__restrict__ F, uint64_t l_pac,
 inline unsigned grid(uint64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 inline int bitlen(uint64_t x) { return x ? 64 - __builtin_clzll(x) : 0; }
 
+// ---- the 64-bit path (texts of 2^32 - 64 symbols or more) ----
+// Positions, ranks and slots are 64-bit. Round 0 runs bucket by bucket: suffixes are grouped by their first
+// kWPre symbols (a histogram of those prefix codes, then runs of consecutive codes holding at most `chunk`
+// suffixes), each bucket's suffixes are selected from the text, sorted by their 21-symbol keys and ranked;
+// the unsorted ones are appended to one list U of (position, slot) in slot order. A later round walks U in
+// chunks of whole groups: each item's key is (its group's number in the chunk, rank of p + h), the chunk is
+// sorted, ranked and its still-unsorted items compacted back into U in place. Ranks are updated while the
+// round goes on: a rank that another chunk has refined already is still consistent with the suffix order
+// (its group only split into ordered parts), so sorting by it can only refine further (Larsson-Sadakane's
+// argument). The BWT and the SA samples are scattered from the final ranks without a suffix array.
+constexpr int kWPre = 5;                                  // symbols of a bucket prefix
+constexpr uint32_t kWCodes = 1u << (3 * kWPre);           // prefix codes (3 bits a symbol)
+constexpr int kWHistTile = 1 << 20;                       // text positions per histogram block
+constexpr int kWSelTile = 1 << 14;                        // text positions per selection block
+constexpr int kWSelThreads = 256;
+
+__device__ __forceinline__ uint64_t key21(const uint8_t *__restrict__ T, uint64_t N, uint64_t i)
+{
+    uint64_t k = 0;
+    for (int j = 0; j < kPrefix; ++j) {
+        const uint64_t p = i + j;
+        k = (k << 3) | (p < N ? (uint64_t)T[p] + 1 : 0);
+    }
+    return k;
+}
+
+__device__ __forceinline__ uint32_t code5(const uint8_t *__restrict__ T, uint64_t N, uint64_t i)
+{
+    uint32_t c = 0;
+    for (int j = 0; j < kWPre; ++j) {
+        const uint64_t p = i + j;
+        c = (c << 3) | (p < N ? (uint32_t)T[p] + 1 : 0u);
+    }
+    return c;
+}
+
+// hist[c] += the text positions whose kWPre-symbol prefix code is c (a shared-memory histogram per block)
+__global__ void __launch_bounds__(1024) w_hist(const uint8_t *__restrict__ T, uint64_t N,
+                                               unsigned long long *__restrict__ hist)
+{
+    extern __shared__ uint32_t hs[];
+    for (uint32_t c = threadIdx.x; c < kWCodes; c += blockDim.x) hs[c] = 0;
+    __syncthreads();
+    const uint64_t base = (uint64_t)blockIdx.x * kWHistTile;
+    const uint64_t end = min(N, base + kWHistTile);
+    for (uint64_t i = base + threadIdx.x; i < end; i += blockDim.x) atomicAdd(&hs[code5(T, N, i)], 1u);
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < kWCodes; c += blockDim.x)
+        if (hs[c]) atomicAdd(&hist[c], (unsigned long long)hs[c]);
+}
+
+// per selection tile: how many positions have a prefix code in [lo, hi]
+__global__ void __launch_bounds__(kWSelThreads) w_sel_count(const uint8_t *__restrict__ T, uint64_t N, uint32_t lo,
+                                                            uint32_t hi, uint32_t *__restrict__ tcount)
+{
+    __shared__ uint32_t s[kWSelThreads / 32];
+    const uint64_t base = (uint64_t)blockIdx.x * kWSelTile;
+    const uint64_t end = min(N, base + kWSelTile);
+    uint32_t c = 0;
+    for (uint64_t i = base + threadIdx.x; i < end; i += kWSelThreads) {
+        const uint32_t x = code5(T, N, i);
+        c += (x >= lo && x <= hi) ? 1u : 0u;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kWSelThreads / 32; ++w) t += s[w];
+        tcount[blockIdx.x] = t;
+    }
+}
+
+// writes the selected positions in text order (tile offsets from an exclusive scan of w_sel_count) with
+// their 21-symbol keys
+__global__ void __launch_bounds__(kWSelThreads) w_sel_write(const uint8_t *__restrict__ T, uint64_t N, uint32_t lo,
+                                                            uint32_t hi, const uint32_t *__restrict__ toff,
+                                                            uint64_t *__restrict__ K, uint64_t *__restrict__ P)
+{
+    __shared__ uint32_t s[kWSelThreads / 32];
+    __shared__ uint32_t run;
+    const uint64_t base = (uint64_t)blockIdx.x * kWSelTile;
+    const uint64_t end = min(N, base + kWSelTile);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) run = toff[blockIdx.x];
+    __syncthreads();
+    for (uint64_t i0 = base; i0 < end; i0 += kWSelThreads) {
+        const uint64_t i = i0 + threadIdx.x;
+        const uint32_t x = i < end ? code5(T, N, i) : 0u;
+        const bool sel = i < end && x >= lo && x <= hi;
+        const uint32_t b = __ballot_sync(0xffffffffu, sel);
+        if (lane == 0) s[w] = (uint32_t)__popc(b);
+        __syncthreads();
+        uint32_t before = run;
+        for (int ww = 0; ww < w; ++ww) before += s[ww];
+        if (sel) {
+            const uint64_t o = before + (uint32_t)__popc(b & ((1u << lane) - 1u));
+            K[o] = key21(T, N, i);
+            P[o] = i;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t t = 0;
+            for (int ww = 0; ww < kWSelThreads / 32; ++ww) t += s[ww];
+            run += t;
+        }
+        __syncthreads();
+    }
+}
+
+// H[k] = slot of item k (slot0 + k, or slot[k]) if its key starts a group, else 0
+__global__ void w_heads(const uint64_t *__restrict__ K, uint64_t M, uint64_t slot0, const uint64_t *__restrict__ slot,
+                        uint64_t *__restrict__ H)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M) return;
+    const bool head = k == 0 || K[k] != K[k - 1];
+    H[k] = head ? (slot ? slot[k] : slot0 + k) : 0;
+}
+
+// rank[position] = its group's first slot; C[k] = 1 when item k stays unsorted
+__global__ void w_rank(const uint64_t *__restrict__ K, const uint64_t *__restrict__ P, const uint64_t *__restrict__ H,
+                       uint64_t M, uint64_t *__restrict__ rank, uint32_t *__restrict__ C)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M) return;
+    const bool head = k == 0 || K[k] != K[k - 1];
+    const bool last = k + 1 == M || K[k + 1] != K[k];
+    rank[P[k]] = H[k];
+    C[k] = (head && last) ? 0u : 1u;
+}
+
+// kept item k goes to U at out + C[k] - 1 with its position and slot (slot0 + k, or slot[k])
+__global__ void w_compact(const uint64_t *__restrict__ P, const uint32_t *__restrict__ C, uint64_t M, uint64_t slot0,
+                          const uint64_t *__restrict__ slot, uint64_t out, uint64_t *__restrict__ Upos,
+                          uint64_t *__restrict__ Uslot)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M) return;
+    const uint32_t c = C[k], prev = k ? C[k - 1] : 0u;
+    if (c == prev) return;
+    Upos[out + c - 1] = P[k];
+    Uslot[out + c - 1] = slot ? slot[k] : slot0 + k;
+}
+
+// group starts of U's items [a, a + m): F[k] = 1 when item a + k starts a group (its rank differs from the
+// item before it); the flags' inclusive scan numbers the groups
+__global__ void w_group_flags(const uint64_t *__restrict__ Upos, uint64_t a, uint64_t m, const uint64_t *__restrict__ rank,
+                              uint32_t *__restrict__ F)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    F[k] = (k == 0 || rank[Upos[a + k]] != rank[Upos[a + k - 1]]) ? 1u : 0u;
+}
+
+// the last group start in U's items (a, e], or a when there is none (one group fills the window)
+__global__ void w_last_start(const uint64_t *__restrict__ Upos, uint64_t a, uint64_t e, const uint64_t *__restrict__ rank,
+                             unsigned long long *__restrict__ best)
+{
+    const uint64_t k = a + 1 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > e) return;
+    if (rank[Upos[k]] != rank[Upos[k - 1]]) atomicMax(best, (unsigned long long)k);
+}
+
+// key of chunk item k: (its group number, rank of p + h plus one; 0 past the end), position as the value;
+// the chunk's slots are copied aside (U's slot array is overwritten by the compaction)
+__global__ void w_key(const uint64_t *__restrict__ Upos, const uint64_t *__restrict__ Uslot, uint64_t a, uint64_t m,
+                      const uint32_t *__restrict__ G, const uint64_t *__restrict__ rank, uint64_t N, uint64_t h,
+                      int lo_bits, uint64_t *__restrict__ K, uint64_t *__restrict__ P)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const uint64_t p = Upos[a + k], q = p + h;
+    const uint64_t lo = q < N ? rank[q] + 1 : 0;
+    K[k] = ((uint64_t)(G[k] - 1) << lo_bits) | lo;
+    P[k] = p;
+}
+
+__global__ void w_copy_u64(const uint64_t *__restrict__ src, uint64_t m, uint64_t *__restrict__ dst)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) dst[k] = src[k];
+}
+
+// the BWT without the $ of row `primary` (row r's symbol is T[SA[r] - 1]; suffix i is at row rank[i] + 1,
+// the $ suffix at row 0) and the SA samples of rows 32, 64, ...
+__global__ void w_bwt_scatter(const uint8_t *__restrict__ T, const uint64_t *__restrict__ rank, uint64_t N,
+                              uint64_t primary, uint8_t *__restrict__ L, uint64_t *__restrict__ smp)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    if (i == 0) L[0] = T[N - 1];
+    const uint64_t row = rank[i] + 1;
+    if (i > 0) L[row < primary ? row : row - 1] = T[i - 1];
+    if ((row & 31) == 0) smp[row / 32 - 1] = i;
+}
+
 struct DevMem {
     std::vector<void *> ptrs;
     ~DevMem()
@@ -463,15 +665,297 @@ struct DevMem {
     }
 };
 
+// Round 0 of the 64-bit path, then the doubling rounds over U; fills rank[0..N). Returns 0 or an error.
+int wide_sort(const uint8_t *T, uint64_t N, uint64_t *rank, Sorter<uint64_t> &srt, Scratch &scr, uint64_t chunk,
+              uint64_t *Upos, uint64_t *Uslot, uint64_t ucap, uint32_t *tcount, unsigned long long *hist,
+              unsigned long long *best, cudaStream_t st, int &rounds, uint64_t &sorted)
+{
+    rounds = 0;
+    sorted = 0;
+    // bucket plan: runs of consecutive prefix codes holding at most `chunk` suffixes each
+    if (cudaMemsetAsync(hist, 0, kWCodes * 8, st) != cudaSuccess) return GALN_ECUDA;
+    w_hist<<<grid(N, kWHistTile), 1024, kWCodes * 4, st>>>(T, N, hist);
+    std::vector<unsigned long long> h(kWCodes);
+    if (cudaMemcpyAsync(h.data(), hist, kWCodes * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return GALN_ECUDA;
+    const uint64_t sel_tiles = (N + kWSelTile - 1) / kWSelTile;
+    uint64_t u_n = 0, slot0 = 0;
+    uint32_t lo = 0;
+    while (lo < kWCodes) {
+        uint64_t m = 0;
+        uint32_t hi = lo;
+        while (hi < kWCodes && (m + h[hi] <= chunk || (m == 0 && h[hi] <= chunk))) m += h[hi++];
+        if (hi == lo) {
+            fprintf(stderr, "[galn index] %llu suffixes share a %d-symbol prefix: more than %llu at once\n",
+                    (unsigned long long)h[lo], kWPre, (unsigned long long)chunk);
+            return GALN_ENOMEM;
+        }
+        if (m > 0) {
+            w_sel_count<<<(unsigned)sel_tiles, kWSelThreads, 0, st>>>(T, N, lo, hi - 1, tcount);
+            int rc = scan<uint32_t, OpSum<uint32_t>, false>(tcount, sel_tiles, scr, st);
+            if (rc) return rc;
+            w_sel_write<<<(unsigned)sel_tiles, kWSelThreads, 0, st>>>(T, N, lo, hi - 1, tcount, srt.k[0], srt.v[0]);
+            int kb = 0;
+            rc = radix_sort(srt, 0, m, 3 * kPrefix, st, kb);
+            if (rc) return rc;
+            sorted += m;
+            uint64_t *H = srt.k[kb ^ 1];
+            uint32_t *C = reinterpret_cast<uint32_t *>(srt.v[kb ^ 1]);
+            w_heads<<<grid(m, 256), 256, 0, st>>>(srt.k[kb], m, slot0, nullptr, H);
+            rc = scan<uint64_t, OpMax<uint64_t>, true>(H, m, scr, st);
+            if (rc) return rc;
+            w_rank<<<grid(m, 256), 256, 0, st>>>(srt.k[kb], srt.v[kb], H, m, rank, C);
+            rc = scan<uint32_t, OpSum<uint32_t>, true>(C, m, scr, st);
+            if (rc) return rc;
+            uint32_t kept = 0;
+            if (cudaMemcpyAsync(&kept, C + m - 1, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return GALN_ECUDA;
+            if (u_n + kept > ucap) {
+                fprintf(stderr, "[galn index] %llu unsorted suffixes after the first sort: more than fit\n",
+                        (unsigned long long)(u_n + kept));
+                return GALN_ENOMEM;
+            }
+            w_compact<<<grid(m, 256), 256, 0, st>>>(srt.v[kb], C, m, slot0, nullptr, u_n, Upos, Uslot);
+            u_n += kept;
+            slot0 += m;
+        }
+        lo = hi;
+    }
+    if (slot0 != N) return GALN_ECUDA;
+    // doubling rounds over U in chunks of whole groups
+    const int lo_bits = bitlen(N);
+    uint64_t h2 = kPrefix;
+    while (u_n > 0) {
+        if (++rounds > kMaxRounds) return GALN_EINVAL;
+        uint64_t a = 0, out = 0;
+        while (a < u_n) {
+            uint64_t e = std::min(u_n, a + chunk);
+            if (e < u_n) {   // end the chunk at the last group start inside the window
+                unsigned long long b = a;
+                if (cudaMemcpyAsync(best, &b, 8, cudaMemcpyHostToDevice, st) != cudaSuccess) return GALN_ECUDA;
+                w_last_start<<<grid(e - a, 256), 256, 0, st>>>(Upos, a, e, rank, best);
+                if (cudaMemcpyAsync(&b, best, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                    cudaStreamSynchronize(st) != cudaSuccess)
+                    return GALN_ECUDA;
+                if (b == a) {
+                    fprintf(stderr, "[galn index] a group of more than %llu suffixes\n", (unsigned long long)chunk);
+                    return GALN_ENOMEM;
+                }
+                e = b;
+            }
+            const uint64_t m = e - a;
+            uint32_t *G = reinterpret_cast<uint32_t *>(srt.k[1]);
+            w_group_flags<<<grid(m, 256), 256, 0, st>>>(Upos, a, m, rank, G);
+            int rc = scan<uint32_t, OpSum<uint32_t>, true>(G, m, scr, st);
+            if (rc) return rc;
+            uint32_t n_groups = 0;
+            if (cudaMemcpyAsync(&n_groups, G + m - 1, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return GALN_ECUDA;
+            if (bitlen(n_groups) + lo_bits > 64) return GALN_EINVAL;
+            w_key<<<grid(m, 256), 256, 0, st>>>(Upos, Uslot, a, m, G, rank, N, h2, lo_bits, srt.k[0], srt.v[0]);
+            int kb = 0;
+            rc = radix_sort(srt, 0, m, lo_bits + bitlen(n_groups - 1), st, kb);
+            if (rc) return rc;
+            sorted += m;
+            uint64_t *H = srt.k[kb ^ 1];
+            uint32_t *C = reinterpret_cast<uint32_t *>(srt.v[kb ^ 1]);
+            w_heads<<<grid(m, 256), 256, 0, st>>>(srt.k[kb], m, 0, Uslot + a, H);
+            rc = scan<uint64_t, OpMax<uint64_t>, true>(H, m, scr, st);
+            if (rc) return rc;
+            w_rank<<<grid(m, 256), 256, 0, st>>>(srt.k[kb], srt.v[kb], H, m, rank, C);
+            rc = scan<uint32_t, OpSum<uint32_t>, true>(C, m, scr, st);
+            if (rc) return rc;
+            uint32_t kept = 0;
+            if (cudaMemcpyAsync(&kept, C + m - 1, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return GALN_ECUDA;
+            // the chunk's slots aside (H is consumed), then compacted into U in place: every write lands at
+            // or before the chunk's own start
+            w_copy_u64<<<grid(m, 256), 256, 0, st>>>(Uslot + a, m, H);
+            w_compact<<<grid(m, 256), 256, 0, st>>>(srt.v[kb], C, m, 0, H, out, Upos, Uslot);
+            out += kept;
+            a = e;
+        }
+        u_n = out;
+        h2 *= 2;
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : GALN_ECUDA;
+}
+
 }  // namespace ixb
 
-// The whole device part: forward sequence (host) -> .bwt words, L2, primary, .sa samples (host).
-int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bwt, uint64_t L2[5], uint64_t &primary,
-                     std::vector<uint64_t> &samples, galn_build_stats *stats)
+// The 64-bit device part (see the 64-bit path above): forward sequence (host) -> .bwt words, L2, primary,
+// .sa samples (host). chunk: suffixes sorted at once (0: from free device memory).
+static int dev_build_bwt_sa_wide(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bwt, uint64_t L2[5],
+                                 uint64_t &primary, std::vector<uint64_t> &samples, galn_build_stats *stats,
+                                 uint64_t chunk)
 {
     using namespace ixb;
     const uint64_t N = 2 * l_pac;
-    if (l_pac == 0 || N > 0xFFFFFFFFull - 64) return GALN_EINVAL;
+    if (l_pac == 0 || N >= (1ull << 40)) return GALN_EINVAL;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return GALN_ECUDA;
+    // fixed: text, ranks, bucket histogram, selection tile counts; per sorted suffix 32 bytes (keys, values)
+    // plus radix tile counts; U: 16 bytes per unsorted suffix; the end: BWT bytes, block counts and body
+    const uint64_t sel_tiles = (N + kWSelTile - 1) / kWSelTile;
+    const size_t fixed = (size_t)N + 64 + (size_t)N * 8 + kWCodes * 8 + sel_tiles * 4 + (256ull << 20);
+    if (!chunk) {
+        const size_t spare = fr > fixed ? fr - fixed : 0;
+        chunk = std::min<uint64_t>(N, std::max<uint64_t>(1 << 20, spare / 4 / 34));   // a quarter for sorting
+        chunk = std::min<uint64_t>(chunk, 1ull << 31);
+    }
+    chunk = std::min<uint64_t>(chunk, N);
+    const uint64_t rtiles = (chunk + kRTile - 1) / kRTile;
+    const size_t sort_bytes = (size_t)chunk * 32 + rtiles * 1024 + (size_t)(chunk / 1000 + 4096) * 32;
+    if (fixed + sort_bytes + (16ull << 20) > fr) {
+        fprintf(stderr, "[galn index] a text of %llu symbols needs more than %.1f GB of device memory, %.1f GB free\n",
+                (unsigned long long)N, (fixed + sort_bytes) / 1e9, fr / 1e9);
+        return GALN_ENOMEM;
+    }
+    const uint64_t ucap = std::min<uint64_t>(N, (fr - fixed - sort_bytes - (16ull << 20)) / 16);
+    cudaStream_t st;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return GALN_ECUDA;
+    cudaFuncSetAttribute(radix_scatter<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(ScatterSmem<uint64_t>));
+    cudaFuncSetAttribute(w_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kWCodes * 4));
+    const uint64_t nb = (N + 127) / 128, nw = (N + 15) / 16;
+    const uint64_t body_words = 16 * nb - (8 - (nw - 8 * (nb - 1)));
+    const uint64_t ns = (N + 32) / 32 - 1;
+    bwt.resize(body_words + 8);
+    samples.resize(ns);
+    int rc = 0;
+    cudaEvent_t ea, e0, e1, eb;
+    cudaEventCreate(&ea);
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&eb);
+    Sorter<uint64_t> srt;
+    Scratch scr;
+    int rounds = 0;
+    uint64_t sorted = 0;
+    {
+        DevMem m;
+        uint8_t *T = m.get<uint8_t>(N + 64);
+        uint64_t *rank = m.get<uint64_t>(N);
+        unsigned long long *hist = m.get<unsigned long long>(kWCodes + 1);
+        uint32_t *tcount = m.get<uint32_t>(sel_tiles);
+        if (!T || !rank || !hist || !tcount) rc = GALN_ENOMEM;
+        if (!rc) {
+            cudaEventRecord(ea, st);
+            // the forward half and its reverse complement, uploaded through the end of T (freed after)
+            DevMem fm;
+            uint8_t *F_d = fm.get<uint8_t>(l_pac);
+            if (!F_d) rc = GALN_ENOMEM;
+            if (!rc) {
+                cudaMemcpyAsync(F_d, F, l_pac, cudaMemcpyHostToDevice, st);
+                cudaEventRecord(e0, st);
+                text_from_forward<<<grid(N, 256), 256, 0, st>>>(F_d, l_pac, T);
+                cudaMemsetAsync(T + N, 0, 64, st);
+                if (cudaStreamSynchronize(st) != cudaSuccess) rc = GALN_ECUDA;
+            }
+        }
+        if (!rc) {
+            DevMem sm;
+            srt.k[0] = sm.get<uint64_t>(chunk);
+            srt.k[1] = sm.get<uint64_t>(chunk);
+            srt.v[0] = sm.get<uint64_t>(chunk);
+            srt.v[1] = sm.get<uint64_t>(chunk);
+            srt.counts = sm.get<uint32_t>(rtiles * 256);
+            scr.cap = (size_t)(chunk / 1000 + 4096) * 32;
+            scr.p = sm.get<unsigned char>(scr.cap);
+            srt.scr = &scr;
+            uint64_t *Upos = sm.get<uint64_t>(ucap), *Uslot = sm.get<uint64_t>(ucap);
+            if (!srt.k[0] || !srt.k[1] || !srt.v[0] || !srt.v[1] || !srt.counts || !scr.p || !Upos || !Uslot)
+                rc = GALN_ENOMEM;
+            if (!rc) rc = wide_sort(T, N, rank, srt, scr, chunk, Upos, Uslot, ucap, tcount, hist, hist + kWCodes, st,
+                                    rounds, sorted);
+            if (rc) cudaStreamSynchronize(st);
+        }
+        if (!rc) {
+            uint64_t r0 = 0;
+            if (cudaMemcpyAsync(&r0, rank, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                rc = GALN_ECUDA;
+            primary = r0 + 1;
+        }
+        if (!rc) {
+            DevMem em;
+            uint8_t *L = em.get<uint8_t>(N);
+            U4 *cnt = em.get<U4>(nb);
+            uint32_t *body = em.get<uint32_t>(nb * 16);
+            uint64_t *smp = em.get<uint64_t>(std::max<uint64_t>(ns, 1));
+            scr.cap = (size_t)(nb / 100 + 4096) * 64;
+            scr.top = 0;
+            scr.p = em.get<unsigned char>(scr.cap);
+            if (!L || !cnt || !body || !smp || !scr.p) rc = GALN_ENOMEM;
+            if (!rc) {
+                w_bwt_scatter<<<grid(N, 256), 256, 0, st>>>(T, rank, N, primary, L, smp);
+                bwt_block_counts<<<grid(nb, 128), 128, 0, st>>>(L, N, nb, cnt);
+                rc = scan<U4, OpSum<U4>, true>(cnt, nb, scr, st);
+            }
+            if (!rc) {
+                bwt_write<<<grid(nb * 16, 256), 256, 0, st>>>(L, N, nb, cnt, body);
+                U4 totals{};
+                cudaEventRecord(e1, st);
+                cudaMemcpyAsync(bwt.data(), body, body_words * 4, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(&totals, cnt + nb - 1, sizeof(U4), cudaMemcpyDeviceToHost, st);
+                if (ns) cudaMemcpyAsync(samples.data(), smp, ns * 8, cudaMemcpyDeviceToHost, st);
+                cudaEventRecord(eb, st);
+                if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = GALN_ECUDA;
+                if (!rc) {
+                    memcpy(bwt.data() + body_words, totals.c, sizeof(totals.c));
+                    L2[0] = 0;
+                    for (int c = 0; c < 4; ++c) L2[c + 1] = L2[c] + totals.c[c];
+                }
+            }
+            if (rc) cudaStreamSynchronize(st);
+        }
+        if (stats && !rc) {
+            stats->n = N;
+            stats->primary = primary;
+            stats->rounds = rounds;
+            stats->sorted_items = sorted;
+            stats->sort_passes = srt.passes;
+            stats->scatter_items = srt.scatter_items;
+            float ms = 0, up = 0, down = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            cudaEventElapsedTime(&up, ea, e0);
+            cudaEventElapsedTime(&down, e1, eb);
+            stats->ms_device = ms;
+            stats->ms_copies = up + down;
+            double sc = 0;
+            for (size_t i = 0; i + 1 < srt.ev.size(); i += 2) {
+                float x = 0;
+                cudaEventElapsedTime(&x, srt.ev[i], srt.ev[i + 1]);
+                sc += x;
+            }
+            stats->ms_scatter = sc;
+        }
+    }
+    for (cudaEvent_t e : srt.ev) cudaEventDestroy(e);
+    cudaEventDestroy(ea);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(eb);
+    cudaStreamDestroy(st);
+    if (rc == GALN_ECUDA) cudaGetLastError();
+    return rc;
+}
+
+// The whole device part: forward sequence (host) -> .bwt words, L2, primary, .sa samples (host). Texts of
+// 2^32 - 64 symbols or more, or any text when sort_chunk > 0, take the 64-bit path.
+int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bwt, uint64_t L2[5], uint64_t &primary,
+                     std::vector<uint64_t> &samples, galn_build_stats *stats, int64_t sort_chunk)
+{
+    using namespace ixb;
+    const uint64_t N = 2 * l_pac;
+    if (sort_chunk > 0 || (l_pac > 0 && N > 0xFFFFFFFFull - 64))
+        return dev_build_bwt_sa_wide(F, l_pac, bwt, L2, primary, samples, stats,
+                                     sort_chunk > 0 ? (uint64_t)sort_chunk : 0);
+    if (l_pac == 0) return GALN_EINVAL;
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return GALN_ECUDA;
     const uint64_t tiles = (N + kRTile - 1) / kRTile;
@@ -484,7 +968,8 @@ int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bw
     cudaStream_t st;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return GALN_ECUDA;
     // per device: the attribute belongs to the current device's context
-    cudaFuncSetAttribute(radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ScatterSmem));
+    cudaFuncSetAttribute(radix_scatter<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(ScatterSmem<uint32_t>));
     // the copies go straight from and to the caller's pageable arrays: page-locking them for one build costs
     // more host time than the copies save
     const uint64_t nb = (N + 127) / 128, nw = (N + 15) / 16;
@@ -498,7 +983,7 @@ int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bw
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventCreate(&eb);
-    Sorter srt;
+    Sorter<uint32_t> srt;
     Scratch scr;
     {
         DevMem m;

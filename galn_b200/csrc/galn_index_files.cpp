@@ -305,7 +305,7 @@ double now_ms()
 }
 
 int build_text(const uint8_t *fwd, uint64_t l_pac, const std::string &prefix, int device, galn_build_stats *stats,
-               double ms_before)
+               double ms_before, int64_t sort_chunk = 0)
 {
     for (uint64_t i = 0; i < l_pac; ++i)
         if (fwd[i] > 3) return GALN_EINVAL;
@@ -314,7 +314,7 @@ int build_text(const uint8_t *fwd, uint64_t l_pac, const std::string &prefix, in
     uint64_t L2[5] = {0, 0, 0, 0, 0}, primary = 0;
     galn_build_stats st{};
     if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return GALN_ECUDA; }
-    int rc = galn::dev_build_bwt_sa(fwd, l_pac, bwt, L2, primary, samples, &st);
+    int rc = galn::dev_build_bwt_sa(fwd, l_pac, bwt, L2, primary, samples, &st, sort_chunk);
     if (rc) return rc;
     const double t0 = now_ms();
     rc = write_bwt_sa(prefix, primary, L2, bwt, 2 * l_pac, samples);
@@ -330,6 +330,13 @@ extern "C" int galn_index_build_text(const uint8_t *fwd, uint64_t l_pac, const c
 {
     if (!fwd || !prefix || l_pac == 0) return GALN_EINVAL;
     return build_text(fwd, l_pac, prefix, device, stats, 0.0);
+}
+
+extern "C" int galn_index_build_text_ex(const uint8_t *fwd, uint64_t l_pac, const char *prefix, int device,
+                                        int64_t sort_chunk, galn_build_stats *stats)
+{
+    if (!fwd || !prefix || l_pac == 0 || sort_chunk < 0) return GALN_EINVAL;
+    return build_text(fwd, l_pac, prefix, device, stats, 0.0, sort_chunk);
 }
 
 extern "C" int galn_fasta_to_pac(const char *fasta, const char *prefix, uint64_t *l_pac)

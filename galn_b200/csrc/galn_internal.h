@@ -126,7 +126,9 @@ int32_t *warp_queue(const WarpCfg &c, int n, void *ws_mem, int32_t **slots);
 // The device part of `galn index` (galn_build_index.cu): the forward sequence F[0..l_pac) (host, codes
 // 0..3) -> the .bwt words after its header (the Occ-interleaved body and the four totals), L2, primary and
 // the .sa samples SA[32], SA[64], ...
+// Texts of 2^32 - 64 symbols or more, or any text with sort_chunk > 0 (suffixes sorted at once), take the
+// builder's 64-bit path.
 int dev_build_bwt_sa(const uint8_t *F, uint64_t l_pac, std::vector<uint32_t> &bwt, uint64_t L2[5], uint64_t &primary,
-                     std::vector<uint64_t> &samples, galn_build_stats *stats);
+                     std::vector<uint64_t> &samples, galn_build_stats *stats, int64_t sort_chunk = 0);
 
 }  // namespace galn

@@ -5,9 +5,15 @@
 // requests -- every request first gets an equal share, what is left goes to the oldest -- and searches them
 // together in one pass of the device tiers, so requests share the same kernels. A request that arrives
 // while a step runs joins the next step; a request leaves as soon as its last read has been searched.
-// Admission is bounded by the step size (the device workspace of one step) and by max_active requests in
-// flight; later requests wait in the queue. Several steps run at once (n_workers, each with its own stream
-// and device buffers), so the last heavy reads of one step overlap the next step's work on the device.
+// Admission is by the device memory the requests' search stacks need (the reference sizes its warps and
+// stack arenas from free device memory, src/galn.cu:908-965): each request's need comes from its option set
+// and size (request_stack_need: a first-tier stack per read in flight, sized by n_stacks and the longest read,
+// and the max_entries-deep arenas of the heavy-read warps its reads can occupy), and a queued request is
+// admitted only while the needs of the admitted requests fit the server's stack budget. A request that does
+// not fit waits while later, smaller ones are admitted past it, up to kMaxBypass of them; then admission
+// waits until it fits (it is admitted alone at worst, so nothing waits for ever). max_active bounds the
+// requests in flight as well. Several steps run at once (n_workers, each with its own stream and device
+// buffers), so the last heavy reads of one step overlap the next step's work on the device.
 //
 // Results do not depend on what else is in a step: each read's options are its request's, and each bwa
 // batch's options come from the longest read of that batch in its own request (batch_max_len), whether the
@@ -42,6 +48,8 @@ struct Chunk {                         // results of reads [r0, r0 + m) of a req
 
 struct Request {
     int64_t id = 0;
+    uint64_t need = 0;                 // device memory its search stacks need (request_stack_need)
+    int64_t admit_seq = -1;            // order of admission
     galn_opts opt;
     std::vector<char> seq;
     std::vector<int64_t> off;
@@ -78,11 +86,82 @@ struct galn_server {
     int n_workers = 2;
     std::vector<galn::ExecCtx *> ctxs;
     std::vector<std::thread> workers;
+    // admission by stack memory
+    uint64_t mem_budget = 0;           // device memory the admitted requests' stacks may take
+    uint64_t mem_active = 0, mem_peak = 0;
+    int head_passed = 0;               // requests admitted past the queue's head while it did not fit
+    int64_t held_back = 0;             // times a queued request was passed over for lack of stack memory
+    int64_t admitted = 0;
+    std::vector<int64_t> admit_order;  // request ids in the order they were admitted (finished requests)
     // statistics
     std::vector<double> lat_ms;
     int64_t reads_done = 0, steps = 0;
     double busy_ms = 0;
 };
+
+namespace {
+
+constexpr int kMaxBypass = 64;         // later requests admitted past one that does not fit, at most
+
+// The device memory the search stacks of a request need: a first-tier stack for each of its reads in
+// flight (reads of a step), as the first tier sizes one (entries and links, a head per score bucket, the
+// width arrays of the longest read, the records), and the deepest stack one of its reads may build, an arena
+// that holds the max_entries cut-off (the heavy-read tier's; the reference sizes its arenas the same way,
+// src/galn.cu:916-918). n_stacks, max_diff and the entry width follow the options as the engine derives them
+// (src/aln_host.c:23-38).
+uint64_t request_stack_need(const galn_index *ix, const galn_opts *o, int n, int max_len, int step_reads)
+{
+    int max_diff = o->max_diff, max_gapo = o->max_gapo;
+    if (o->fnr > 0.0) max_diff = galn_cal_maxdiff(max_len, 0.02, o->fnr);
+    if (max_diff < max_gapo) max_gapo = max_diff;
+    const int64_t n_stacks = std::max<int64_t>(1, (int64_t)(max_diff + 1) * o->s_mm + (int64_t)(max_gapo + 1) * o->s_gapo +
+                                                      (int64_t)(o->max_gape + 1) * o->s_gape);
+    const bool wide = max_diff > 125 || max_gapo > 126 || o->max_gape > 126 || ix->dev.seq_len >= (1ull << 38);
+    const uint64_t esz = (wide ? 32 : 16) + 4;
+    const int seed = o->seed_len >= 0 && o->seed_len < max_len ? o->seed_len + 1 : 0;
+    const uint64_t slot = (uint64_t)ix->t0_cap * esz + (uint64_t)n_stacks * 4 + (uint64_t)(max_len + 2 + seed) * 8 +
+                          (uint64_t)ix->t0_aln * 24;
+    const uint64_t deepest = ((uint64_t)std::max(o->max_entries, 0) + 16) * esz + (uint64_t)n_stacks * 4;
+    return (uint64_t)std::min(n, step_reads) * slot + (n > 0 ? deepest : 0);
+}
+
+}  // namespace
+
+// Moves queued requests into the active set while their stack memory fits (and max_active allows); a
+// request that does not fit is passed by later ones up to kMaxBypass times. Returns whether any was admitted.
+static bool admit(galn_server *s, bool dry_run)
+{
+    bool any = false;
+    int passed = s->head_passed;
+    uint64_t used = s->mem_active;
+    size_t n_active = s->active.size();
+    for (size_t q = 0; q < s->queue.size() && (int)n_active < s->max_active;) {
+        Request *rq = s->queue[q];
+        const bool fits = n_active == 0 || used + rq->need <= s->mem_budget;
+        if (!fits) {
+            if (q == 0 && passed >= kMaxBypass) break;   // the head has waited long enough: nothing passes it
+            if (!dry_run) ++s->held_back;
+            ++q;
+            continue;
+        }
+        any = true;
+        used += rq->need;
+        ++n_active;
+        if (q > 0) ++passed;
+        if (dry_run) { ++q; continue; }
+        if (q == 0) passed = 0;
+        rq->admit_seq = s->admitted++;
+        if (s->admit_order.size() < ((size_t)1 << 20)) s->admit_order.push_back(rq->id);
+        s->active.push_back(rq);
+        s->queue.erase(s->queue.begin() + (long)q);
+    }
+    if (!dry_run) {
+        s->head_passed = passed;
+        s->mem_active = used;
+        s->mem_peak = std::max(s->mem_peak, used);
+    }
+    return any;
+}
 
 static void finish_request(Request *rq)
 {
@@ -131,10 +210,9 @@ static void serve_loop(galn_server *s, galn::ExecCtx *ctx)
             std::unique_lock<std::mutex> lk(s->mu);
             // wait for reads nobody has taken yet (a request may be active with all its reads in flight)
             auto has_work = [&] {
-                if (!s->queue.empty() && (int)s->active.size() < s->max_active) return true;
                 for (Request *rq : s->active)
                     if (rq->next < rq->n || (rq->n == 0 && rq->next == 0)) return true;
-                return false;
+                return !s->queue.empty() && admit(s, true);
             };
             // with a step already running, a fill target makes the next step wait until it can take that
             // many reads (or the running step ends): fewer, fuller steps when requests arrive quickly
@@ -148,10 +226,7 @@ static void serve_loop(galn_server *s, galn::ExecCtx *ctx)
             };
             s->cv_work.wait(lk, [&] { return s->stop || (has_work() && can_start()); });
             if (s->stop && !has_work()) return;
-            while (!s->queue.empty() && (int)s->active.size() < s->max_active) {
-                s->active.push_back(s->queue.front());
-                s->queue.pop_front();
-            }
+            admit(s, false);
             // equal shares first, then the oldest requests take what is left
             int budget = s->step_reads;
             int na = (int)s->active.size();
@@ -263,6 +338,7 @@ static void serve_loop(galn_server *s, galn::ExecCtx *ctx)
                     rq->done = true;
                     s->lat_ms.push_back(rq->t_done - rq->t_submit);
                     s->active.erase(std::find(s->active.begin(), s->active.end(), rq));
+                    s->mem_active -= rq->need;
                 }
             }
         }
@@ -277,12 +353,13 @@ extern "C" galn_server *galn_server_start(galn_index *ix, size_t stack_bytes, in
     if (!ix) { if (err) *err = GALN_EINVAL; return nullptr; }
     auto *s = new galn_server();
     s->ix = ix;
-    if (stack_bytes) {
-        // a step's device workspace scales with its reads: about 100 KB per first-tier thread slot
-        size_t reads = stack_bytes / (100 * 1024);
-        s->step_reads = (int)std::max<size_t>(16384, std::min<size_t>(reads, 1 << 20));
-    }
     if (cudaSetDevice(ix->dev.device) != cudaSuccess) { delete s; if (err) *err = GALN_ECUDA; return nullptr; }
+    s->mem_budget = stack_bytes;
+    if (!stack_bytes) {   // default: half of the device memory free now (the index is already resident)
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { delete s; if (err) *err = GALN_ECUDA; return nullptr; }
+        s->mem_budget = free_b / 2;
+    }
     for (int w = 0; w < s->n_workers; ++w) {
         auto *c = new galn::ExecCtx();
         c->mem_share = 1.0 / s->n_workers;
@@ -371,8 +448,10 @@ extern "C" int64_t galn_aln_submit(galn_server *s, const galn_opts *o, const gal
     rq->n_aln.reserve((size_t)n);
     rq->pops.reserve((size_t)n);
     rq->trace.reserve((size_t)n);
+    const int max_len = n ? *std::max_element(rq->bmax.begin(), rq->bmax.end()) : 0;
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->queue.size() >= s->max_queued) { delete rq; return GALN_EBUSY; }
+    rq->need = request_stack_need(s->ix, o, n, max_len, s->step_reads);
     rq->id = s->next_id++;
     rq->t_submit = now_ms();
     s->all[rq->id] = rq;
@@ -396,6 +475,38 @@ extern "C" int galn_aln_wait(galn_server *s, int64_t id, int timeout_ms, galn_re
     s->all.erase(it);
     delete rq;
     return rc;
+}
+
+extern "C" int galn_stack_need(galn_server *s, const galn_opts *o, const galn_reads *in, uint64_t *bytes)
+{
+    if (!s || !o || !in || !bytes || in->n_reads < 0 || (in->n_reads > 0 && !in->offset)) return GALN_EINVAL;
+    int max_len = 0;
+    for (int r = 0; r < in->n_reads; ++r) max_len = std::max<int64_t>(max_len, in->offset[r + 1] - in->offset[r]);
+    if (in->batch_max_len)
+        for (int b = 0; b < in->n_batches; ++b) max_len = std::max(max_len, (int)in->batch_max_len[b]);
+    std::lock_guard<std::mutex> lk(s->mu);
+    *bytes = request_stack_need(s->ix, o, in->n_reads, max_len, s->step_reads);
+    return 0;
+}
+
+extern "C" int galn_server_memory(galn_server *s, uint64_t *budget, uint64_t *in_use, uint64_t *peak, int64_t *held_back)
+{
+    if (!s) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (budget) *budget = s->mem_budget;
+    if (in_use) *in_use = s->mem_active;
+    if (peak) *peak = s->mem_peak;
+    if (held_back) *held_back = s->held_back;
+    return 0;
+}
+
+extern "C" int galn_server_admissions(galn_server *s, int64_t *ids, int n)
+{
+    if (!s || n < 0 || (n > 0 && !ids)) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    const int k = (int)std::min<size_t>((size_t)n, s->admit_order.size());
+    for (int i = 0; i < k; ++i) ids[i] = s->admit_order[(size_t)i];
+    return k;
 }
 
 extern "C" int galn_server_stats(galn_server *s, double *p50_ms, double *p99_ms, int64_t *n_requests, int64_t *n_reads,

@@ -165,8 +165,11 @@ int galn_sa2pos(galn_index *ix, const uint64_t *rows, const int32_t *ref_len, in
  * The files of `bwa index` 0.7.19, byte for byte: <prefix>.pac/.ann/.amb from the FASTA records (the
  * reference's src/index/fasta_pac.c, bwa's bns_fasta2bntseq) and <prefix>.bwt/.sa from the text
  * F . revcomp(F), F the forward sequence with ambiguous bases replaced (the reference's GPU builder,
- * src/index/gpu_index.cu:1-20). The suffix sort, BWT, Occ packing and SA sampling run on the GPU; texts
- * up to 2^32 - 64 symbols (references up to about 2.1 Gbp), about 38 bytes of device memory per symbol. */
+ * src/index/gpu_index.cu:1-20). The suffix sort, BWT, Occ packing and SA sampling run on the GPU. Texts
+ * below 2^32 - 64 symbols (references up to about 2.1 Gbp) take a 32-bit path, about 38 bytes of device
+ * memory per symbol; longer ones (a 3.1 Gbp genome is 6.2 x 10^9 symbols) a 64-bit path that sorts in
+ * buckets and chunks: 9 bytes per symbol plus 16 per suffix still unsorted after the first 21 symbols, plus
+ * the sort buffers (the reference's low-memory builder for such texts is src/index/gpu_sa.cu:1-18). */
 typedef struct {
     uint64_t n;                 /* text length, 2 x reference length */
     uint64_t primary;           /* the BWT row of the whole text */
@@ -189,6 +192,12 @@ int galn_fasta_to_pac(const char *fasta, const char *prefix, uint64_t *l_pac);
  * Returns 0, GALN_EINVAL (empty or too long), GALN_ENOMEM (device memory), GALN_EIO or GALN_ECUDA.
  * stats may be NULL. */
 int galn_index_build_text(const uint8_t *fwd, uint64_t l_pac, const char *prefix, int device, galn_build_stats *stats);
+/* The same with the 64-bit path's sort chunk (no reference counterpart): 0 chooses the path by the text's
+ * length and the chunk from free device memory; sort_chunk > 0 takes the 64-bit path at any length with at
+ * most that many suffixes sorted at once (so small texts exercise its buckets and chunks). The files are
+ * the same either way. */
+int galn_index_build_text_ex(const uint8_t *fwd, uint64_t l_pac, const char *prefix, int device, int64_t sort_chunk,
+                             galn_build_stats *stats);
 
 /* All five files for a FASTA file (plain or gzip), built on `device`, as `galn index -a gpu -p <prefix>
  * <fasta>` writes them (src/index/galn_index.c:36-71). */
@@ -212,11 +221,23 @@ int galn_sai_close(galn_sai_writer *w);
 /* A resident index serves requests with their own options and batch boundaries (continuous batching):
  * steps of up to step_reads reads are taken from all admitted requests (equal shares, then oldest first)
  * and searched together; a request that arrives while a step runs joins the next one, and leaves when its
- * last read is done. stack_bytes (0: default) bounds a step's device workspace. Each request's results
- * are the same bytes as a galn_aln_run_batch of it alone. The reference's equivalent is its per-batch
- * scheduling of one input file (src/galn.cu:605-635, 835-905). */
+ * last read is done. Requests are admitted by the device memory their search stacks need (galn_stack_need)
+ * against a budget of stack_bytes (0: half of the device memory free at start); one that does not fit waits
+ * while later requests that fit pass it (at most 64 of them), and is admitted alone at worst. Each
+ * request's results are the same bytes as a galn_aln_run_batch of it alone. The reference's equivalent is
+ * its per-batch scheduling of one input file with warps and stack arenas sized from free device memory
+ * (src/galn.cu:605-635, 835-965). */
 typedef struct galn_server galn_server;
 galn_server *galn_server_start(galn_index *ix, size_t stack_bytes, int *err);
+/* The device memory the server reserves for a request's search stacks while it is admitted (no reference
+ * counterpart): a first-tier stack per read of a step (entries, a head per score bucket of its options,
+ * the width arrays of its longest read, the records) plus one stack deep enough for its max_entries. */
+int galn_stack_need(galn_server *s, const galn_opts *o, const galn_reads *in, uint64_t *bytes);
+/* The stack budget, the reservation of the admitted requests now and at most, and how many times a queued
+ * request was passed over for lack of stack memory (no reference counterpart). */
+int galn_server_memory(galn_server *s, uint64_t *budget, uint64_t *in_use, uint64_t *peak, int64_t *held_back);
+/* Up to n request ids in the order they were admitted; returns how many (no reference counterpart). */
+int galn_server_admissions(galn_server *s, int64_t *ids, int n);
 int galn_server_stop(galn_server *s);
 /* copies the request's inputs; returns a request id > 0, or an error */
 int64_t galn_aln_submit(galn_server *s, const galn_opts *o, const galn_reads *in);

@@ -218,7 +218,7 @@ def build_index(fasta: str, prefix: str, device: str | None = None) -> dict:
 
 def build_from_reference(ref, prefix: str, device: str | None = None) -> dict:
     """Index a synth.Reference directly (writes its FASTA next to the index as <prefix>.fa)."""
-    from . import synth
+    from galn_b200 import synth
     fa = prefix + ".fa"
     synth.write_fasta(fa, ref)
     return build_index(fa, prefix, device)

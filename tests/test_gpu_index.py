@@ -79,6 +79,38 @@ def test_texts_against_oracle(name, F, tmp_path):
         assert _same(str(tmp_path / ("g." + ext)), str(tmp_path / ("o." + ext))), ext
 
 
+# suffixes the 64-bit path sorts at once, per text: small enough for several buckets and round chunks where
+# the text allows it (a homopolymer's suffixes share one prefix and one group, so it needs the whole text)
+WIDE_CHUNK = {"random": 31_250, "repeats": 16_000, "palindrome": 4_000}
+
+
+@pytest.mark.parametrize("name,F", list(_texts()), ids=[t[0] for t in _texts()])
+def test_texts_64bit_path_against_oracle(name, F, tmp_path):
+    """The builder's 64-bit path (bucketed first sort, doubling rounds in chunks of whole groups, BWT and
+    samples scattered from the ranks) forced on the same texts: the oracle's .bwt and .sa."""
+    F = np.asarray(F, dtype=np.uint8)
+    chunk = WIDE_CHUNK.get(name, 2 * len(F))
+    st = galn_b200.index_text(F, str(tmp_path / "w"), sort_chunk=chunk)
+    oracle.index_files(F, str(tmp_path / "o"))
+    for ext in ("bwt", "sa"):
+        assert _same(str(tmp_path / ("w." + ext)), str(tmp_path / ("o." + ext))), ext
+    assert st["n"] == 2 * len(F)
+
+
+def test_genome_shape_64bit_path_equals_32bit_path(tmp_path):
+    """8 Mbp with repeat families, tandem repeats and N runs (16 M suffixes): the 64-bit path with a million
+    suffixes per sort (many buckets, many chunks per round) writes the 32-bit path's files."""
+    ref = synth.reference_genome(8_000_000, 31, n_contigs=5)
+    fa = str(tmp_path / "ref.fa")
+    synth.write_fasta(fa, ref)
+    galn_b200.index_fasta(fa, str(tmp_path / "n"))
+    F = oracle.forward_from_pac(str(tmp_path / "n.pac"))
+    st = galn_b200.index_text(F, str(tmp_path / "w"), sort_chunk=1 << 20)
+    for ext in ("bwt", "sa"):
+        assert _same(str(tmp_path / ("w." + ext)), str(tmp_path / ("n." + ext))), ext
+    assert st["rounds"] >= 2 and st["sorted_items"] > st["n"]
+
+
 def test_genome_shape_against_fixture_builder(tmp_path):
     """8 Mbp with repeat families, tandem repeats and N runs: the fixture builder (prefix doubling on
     torch.sort, byte-identical to the reference builder on the golden genomes) gives the same five files."""

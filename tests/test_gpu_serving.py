@@ -81,3 +81,36 @@ def test_empty_request(ix):
     rid = srv.submit([], galn_b200.Reads.from_strings([]))
     assert len(srv.wait(rid)) == 0
     srv.close()
+
+
+def test_heavy_request_held_back_by_stack_memory(ix):
+    """Admission by stack memory: with a budget that holds a large light request and a small one, a request
+    whose options need a much deeper stack (-m 50,000,000) is held back while light requests submitted after
+    it are admitted; every result still equals the request searched alone."""
+    plain = galn_b200.read_fastq(case_paths("plain", CASES["plain"])["fq"])
+    adna = galn_b200.read_fastq(case_paths("adna", CASES["adna"])["fq"])
+    seqs = [bytes(plain.seq[plain.offset[i]:plain.offset[i + 1]]) for i in range(len(plain))]
+    big = galn_b200.Reads.from_strings(seqs * 40)                      # 80,000 reads, default options
+    small = galn_b200.Reads(plain.seq, plain.offset)
+    heavy_opts = list(CASES["adna"]["opts"]) + ["-m", "50000000"]
+    heavy = galn_b200.Reads(adna.seq, adna.offset)
+    reqs = [("L1", [], big), ("H", heavy_opts, heavy), ("L2", [], small), ("L3", [], small)]
+    alone = {name: galn_b200.aln(ix, opts, reads).sai_bytes() for name, opts, reads in reqs}
+    probe = galn_b200.Server(ix)
+    need = {name: probe.stack_need(opts, reads) for name, opts, reads in reqs}
+    probe.close()
+    assert need["H"] > need["L2"] + (1 << 20)
+    budget = need["L1"] + need["L2"] + (1 << 20)
+    srv = galn_b200.Server(ix, stack_bytes=budget)
+    try:
+        ids = {name: srv.submit(opts, reads) for name, opts, reads in reqs}
+        got = {name: srv.wait(rid).sai_bytes() for name, rid in ids.items()}
+        order = srv.admissions()
+        mem = srv.memory()
+    finally:
+        srv.close()
+    for name in alone:
+        assert got[name] == alone[name], name
+    assert mem["budget"] == budget and mem["peak"] <= budget
+    assert mem["held_back"] >= 1
+    assert order.index(ids["H"]) > order.index(ids["L2"]), "the heavy request was not held back"

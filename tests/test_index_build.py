@@ -157,3 +157,16 @@ def test_random_bwt_helper_matches_brute_force(n, tmp_path):
         rows = np.concatenate([np.arange(n + 1, dtype=np.uint64), np.array([(1 << 64) - 1], np.uint64)])
         got = oracle.Index(path).occ4(rows)
         np.testing.assert_array_equal(got, bwt_synth.occ_brute(sym, primary, rows))
+
+
+def test_fixture_builder_from_reference(tmp_path):
+    """The fixture builder indexes a synthetic reference directly (on the host here) with the oracle's
+    .bwt and .sa."""
+    import fixture_index
+    from galn_b200 import synth
+    ref = synth.reference_adna(20_000, 5, n_contigs=2)
+    fixture_index.build_from_reference(ref, str(tmp_path / "fx"), "cpu")
+    F = oracle.forward_from_pac(str(tmp_path / "fx.pac"))
+    oracle.index_files(F, str(tmp_path / "o"))
+    for ext in ("bwt", "sa"):
+        assert filecmp.cmp(str(tmp_path / ("fx." + ext)), str(tmp_path / ("o." + ext)), shallow=False), ext
