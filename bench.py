@@ -374,7 +374,7 @@ def divergent_run(ix, ref, d: str, args, cores: int, prefix: str) -> dict:
     reads, opts = synth.workload_reads("divergent", ref, n, seed=1)
     R = galn_b200.Reads(reads.ascii(), reads.off.copy())
     log(f"[bench] divergent: {n} reads generated in {time.time() - t:.1f} s")
-    tune = ix.autotune(opts, R, max_sample=min(n, 16384))
+    tune = ix.autotune(opts, R, max_sample=min(n, 4096))
 
     def timed(eng, rr, k, w):
         dev, e2e = [], []

@@ -415,15 +415,20 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
             for (int32_t r : elig) sorted[(size_t)cnt[(size_t)key(r)]++] = r;
             elig.swap(sorted);
         }
-        // pass 1: the tuned arena per warp, plus up to kBigWarps warps whose arenas hold the max_entries
+        // pass 1: the tuned arena per warp, plus up to n_big_max warps whose arenas hold the max_entries
         // cut-off and take over, in the same launch, the reads that outgrow the small ones; pass 2, only for
         // reads still queued when pass 1 ended, with big arenas for every warp
         const int aln_cap_w = 4096;
-        const int kBigWarps = 128;
+        // the arena per warp and the big-arena warps: the autotuner's for this option set, else the index's
+        int arena = ix->warp_arena, n_big_max = ix->warp_big;
+        if (!ix->tune_active) {
+            auto it = ix->tuned.find(opts_key(&sets[0]));
+            if (it != ix->tuned.end() && it->second.arena > 0) { arena = it->second.arena; n_big_max = it->second.big; }
+        }
         // the cut-off, one wave's staged pushes and a partly filled chunk per bucket
         const int64_t full = (max_entries_all + 16 + 3 * 32 * 128 + kWarpMaxStacks * kWarpChunk) / kWarpChunk
                              + kWarpMaxStacks + 1;
-        const int big_chunks = (int)std::min<int64_t>(std::max<int64_t>(full, ix->warp_arena), 1 << 22);
+        const int big_chunks = (int)std::min<int64_t>(std::max<int64_t>(full, arena), 1 << 22);
         for (int pass = 0; pass < 2 && !elig.empty(); ++pass) {
             int ne = (int)elig.size();
             int res_w = warp_resident(ix->dev.device);
@@ -431,11 +436,11 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
             WarpCfg wc;
             wc.aln_cap = aln_cap_w;
             wc.n_warps = std::min(ne, res_w);
-            wc.arena_chunks = ix->warp_arena;
+            wc.arena_chunks = arena;
             wc.big_chunks = big_chunks;
             wc.q_wait_ns = ix->warp_wait_ns;
             if (pass == 0) {
-                wc.n_big = std::min(kBigWarps, wc.n_warps / 8);
+                wc.n_big = std::min(n_big_max, wc.n_warps / 8);
                 if (big_chunks <= wc.arena_chunks) wc.n_big = 0;
                 while (wc.n_big > 0 && warp_ws_bytes(wc, ne) > budget) wc.n_big /= 2;
                 while (wc.arena_chunks > 1024 && warp_ws_bytes(wc, ne) > budget) wc.arena_chunks /= 2;

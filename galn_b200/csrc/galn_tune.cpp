@@ -6,8 +6,10 @@
 // best depth depends on the options (how many reads backtrack deeply) and on the index (how long
 // exact-match chains run), so it is measured: a sample of the job's reads is searched once per candidate
 // (layout x depth x block size) and the fastest device time wins. The layout (64 or 80 symbols per 32-byte
-// block) trades index size, which decides how much of it stays in L2, against popcounts per lookup. Results never depend on the choice; only speed
-// does. The table is keyed by the option block, so every parameter set has its own entry.
+// block) trades index size, which decides how much of it stays in L2, against popcounts per lookup. A second
+// stage, with that choice fixed, times the warp tier's stack arena per warp and its count of big-arena warps
+// (the warps that take reads outgrowing a small arena). Results never depend on the choice; only speed does.
+// The table is keyed by the option block, so every parameter set has its own entry.
 #include <string.h>
 
 #include <algorithm>
@@ -42,38 +44,78 @@ extern "C" int galn_autotune(galn_index *ix, const galn_opts *o, const galn_read
     static const int caps[] = {256, 512, 1024, 2048, 4096};
     static const int blocks[] = {128, 256};
     static const int layouts[] = {64, 80};
+    // the warp tier's arena per warp (64-entry chunks) and its count of big-arena warps, timed with the
+    // first stage's choice
+    static const int arenas[] = {2048, 8192, 16384};
+    static const int bigs[] = {64, 128, 256};
     const int saved_cap = ix->t0_cap, saved_block = ix->t0_block, saved_occ = ix->occ;
+    const int saved_arena = ix->warp_arena, saved_big = ix->warp_big;
     const bool saved_stats = ix->keep_stats;
     ix->keep_stats = false;
-    int bc = saved_cap, bb = saved_block, bo = saved_occ;
+    int bc = saved_cap, bb = saved_block, bo = saved_occ, ba = saved_arena, bg = saved_big;
     double bms = 1e300;
     int rc = 0;
+    auto time_one = [&](double &ms) {
+        ix->tune_active = true;
+        galn_results res;
+        memset(&res, 0, sizeof(res));
+        int r = run_job(ix, ix->main, o, &s, GALN_ENGINE_PERSISTENT, &res);
+        ix->tune_active = false;
+        if (r) return r;
+        galn_results_free(&res);
+        ms = ix->main.last.ms_device;
+        return 0;
+    };
     for (int occ : layouts)
         for (int cap : caps)
             for (int blk : blocks) {
+                if (rc) break;
                 ix->t0_cap = cap;
                 ix->t0_block = blk;
                 ix->occ = occ;
-                ix->tune_active = true;
-                galn_results res;
-                memset(&res, 0, sizeof(res));
-                rc = run_job(ix, ix->main, o, &s, GALN_ENGINE_PERSISTENT, &res);
-                ix->tune_active = false;
-                if (rc) break;
-                galn_results_free(&res);
-                double ms = ix->main.last.ms_device;
-                if (ms < bms) { bms = ms; bc = cap; bb = blk; bo = occ; }
+                double ms = 0;
+                rc = time_one(ms);
+                if (!rc && ms < bms) { bms = ms; bc = cap; bb = blk; bo = occ; }
             }
+    ix->t0_cap = bc;
+    ix->t0_block = bb;
+    ix->occ = bo;
+    for (int ar : arenas)
+        for (int bg2 : bigs) {
+            if (rc) break;
+            ix->warp_arena = ar;
+            ix->warp_big = bg2;
+            double ms = 0;
+            rc = time_one(ms);
+            if (!rc && ms < bms) { bms = ms; ba = ar; bg = bg2; }
+        }
     ix->t0_cap = saved_cap;
     ix->t0_block = saved_block;
     ix->occ = saved_occ;
+    ix->warp_arena = saved_arena;
+    ix->warp_big = saved_big;
     ix->keep_stats = saved_stats;
     if (rc) return rc;
-    ix->tuned[opts_key(o)] = galn_index::TuneChoice{bc, bb, bo};
+    ix->tuned[opts_key(o)] = galn_index::TuneChoice{bc, bb, bo, ba, bg};
     if (best_cap) *best_cap = bc;
     if (best_block) *best_block = bb;
     if (best_occ) *best_occ = bo;
     if (best_ms) *best_ms = bms;
+    return 0;
+}
+
+extern "C" int galn_autotune_choice(galn_index *ix, const galn_opts *o, int *cap, int *block, int *occ,
+                                    int *warp_arena, int *warp_big)
+{
+    if (!ix || !o) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    auto it = ix->tuned.find(opts_key(o));
+    if (it == ix->tuned.end()) return GALN_EINVAL;
+    if (cap) *cap = it->second.cap;
+    if (block) *block = it->second.block;
+    if (occ) *occ = it->second.occ;
+    if (warp_arena) *warp_arena = it->second.arena;
+    if (warp_big) *warp_big = it->second.big;
     return 0;
 }
 

@@ -297,11 +297,15 @@ int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, in
 
 /* The autotuner (no reference counterpart): times the first max_sample reads (0: all) once per candidate
  * occurrence layout (64 or 80 symbols per 32-byte block), first-tier stack depth (256..4096 entries: the
- * split between thread-per-read and warp-per-read) and block size, and keeps the fastest for this option
- * set; later searches with the same options use it. Returns the choice and its device milliseconds.
- * galn_autotune_clear forgets all choices. */
+ * split between thread-per-read and warp-per-read) and block size, then, with that choice, once per warp-tier
+ * arena per warp (2048..16384 chunks of 64 entries) and count of big-arena warps (64..256), and keeps the
+ * fastest for this option set; later searches with the same options use it. Returns the first stage's
+ * choice and the best device milliseconds; galn_autotune_choice gives the whole choice for an option set
+ * (GALN_EINVAL if it has none). galn_autotune_clear forgets all choices. */
 int galn_autotune(galn_index *ix, const galn_opts *o, const galn_reads *in, int max_sample, int *best_cap,
                   int *best_block, int *best_occ, double *best_ms);
+int galn_autotune_choice(galn_index *ix, const galn_opts *o, int *cap, int *block, int *occ, int *warp_arena,
+                         int *warp_big);
 int galn_autotune_clear(galn_index *ix);
 
 /* How many of the last run's kernel launches went through a CUDA graph (no reference counterpart). */
