@@ -115,6 +115,8 @@ def lib():
     L.galn_fasta_to_pac.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_uint64)]
     L.galn_gather_peak.argtypes = [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_double)]
     L.galn_index_set_warp_wait.argtypes = [vp, C.c_int64]
+    L.galn_index_set_fused.argtypes = [vp, C.c_int]
+    L.galn_last_run_fused.argtypes = [vp, C.POINTER(C.c_int)]
     L.galn_index_occ.argtypes = [vp, C.c_int, vp, C.c_int64, vp, vp]
     L.galn_stack_need.argtypes = [vp, C.POINTER(Options), C.POINTER(_Reads), C.POINTER(C.c_uint64)]
     L.galn_server_memory.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
@@ -183,6 +185,11 @@ class Index:
     def set_warp_tier(self, on: bool, arena_chunks: int = 1 << 13):
         if lib().galn_index_set_warp_tier(self.h, int(on), arena_chunks):
             raise GalnError("bad warp tier setting")
+
+    def set_fused(self, on: bool):
+        """The persistent engine's first and warp tiers as one launch (galn_index_set_fused; on by default)."""
+        if lib().galn_index_set_fused(self.h, int(on)):
+            raise GalnError("bad fused setting")
 
     def set_warp_wait(self, wait_ns: int):
         """How long a big-arena warp waits for queued reads (galn_index_set_warp_wait; default 2 s)."""
@@ -283,8 +290,10 @@ class Index:
                                          fetch.ctypes.data if n else None, tier.ctypes.data if n else None, n)
         if rc:
             raise GalnError(f"no profile ({rc})")
+        fused = C.c_int(0)
+        lib().galn_last_run_fused(self.h, C.byref(fused))
         out = dict(ms_device=dev.value, ms_tier=list(tiers), tier_reads=treads.tolist(),
-                   tier_threads=tthreads.tolist())
+                   tier_threads=tthreads.tolist(), fused=bool(fused.value))
         if n:
             out["fetch"] = fetch[:n]
             out["tier"] = tier[:n]

@@ -225,7 +225,22 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     // reads ordered by batch (stable): each batch is one contiguous segment of the list
     std::vector<int> bstart((size_t)n_batches + 1, 0);
     for (int b = 0; b < n_batches; ++b) bstart[(size_t)b + 1] = bstart[(size_t)b] + bcount[(size_t)b];
-    if (sorted) {
+    // the fused launch (first tier and warp tier in one launch) for the persistent engine when the warp tier
+    // can run: its first tier claims the reads longest expected search first (max_diff, then length), so that
+    // heavy reads reach the warp tier early; results do not depend on the order
+    const bool use_fused = engine == GALN_ENGINE_PERSISTENT && ix->use_fused && ix->use_warp && !wide && n > 0;
+    if (use_fused) {
+        const int kL = kWarpMaxLen + 1, nkey = 126 * kL;
+        auto key = [&](int r) {
+            const int md = std::min(std::max(h_md[r], 0), 125);
+            const int len = (int)std::min<int64_t>(in->offset[r + 1] - in->offset[r], kWarpMaxLen);
+            return (125 - md) * kL + (kWarpMaxLen - len);   // ascending key = descending (max_diff, length)
+        };
+        std::vector<int32_t> cnt((size_t)nkey + 1, 0);
+        for (int r = 0; r < n; ++r) ++cnt[(size_t)key(r) + 1];
+        for (int k = 0; k < nkey; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];
+        for (int r = 0; r < n; ++r) h_list[cnt[(size_t)key(r)]++] = r;
+    } else if (sorted) {
         par([&](int r0, int r1, int) { for (int r = r0; r < r1; ++r) h_list[r] = r; });
     } else {
         std::vector<int> fill(bstart.begin(), bstart.end() - 1);
@@ -279,7 +294,7 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     ECK(cudaEventCreate(&e0));
     ECK(cudaEventCreate(&e1));
     float k_ms = 0;
-    RCK(B.h_misc.ensure(64));
+    RCK(B.h_misc.ensure(256));   // counters and queue words (16 ints), then the warp counters at byte 128
     int32_t *h_cnt = (int32_t *)B.h_misc.p;
 
     // run one tier over list[0..m) with overflow going to ovf; returns the overflow count
@@ -358,7 +373,137 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
         auto it = ix->tuned.find(opts_key(&sets[0]));
         if (it != ix->tuned.end()) { t0.cap = it->second.cap; t0.block = it->second.block; }
     }
-    if (engine == GALN_ENGINE_PERSISTENT) {
+    // the warp tier's arena per warp and its big-arena warps: the autotuner's for this option set, else the
+    // index's
+    int arena = ix->warp_arena, n_big_max = ix->warp_big;
+    if (!ix->tune_active) {
+        auto it = ix->tuned.find(opts_key(&sets[0]));
+        if (it != ix->tuned.end() && it->second.arena > 0) { arena = it->second.arena; n_big_max = it->second.big; }
+    }
+    // the cut-off, one wave's staged pushes and a partly filled chunk per bucket
+    const int64_t full_chunks = (max_entries_all + 16 + 3 * 32 * 128 + kWarpMaxStacks * kWarpChunk) / kWarpChunk
+                                + kWarpMaxStacks + 1;
+    const int big_chunks = (int)std::min<int64_t>(std::max<int64_t>(full_chunks, arena), 1 << 22);
+    const int aln_cap_w = 4096;
+    const bool warp_ok = ix->use_warp && !wide && engine != GALN_ENGINE_PLAIN;
+    unsigned long long *h_dbg = (unsigned long long *)((char *)B.h_misc.p + 128);
+    bool fused = false;
+    std::vector<int32_t> elig, rest;     // reads for the warp tier's next pass, and for the thread tiers
+    if (use_fused) {
+        // one persistent launch of both tiers: blocks of kFusedWarps warps, as many as stay resident; a quarter
+        // of them are warp-tier warps from the start, the others run the first tier first
+        const int grid = fused_resident_blocks(ix->dev.device);
+        if (grid <= 0) return GALN_ECUDA;
+        const int n_w_blocks = std::max(1, grid / 4);
+        TierCfg ft = t0;
+        ft.persistent = true;
+        ft.threads = (grid - n_w_blocks) * kFusedWarps * 32;
+        ft.block = kFusedWarps * 32;
+        WarpCfg wc;
+        wc.n_warps = grid * kFusedWarps;
+        wc.aln_cap = aln_cap_w;
+        wc.arena_chunks = arena;
+        wc.big_chunks = big_chunks;
+        wc.q_wait_ns = ix->warp_wait_ns;
+        wc.n_big = big_chunks > arena ? std::min(n_big_max, n_w_blocks * kFusedWarps) : 0;
+        while (wc.n_big > 0 && fused_ws_bytes(ft, job, wc, n) > budget) wc.n_big /= 2;
+        while (wc.arena_chunks > 1024 && fused_ws_bytes(ft, job, wc, n) > budget) wc.arena_chunks /= 2;
+        if (fused_ws_bytes(ft, job, wc, n) <= budget) {
+            RCK(B.ws.ensure(fused_ws_bytes(ft, job, wc, n)));
+            unsigned long long *dbg = nullptr;
+            if (ix->keep_stats) {
+                RCK(B.dbg.ensure(kWarpDbg * 8));
+                dbg = (unsigned long long *)B.dbg.p;
+            }
+            FusedQueues fq;
+            fused_queues(ft, job, wc, n, B.ws.p, fq);
+            // counters, timing events, the launch and the read-back of its counters and queue control words,
+            // captured once as a CUDA graph and updated in place when only parameters change
+            auto record = [&]() -> int {
+                if (cudaMemsetAsync(job.counters, 0, 64, st) != cudaSuccess) return GALN_ECUDA;
+                if (dbg && cudaMemsetAsync(dbg, 0, kWarpDbg * 8, st) != cudaSuccess) return GALN_ECUDA;
+                if (cudaEventRecordWithFlags(e0, st, cudaEventRecordExternal) != cudaSuccess) return GALN_ECUDA;
+                int lrc = dev_search_fused(ix->dev, job, ft, wc, n_w_blocks, cur, n, nxt, B.ws.p, st, dbg);
+                if (lrc) return lrc;
+                if (cudaEventRecordWithFlags(e1, st, cudaEventRecordExternal) != cudaSuccess) return GALN_ECUDA;
+                if (cudaMemcpyAsync(h_cnt, job.counters, 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                    cudaMemcpyAsync(h_cnt + 4, fq.hq_ctl, 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                    cudaMemcpyAsync(h_cnt + 8, fq.q_ctl, 16, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+                    return GALN_ECUDA;
+                if (dbg && cudaMemcpyAsync(h_dbg, dbg, kWarpDbg * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+                    return GALN_ECUDA;
+                return 0;
+            };
+            if (ix->use_graph) {
+                cudaGraph_t g = nullptr;
+                ECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                const int lrc = record();
+                cudaError_t ce = cudaStreamEndCapture(st, &g);
+                if (lrc || ce != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return lrc ? lrc : GALN_ECUDA; }
+                bool updated = false;
+                if (ctx.fused_exec) {
+                    cudaGraphExecUpdateResultInfo info;
+                    updated = cudaGraphExecUpdate(ctx.fused_exec, g, &info) == cudaSuccess;
+                    if (!updated) { cudaGetLastError(); cudaGraphExecDestroy(ctx.fused_exec); ctx.fused_exec = nullptr; }
+                }
+                if (!updated && cudaGraphInstantiate(&ctx.fused_exec, g, 0) != cudaSuccess) {
+                    cudaGraphDestroy(g);
+                    ctx.fused_exec = nullptr;
+                    return GALN_ECUDA;
+                }
+                cudaGraphDestroy(g);
+                ECK(cudaGraphLaunch(ctx.fused_exec, st));
+                S.graph_launches += 1;
+            } else {
+                RCK(record());
+            }
+            ECK(cudaStreamSynchronize(st));
+            float ms = 0;
+            ECK(cudaEventElapsedTime(&ms, e0, e1));
+            k_ms += ms;
+            S.ms_tier[0] += ms;
+            S.kernel_launches += 1;
+            S.fused = true;
+            S.tier_threads[0] = ft.threads;
+            S.tier_threads[1] = (int64_t)wc.n_warps * 32;
+            S.tier_reads[0] += n;
+            if (dbg)
+                for (int q = 0; q < kWarpDbg; ++q) S.warp_dbg[q] = h_dbg[q];
+            // what the launch left: the first tier's overflow the warp tier cannot take, the warp tier's
+            // overflow, and reads still queued (all that were ever queued when a slot was lost)
+            const int t0_ovf = h_cnt[1], w_ovf = h_cnt[3];
+            const int hq_head = h_cnt[4], hq_tail = h_cnt[5], hq_lost = h_cnt[7];
+            const int bq_head = h_cnt[8], bq_tail = h_cnt[9], bq_lost = h_cnt[11];
+            S.overflow_reads[0] = t0_ovf;
+            S.tier_reads[1] += hq_tail;
+            S.warp_queued = (int64_t)bq_tail + hq_tail;
+            S.warp_gave_up = (hq_lost || bq_lost) ? 1 : 0;
+            const int hq_from = hq_lost ? 0 : std::min(hq_head, hq_tail);
+            const int bq_from = bq_lost ? 0 : std::min(bq_head, bq_tail);
+            const int n_hq = std::max(0, hq_tail - hq_from), n_bq = wc.n_big > 0 ? std::max(0, bq_tail - bq_from) : 0;
+            rest.resize((size_t)t0_ovf);
+            elig.resize((size_t)w_ovf + n_hq + n_bq);
+            if (t0_ovf) ECK(cudaMemcpyAsync(rest.data(), nxt, (size_t)t0_ovf * 4, cudaMemcpyDeviceToHost, st));
+            if (w_ovf) ECK(cudaMemcpyAsync(elig.data(), fq.w_ovf, (size_t)w_ovf * 4, cudaMemcpyDeviceToHost, st));
+            if (n_hq) ECK(cudaMemcpyAsync(elig.data() + w_ovf, fq.hq + hq_from, (size_t)n_hq * 4, cudaMemcpyDeviceToHost, st));
+            if (n_bq)
+                ECK(cudaMemcpyAsync(elig.data() + w_ovf + n_hq, fq.big_slots + bq_from, (size_t)n_bq * 4,
+                                    cudaMemcpyDeviceToHost, st));
+            ECK(cudaStreamSynchronize(st));
+            for (int32_t r : rest)
+                if (r < 0 || r >= n) return GALN_ECUDA;
+            for (int32_t r : elig)
+                if (r < 0 || r >= n) return GALN_ECUDA;   // a slot written by no warp
+            if (hq_lost || bq_lost) {   // a read may be both queued and in an overflow list
+                std::sort(elig.begin(), elig.end());
+                elig.erase(std::unique(elig.begin(), elig.end()), elig.end());
+            }
+            fused = true;
+        }
+    }
+    if (fused) {
+        // the warp tier's second pass and the thread tiers follow
+    } else if (engine == GALN_ENGINE_PERSISTENT) {
         t0.persistent = true;
         RCK(run_tier(t0, cur, n, nxt, &n_ovf));
     } else {
@@ -383,21 +528,23 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
         }
         n_ovf = acc;
     }
-    S.overflow_reads[0] = n_ovf;
+    if (!fused) S.overflow_reads[0] = n_ovf;
     std::swap(cur, nxt);
 
-    // ---- W: the warp tier for the reads that overflowed T0 (those it can take) ----
-    const bool warp_ok = ix->use_warp && !wide && engine != GALN_ENGINE_PLAIN;
-    if (warp_ok && n_ovf > 0) {
-        std::vector<int32_t> ov((size_t)n_ovf), elig, rest;
-        ECK(cudaMemcpyAsync(ov.data(), cur, (size_t)n_ovf * 4, cudaMemcpyDeviceToHost, st));
-        ECK(cudaStreamSynchronize(st));
-        for (int32_t r : ov) {
-            int len = (int)(in->offset[r + 1] - in->offset[r]);
-            const HostBatchOpt &h = bopt[bid[r]];
-            if (len <= kWarpMaxLen && h.n_stacks <= kWarpMaxStacks && h.n_stacks > 0 && h.s_mm > 0 && h.s_gapo > 0 &&
-                h.s_gape > 0) elig.push_back(r);
-            else rest.push_back(r);
+    // ---- W: the warp tier for the reads that overflowed T0 (those it can take); after the fused launch,
+    // its second pass for what that launch left ----
+    if (warp_ok && (fused || n_ovf > 0)) {
+        if (!fused) {
+            std::vector<int32_t> ov((size_t)n_ovf);
+            ECK(cudaMemcpyAsync(ov.data(), cur, (size_t)n_ovf * 4, cudaMemcpyDeviceToHost, st));
+            ECK(cudaStreamSynchronize(st));
+            for (int32_t r : ov) {
+                int len = (int)(in->offset[r + 1] - in->offset[r]);
+                const HostBatchOpt &h = bopt[bid[r]];
+                if (len <= kWarpMaxLen && h.n_stacks <= kWarpMaxStacks && h.n_stacks > 0 && h.s_mm > 0 &&
+                    h.s_gapo > 0 && h.s_gape > 0) elig.push_back(r);
+                else rest.push_back(r);
+            }
         }
         // longest expected searches first (max_diff, then length), so that the heaviest reads do not start
         // last and run alone at the end of the launch; results do not depend on the order. A counting sort:
@@ -416,20 +563,10 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
             elig.swap(sorted);
         }
         // pass 1: the tuned arena per warp, plus up to n_big_max warps whose arenas hold the max_entries
-        // cut-off and take over, in the same launch, the reads that outgrow the small ones; pass 2, only for
-        // reads still queued when pass 1 ended, with big arenas for every warp
-        const int aln_cap_w = 4096;
-        // the arena per warp and the big-arena warps: the autotuner's for this option set, else the index's
-        int arena = ix->warp_arena, n_big_max = ix->warp_big;
-        if (!ix->tune_active) {
-            auto it = ix->tuned.find(opts_key(&sets[0]));
-            if (it != ix->tuned.end() && it->second.arena > 0) { arena = it->second.arena; n_big_max = it->second.big; }
-        }
-        // the cut-off, one wave's staged pushes and a partly filled chunk per bucket
-        const int64_t full = (max_entries_all + 16 + 3 * 32 * 128 + kWarpMaxStacks * kWarpChunk) / kWarpChunk
-                             + kWarpMaxStacks + 1;
-        const int big_chunks = (int)std::min<int64_t>(std::max<int64_t>(full, arena), 1 << 22);
-        for (int pass = 0; pass < 2 && !elig.empty(); ++pass) {
+        // cut-off and take over, in the same launch, the reads that outgrow the small ones (the fused launch
+        // is this pass); pass 2, only for reads still queued or not finished when pass 1 ended, with big
+        // arenas for every warp
+        for (int pass = fused ? 1 : 0; pass < 2 && !elig.empty(); ++pass) {
             int ne = (int)elig.size();
             int res_w = warp_resident(ix->dev.device);
             if (res_w <= 0) return GALN_ECUDA;
@@ -731,6 +868,22 @@ extern "C" int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks
     std::lock_guard<std::mutex> lk(ix->mu);
     ix->use_warp = on != 0;
     ix->warp_arena = arena_chunks;
+    return 0;
+}
+
+extern "C" int galn_index_set_fused(galn_index *ix, int on)
+{
+    if (!ix) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    ix->use_fused = on != 0;
+    return 0;
+}
+
+extern "C" int galn_last_run_fused(galn_index *ix, int *fused)
+{
+    if (!ix || !fused) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    *fused = ix->main.last.fused ? 1 : 0;
     return 0;
 }
 

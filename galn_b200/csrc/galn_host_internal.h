@@ -67,6 +67,7 @@ struct RunStats {
     int64_t kernel_launches = 0;
     int64_t graph_launches = 0;      // of those, launched through a CUDA graph
     uint64_t warp_dbg[16] = {};      // warp-tier counters (keep_stats runs)
+    bool fused = false;              // the first tier and the warp tier ran as one launch (ms_tier[0])
     int64_t warp_queued = 0;         // reads the warp tier's first pass queued for its big-arena warps
     int warp_gave_up = 0;            // a big warp's bounded wait ran out in the first pass
     std::vector<uint32_t> fetch;     // per read, of the last run
@@ -80,10 +81,12 @@ struct ExecCtx {
     RunStats last;
     double mem_share = 1.0;            // of the budget this context's workspace may take
     cudaGraphExec_t graph_exec = nullptr;   // the persistent first-tier launch, captured
+    cudaGraphExec_t fused_exec = nullptr;   // the fused launch of the first and warp tiers, captured
     int l2_occ = 0;                    // the layout the stream's persisting L2 window covers (0: none set)
     void release()
     {
         if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+        if (fused_exec) { cudaGraphExecDestroy(fused_exec); fused_exec = nullptr; }
         ws.release();
     }
 };
@@ -109,6 +112,7 @@ struct galn_index {
     int occ = 64;                       // occurrence layout when the autotuner has no choice (64 or 80)
     bool tune_active = false;           // the autotuner is timing a candidate: ignore the table
     bool use_graph = true;              // launch the persistent first tier through a CUDA graph
+    bool use_fused = true;              // the persistent engine's first and warp tiers in one launch
     int warp_arena = 1 << 13;           // chunks (kWarpChunk entries) per warp
     int warp_big = 128;                 // warps of a warp-tier launch whose arenas hold the max_entries cut-off
     uint64_t warp_wait_ns = 2000000000ull;   // a big warp's bounded wait for queued work

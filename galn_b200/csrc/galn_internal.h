@@ -110,6 +110,22 @@ size_t warp_ws_bytes(const WarpCfg &c, int n);
 constexpr int kWarpDbg = 15;   // counters of the warp tier when profiling is on
 int dev_search_warp(const DevIndex &ix, DevJob &job, const WarpCfg &c, int tier, const int32_t *list, int n,
                     int32_t *ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg);
+// The fused launch: the first tier (t0: its slots, cap, records, block of kFusedWarps warps) and the warp tier
+// (c: c.n_warps warps in all, n_w_blocks blocks of them warp-tier warps from the start, the big-arena warps
+// among those) in one persistent launch; heavy reads pass from the first to the warp tier through a device
+// queue. Reads the first tier cannot hand over go to t0_ovf (count in job.counters[1]); reads the warp tier
+// cannot finish to the overflow list in FusedQueues (count in job.counters[3]); reads left in the queues are
+// read back from FusedQueues (control words: 0 head, 1 tail, 3 a slot was lost).
+constexpr int kFusedWarps = 8;
+struct FusedQueues {
+    int32_t *hq = nullptr, *hq_ctl = nullptr, *w_ovf = nullptr, *q_ctl = nullptr, *big_slots = nullptr;
+};
+size_t fused_smem_bytes();
+int fused_resident_blocks(int device);
+size_t fused_ws_bytes(const TierCfg &t0, const DevJob &job, const WarpCfg &c, int n);
+void fused_queues(const TierCfg &t0, const DevJob &job, const WarpCfg &c, int n, void *ws_mem, FusedQueues &q);
+int dev_search_fused(const DevIndex &ix, DevJob &job, const TierCfg &t0, const WarpCfg &c, int n_w_blocks,
+                     const int32_t *list, int n, int32_t *t0_ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg);
 // bwt_sa for n rows d_k (d_ref_len NULL: the forward-reverse coordinate into d_pos) or bwa_sa2pos (with
 // d_ref_len: position and strand, ~0 for a hit across the forward/reverse boundary)
 int dev_sa_walk(const DevIndex &ix, const uint64_t *d_samples, uint64_t intv, const uint64_t *d_k, int64_t n,

@@ -238,6 +238,10 @@ struct KArgs {
     int64_t rec_cap;
     int32_t *ovf;
     int32_t *ovf_n;
+    // the fused launch: reads that overflow this tier and that the warp tier can take go to this queue
+    // (hq_tail counts reserved slots) instead of ovf; NULL otherwise
+    int32_t *hq;
+    int32_t *hq_tail;
 };
 
 template <bool WIDE, bool FREELIST, bool TRACE, int S>
@@ -267,13 +271,22 @@ __device__ __forceinline__ void run_read(const KArgs &a, int pos, int slot)
             a.out_off[r] = (int64_t)o;
         }
     }
-    if (ret == kErrStack || ret == kErrAln) a.ovf[atomicAdd(a.ovf_n, 1)] = r;
     a.out_n[r] = ret;
     a.out_pops[r] = R.pops;
     a.out_trace[r] = R.trace;
     a.out_peak[r] = R.peak;
     a.out_fetch[r] = R.fetches;
     a.out_tier[r] = (int8_t)a.tier;
+    if (ret == kErrStack || ret == kErrAln) {
+        // this tier's outputs are written before the read is handed on, so a warp that takes it from the
+        // queue writes its own after them
+        if (!WIDE && a.hq && len <= kWarpMaxLen && bo.n_stacks > 0 && bo.n_stacks <= kWarpMaxStacks && bo.s_mm > 0 &&
+            bo.s_gapo > 0 && bo.s_gape > 0) {
+            __threadfence();
+            const int q = atomicAdd(a.hq_tail, 1);
+            atomicExch(a.hq + q, r);
+        } else a.ovf[atomicAdd(a.ovf_n, 1)] = r;
+    }
 }
 
 template <bool WIDE, bool FREELIST, bool TRACE, int S>
@@ -781,6 +794,277 @@ int dev_search_warp(const DevIndex &ix, DevJob &job, const WarpCfg &c, int tier,
     } else {
         if (job.trace) warp_kernel<true, kOcc64><<<n_warps, 32, smem, st>>>(a);
         else warp_kernel<false, kOcc64><<<n_warps, 32, smem, st>>>(a);
+    }
+    GALN_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// The fused launch: the first tier and the warp tier in one persistent launch. Blocks of kFWarps warps; the
+// first n_w_blocks blocks are warp-tier warps from the start, the others run the first tier (one read per
+// thread, claimed from the list) and then become warp-tier warps too. A read that overflows the first tier
+// and that the warp tier can take is handed over at once through the heavy queue (hq), so heavy reads start
+// while light ones are still being searched. Every wait is bounded (w.q_wait_ns): a warp that gives up
+// leaves its reads to the host's next pass, and a lost queue slot is flagged (hq_ctl[3]) so that the host
+// searches every queued read again; results never depend on any of it.
+constexpr int kFWarps = kFusedWarps;
+
+struct FArgs {
+    KArgs t;                 // the first tier; t.hq / t.hq_tail point into hq / hq_ctl
+    WArgs w;                 // the warp tier (w.list, w.n and w.claim are unused: reads come from hq)
+    int n_w_blocks;          // blocks that are warp-tier warps from the start (they come first)
+    int32_t *hq;             // heavy queue: read ids, -1 until written
+    int32_t *hq_ctl;         // 0 head (claimed), 1 tail (reserved), 2 first-tier warps still running, 3 a slot was lost
+};
+
+// takes slot `h` of a queue whose producers reserve a slot and then write the read id into it
+__device__ __forceinline__ int queue_take(int32_t *q, int h, uint64_t t0, uint64_t wait, int32_t *lost)
+{
+    for (;;) {
+        const int r = atomicAdd(q + h, 0);
+        if (r >= 0) { __threadfence(); return r; }
+        if (gtimer_ns() - t0 > wait) { atomicExch(lost, 1); return -1; }
+        __nanosleep(100);
+    }
+}
+
+// a small warp's next read (lane 0): the next heavy read; -1 once the first tier has finished and the queue
+// is empty, or when the first tier has shown no progress (reads claimed, reads queued, warps finished) for
+// w.q_wait_ns
+__device__ __noinline__ int heavy_next(const FArgs &f)
+{
+    volatile int32_t *hc = f.hq_ctl;
+    volatile int32_t *claim = f.t.claim;
+    uint64_t t0 = gtimer_ns();
+    int seen_t = hc[1], seen_w = hc[2], seen_c = *claim;
+    for (;;) {
+        const int h = hc[0], t = hc[1];
+        if (h < t) {
+            if (atomicCAS(f.hq_ctl, h, h + 1) == h) return queue_take(f.hq, h, gtimer_ns(), f.w.q_wait_ns, f.hq_ctl + 3);
+            continue;
+        }
+        const int w = hc[2], c = *claim;
+        if (w == 0) {
+            __threadfence();
+            if (hc[0] >= hc[1]) return -1;
+            continue;
+        }
+        const uint64_t now = gtimer_ns();
+        if (t != seen_t || w != seen_w || c != seen_c) { seen_t = t; seen_w = w; seen_c = c; t0 = now; }
+        else if (now - t0 > f.w.q_wait_ns) {               // reads queued later go to the host's next pass
+            if (f.w.q_wait_ns == 0) atomicExch(f.hq_ctl + 3, 1);
+            return -1;
+        }
+        __nanosleep(1000);
+    }
+}
+
+// a big warp's next read (lane 0): one that outgrew a small arena first, else a heavy read; -1 once every
+// small warp has finished and both queues are empty, or after a wait of w.q_wait_ns
+__device__ __noinline__ int fused_big_next(const FArgs &f)
+{
+    volatile int32_t *qc = f.w.q_ctl;
+    volatile int32_t *hc = f.hq_ctl;
+    const int n_small = f.w.n_warps - f.w.n_big;
+    const uint64_t t0 = gtimer_ns();
+    for (;;) {
+        const int h = qc[0], t = qc[1];
+        if (h < t) {
+            if (atomicCAS(f.w.q_ctl, h, h + 1) == h)
+                return queue_take(f.w.ovq, h, gtimer_ns(), f.w.q_wait_ns, f.w.q_ctl + 3);
+            continue;
+        }
+        const int h2 = hc[0], t2 = hc[1];
+        if (h2 < t2) {
+            if (atomicCAS(f.hq_ctl, h2, h2 + 1) == h2)
+                return queue_take(f.hq, h2, gtimer_ns(), f.w.q_wait_ns, f.hq_ctl + 3);
+            continue;
+        }
+        if (qc[2] == n_small) {
+            __threadfence();
+            if (qc[0] >= qc[1]) return -1;
+            continue;
+        }
+        if (gtimer_ns() - t0 > f.w.q_wait_ns) {
+            if (f.w.q_wait_ns == 0) atomicExch(f.w.q_ctl + 3, 1);
+            return -1;
+        }
+        __nanosleep(1000);
+    }
+}
+
+template <bool TRACE, int ST>
+__global__ void __launch_bounds__(kFWarps * 32, 2) fused_kernel(const __grid_constant__ FArgs f)
+{
+    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpSmem *S = reinterpret_cast<WarpSmem *>(fsm_raw) + wib;
+    const int wid = blockIdx.x * kFWarps + wib;
+    if ((int)blockIdx.x >= f.n_w_blocks) {
+        const int slot = ((int)blockIdx.x - f.n_w_blocks) * kFWarps * 32 + threadIdx.x;
+        if (slot < f.t.n_slots) {
+            for (;;) {
+                const int pos = atomicAdd(f.t.claim, 1);
+                if (pos >= f.t.n) break;
+                run_read<false, false, TRACE, ST>(f.t, pos, slot);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence();
+            atomicSub(f.hq_ctl + 2, 1);
+        }
+    }
+    const bool big = wid < f.w.n_big;
+    for (;;) {
+        int r = -1;
+        if (lane == 0) r = big ? fused_big_next(f) : heavy_next(f);
+        r = __shfl_sync(0xffffffffu, r, 0);
+        if (r < 0) break;
+        warp_read<TRACE, ST>(f.w, r, wid, S, lane);
+    }
+    if (!big && f.w.n_big > 0 && lane == 0) {
+        __threadfence();
+        atomicAdd(f.w.q_ctl + 2, 1);
+    }
+}
+
+__global__ void fused_init_kernel(int32_t *hq_ctl, int32_t *q_ctl, int t0_warps)
+{
+    if (threadIdx.x < 4) {
+        hq_ctl[threadIdx.x] = threadIdx.x == 2 ? t0_warps : 0;
+        q_ctl[threadIdx.x] = 0;
+    }
+}
+
+size_t fused_smem_bytes() { return (size_t)kFWarps * sizeof(WarpSmem); }
+
+// blocks of the fused kernel resident per SM (its registers and shared memory allow)
+int fused_resident_blocks(int device)
+{
+    const void *fns[4] = {(const void *)fused_kernel<false, kOcc64>, (const void *)fused_kernel<true, kOcc64>,
+                          (const void *)fused_kernel<false, kOcc80>, (const void *)fused_kernel<true, kOcc80>};
+    int bps = 1 << 30;
+    for (const void *fn : fns) {
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes()) != cudaSuccess)
+            return -22;
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kFWarps * 32, fused_smem_bytes()) != cudaSuccess)
+            return -22;
+        bps = std::min(bps, b);
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return bps * sms;
+}
+
+// workspace: the first tier's (t0.threads slots), the warp tier's (c.n_warps warps), the heavy queue (n slots)
+// and its control words, and the warp tier's overflow list (n slots)
+struct FusedLayout {
+    size_t t0, warp, hq, hq_ctl, w_ovf, total;
+};
+
+static FusedLayout fused_layout(const TierCfg &t0, const DevJob &job, const WarpCfg &c, int n)
+{
+    FusedLayout L;
+    size_t o = 0;
+    L.t0 = o;     o += align256(ws_bytes(t0, job));
+    L.warp = o;   o += align256(warp_ws_bytes(c, n));
+    L.hq = o;     o += align256((size_t)std::max(n, 1) * 4);
+    L.hq_ctl = o; o += 256;
+    L.w_ovf = o;  o += align256((size_t)std::max(n, 1) * 4);
+    L.total = o;
+    return L;
+}
+
+size_t fused_ws_bytes(const TierCfg &t0, const DevJob &job, const WarpCfg &c, int n)
+{
+    return fused_layout(t0, job, c, n).total;
+}
+
+void fused_queues(const TierCfg &t0, const DevJob &job, const WarpCfg &c, int n, void *ws_mem, FusedQueues &q)
+{
+    const FusedLayout L = fused_layout(t0, job, c, n);
+    char *b = (char *)ws_mem;
+    q.hq = (int32_t *)(b + L.hq);
+    q.hq_ctl = (int32_t *)(b + L.hq_ctl);
+    q.w_ovf = (int32_t *)(b + L.w_ovf);
+    q.q_ctl = warp_queue(c, n, b + L.warp, &q.big_slots);
+}
+
+int dev_search_fused(const DevIndex &ix, DevJob &job, const TierCfg &t0, const WarpCfg &c, int n_w_blocks,
+                     const int32_t *list, int n, int32_t *t0_ovf, void *ws_mem, cudaStream_t st, unsigned long long *dbg)
+{
+    if (n == 0) return 0;
+    const int grid = c.n_warps / kFWarps;
+    if (c.n_warps % kFWarps || grid <= n_w_blocks || n_w_blocks < 0 || t0.threads != (grid - n_w_blocks) * kFWarps * 32 ||
+        c.n_big < 0 || c.n_big > n_w_blocks * kFWarps || (c.n_big > 0 && c.big_chunks < 1) || c.arena_chunks < 1 ||
+        job.any_wide)
+        return -20;
+    const FusedLayout L = fused_layout(t0, job, c, n);
+    char *base = (char *)ws_mem;
+    FArgs f;
+    memset(&f, 0, sizeof(f));
+    // the first tier
+    KArgs &a = f.t;
+    if (index_view(ix, job.occ, a.ix)) return -20;
+    a.query = job.query; a.off = job.off; a.bidx = job.bidx; a.maxdiff = job.maxdiff;
+    a.bopt = (const BatchOpt *)job.bopt; a.seed_len = job.seed_len;
+    a.list = list; a.n = n; a.persistent = 1; a.claim = job.counters;
+    a.n_slots = t0.threads;
+    size_t off[6];
+    ws_layout(t0, job, off);
+    char *tb = base + L.t0;
+    a.ws.ent = (uint4 *)(tb + off[0]);
+    a.ws.link = (int32_t *)(tb + off[1]);
+    a.ws.heads = (int32_t *)(tb + off[2]);
+    a.ws.wid = (uint64_t *)(tb + off[3]);
+    a.ws.aln = (uint64_t *)(tb + off[4]);
+    a.ws.cap = t0.cap; a.ws.hcap = job.max_stacks; a.ws.wcap = width_cap(job);
+    a.ws.aln_cap = t0.aln_cap;
+    a.out_n = job.out_n; a.out_off = job.out_off; a.out_pops = job.out_pops; a.out_trace = job.out_trace;
+    a.out_peak = job.out_peak; a.out_fetch = job.out_fetch; a.out_tier = job.out_tier; a.tier = 0;
+    a.trace = job.trace;
+    a.out_rec = job.out_rec; a.rec_top = job.rec_top; a.rec_cap = job.rec_cap;
+    a.ovf = t0_ovf; a.ovf_n = job.counters + 1;
+    f.hq = (int32_t *)(base + L.hq);
+    f.hq_ctl = (int32_t *)(base + L.hq_ctl);
+    a.hq = f.hq; a.hq_tail = f.hq_ctl + 1;
+    // the warp tier
+    WArgs &w = f.w;
+    w.ix = a.ix;
+    w.query = job.query; w.off = job.off; w.bidx = job.bidx; w.maxdiff = job.maxdiff;
+    w.bopt = a.bopt; w.seed_len = job.seed_len;
+    w.list = nullptr; w.n = 0; w.claim = job.counters + 2; w.n_warps = c.n_warps;
+    const WarpLayout WL = warp_layout(c, n);
+    char *wb = base + L.warp;
+    w.chunks = (uint4 *)(wb + WL.chunks);
+    w.chunk_prev = (int32_t *)(wb + WL.chunk_prev);
+    w.free_ids = (int32_t *)(wb + WL.free_ids);
+    w.aln = (uint64_t *)(wb + WL.aln);
+    w.stage = (uint4 *)(wb + WL.stage);
+    w.prec = (uint4 *)(wb + WL.prec);
+    w.side = (WSide *)(wb + WL.side);
+    w.q_ctl = (int32_t *)(wb + WL.q_ctl);
+    w.ovq = (int32_t *)(wb + WL.ovq);
+    w.n_big = c.n_big; w.big_chunks = c.big_chunks; w.q_wait_ns = c.q_wait_ns;
+    w.arena_chunks = c.arena_chunks; w.aln_cap = c.aln_cap;
+    w.out_n = job.out_n; w.out_off = job.out_off; w.out_pops = job.out_pops; w.out_trace = job.out_trace;
+    w.out_peak = job.out_peak; w.out_fetch = job.out_fetch; w.out_tier = job.out_tier; w.tier = 1;
+    w.out_rec = job.out_rec; w.rec_top = job.rec_top; w.rec_cap = job.rec_cap;
+    w.ovf = (int32_t *)(base + L.w_ovf); w.ovf_n = job.counters + 3;
+    w.dbg = dbg;
+    f.n_w_blocks = n_w_blocks;
+    GALN_CUDA(cudaMemsetAsync(f.hq, 0xff, (size_t)n * 4, st));
+    GALN_CUDA(cudaMemsetAsync(w.ovq, 0xff, (size_t)n * 4, st));
+    fused_init_kernel<<<1, 32, 0, st>>>(f.hq_ctl, w.q_ctl, (grid - n_w_blocks) * kFWarps);
+    const size_t smem = fused_smem_bytes();
+    if (job.occ == kOcc80) {
+        if (job.trace) fused_kernel<true, kOcc80><<<grid, kFWarps * 32, smem, st>>>(f);
+        else fused_kernel<false, kOcc80><<<grid, kFWarps * 32, smem, st>>>(f);
+    } else {
+        if (job.trace) fused_kernel<true, kOcc64><<<grid, kFWarps * 32, smem, st>>>(f);
+        else fused_kernel<false, kOcc64><<<grid, kFWarps * 32, smem, st>>>(f);
     }
     GALN_CUDA(cudaGetLastError());
     return 0;

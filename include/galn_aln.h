@@ -311,6 +311,16 @@ int galn_autotune_clear(galn_index *ix);
 /* How many of the last run's kernel launches went through a CUDA graph (no reference counterpart). */
 int galn_last_graph_launches(galn_index *ix, int64_t *graph_launches);
 
+/* The persistent engine's first tier and warp tier as one launch (no reference counterpart; on by default):
+ * blocks of 8 warps, as many as stay resident, a quarter of them warp-tier warps from the start and the
+ * others first-tier threads that turn into warp-tier warps when the first tier's reads run out; a read that
+ * overflows the first tier is handed to a warp at once through a device queue (the reference's light tier and
+ * warp phases hand reads over in the same way through its shared list, src/galn.cu:907-1180). Off, the tiers
+ * are two launches. Results never depend on it. galn_last_run_fused tells whether the last run used it
+ * (the launch's time is then ms_tier[0] of galn_last_run_profile). */
+int galn_index_set_fused(galn_index *ix, int on);
+int galn_last_run_fused(galn_index *ix, int *fused);
+
 /* Counters of the warp tier in the last keep_stats run (no reference counterpart): reads searched (with
  * re-runs), waves, entries expanded, entries replayed, pops, chains continued in the next wave, hits, SM
  * cycles in chains / replay / commit / wave loads (summed over warps), pops run (with dropped
@@ -346,8 +356,9 @@ int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks);
  * queued is searched again; results never depend on it. 0 makes every wait run out at once and takes the
  * second of those paths (a way to test it). */
 int galn_index_set_warp_wait(galn_index *ix, int64_t wait_ns);
-/* The last run's warp-tier queue (no reference counterpart): reads its first launch queued for the big-arena
- * warps, and whether a bounded wait ran out (then all of them were searched again). */
+/* The last run's warp-tier queues (no reference counterpart): reads its first launch queued for the big-arena
+ * warps (and, in the fused launch, from the first tier to the warp tier), and whether a lost queue slot
+ * made every queued read be searched again. */
 int galn_last_warp_queue(galn_index *ix, int64_t *queued, int *gave_up);
 
 /* The occurrence blocks in a persisting L2 access-policy window on the index's streams (no reference

@@ -84,6 +84,29 @@ def test_tier_migration_gives_same_bytes(caps, warp, trace, occ):
         assert st["tiers"] >= 2 or name in ("edge_nonstop", "tiny_queue")
 
 
+@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("trace", [True, False])
+def test_fused_and_two_launch_forms_give_same_bytes(fused, trace):
+    """The persistent engine with the first and warp tiers as one launch (heavy reads handed over through a
+    device queue while light ones run) and as two launches: the reference's bytes and the same pops, with a
+    tiny first tier so that most reads cross over."""
+    ix = galn_b200.Index(os.path.join(GOLDEN, "small", "ref"))
+    ix.set_fused(fused)
+    ix.set_trace(trace)
+    for cap in (16, 256):
+        ix.set_tuning(cap, 2, 128, 65536, 1024)
+        for name in ("adna", "divergent", "edge_nonstop", "edge_loggap", "plain", "tiny_queue"):
+            meta = CASES[name]
+            p = case_paths(name, meta)
+            res = galn_b200.aln(ix, meta["opts"], p["fq"], galn_b200.GALN_ENGINE_PERSISTENT)
+            assert res.sai_bytes() == open(p["sai"], "rb").read(), (name, cap)
+            pr = np.load(p["per_read"])
+            np.testing.assert_array_equal(res.pops, pr["pops"])
+            if trace:
+                np.testing.assert_array_equal(res.trace, pr["trace"])
+            assert ix.last_profile()["fused"] == fused
+
+
 @pytest.mark.parametrize("wait_ns", [0, 20_000])
 def test_warp_wait_running_out_gives_same_bytes(wait_ns):
     """The big-arena warps' bounded wait for queued reads, made to run out: at 0 every wait gives up at
