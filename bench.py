@@ -218,6 +218,29 @@ def cpu_reference_full(prefix, reads, opts, d, cores, m):
     return (cb, r), None
 
 
+def gpu_reference(prefix, reads, opts, d, cores, m):
+    """The reference's own GPU path (`galn aln --gpu-only`, its light tier and warp engine compiled for this
+    GPU) on the first m reads, in a process of its own with a time limit: reads/s from its timing line and
+    the md5 of the .sai it wrote."""
+    import oracle
+    if not os.path.exists(oracle.GALN_REF):
+        return {"error": "reference binary oracle/_ref/galn_ref not built"}
+    n = min(m, len(reads))
+    fq = sample_fastq(reads, n, d, "all")
+    out = os.path.join(d, "ref_gpu.sai")
+    try:
+        info = oracle.run_galn_ref(prefix, fq, opts, out, workers=cores, timeout=900.0, mode="--gpu-only")
+    except subprocess.TimeoutExpired:
+        return {"reads": n, "error": "did not finish within 900 s"}
+    if info["rc"] not in (0, 4) or "search_s" not in info:
+        return {"reads": n, "error": "rc %d: %s" % (info["rc"], info["stderr"][-300:])}
+    with open(out, "rb") as f:
+        md5 = hashlib.md5(f.read()).hexdigest()
+    return {"reads": n, "reads_per_s": n / max(info["search_s"], 1e-3), "search_s": info["search_s"], "sai_md5": md5,
+            "how": "reference `galn aln --gpu-only` (its GPU path; CPU workers take only what the GPU cannot), "
+                   "search time from its own timing line"}
+
+
 def cpu_reference_sampled(prefix, reads, opts, sample, d, steps, warmup, cores):
     """The reference arm: the reference's CPU path on a prefix of the reads grown until one run searches
     for a few seconds (its timer has 10 ms resolution), run warmup + steps times."""
@@ -533,6 +556,8 @@ def main():
                     help="first reads of the reference arm's sample (0: no reference runs in the GPU arm)")
     ap.add_argument("--ref-reads", type=int, default=2_000_000,
                     help="reads of the GPU arm's reference run (its cpu_baseline and .sai md5 check)")
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="also time the reference's own GPU path (`galn aln --gpu-only`) on the same reads")
     ap.add_argument("--data-dir", default=None)
     ap.add_argument("--trace", action="store_true", help="compute per-read trace hashes (verification mode)")
     ap.add_argument("--t0-cap", type=int, default=1024, help="first-tier stack entries per thread")
@@ -729,6 +754,14 @@ def main():
                 k = ref_full["n"]
                 Rk = galn_b200.Reads(R.seq[:int(R.offset[k])], R.offset[:k + 1].copy())
                 ref_full["gpu_md5"] = hashlib.md5(galn_b200.aln(ix, opts, Rk, engine).sai_bytes()).hexdigest()
+    ref_gpu = None
+    if args.reference_gpu and rank == 0 and world == 1:
+        ref_gpu = gpu_reference(prefix, reads, opts, d, cores, args.ref_reads)
+        if "sai_md5" in ref_gpu:
+            mine = (ref_full or {}).get("gpu_md5") if ref_gpu["reads"] < n else (sorted(md5)[0] if len(md5) == 1 else None)
+            ref_gpu["sai_md5_vs_this_build"] = ref_gpu["sai_md5"] == mine
+            if ref_full and ref_full["n"] == ref_gpu["reads"]:
+                ref_gpu["sai_md5_vs_reference_cpu"] = ref_gpu["sai_md5"] == ref_full["md5"]
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -778,6 +811,8 @@ def main():
         else:
             line["sai_md5_vs_reference"] = len(md5) == 1 and ref_full["md5"] in md5
         line["sai_md5_vs_reference_reads"] = ref_full["n"]
+    if ref_gpu:
+        line["reference_gpu"] = ref_gpu
     if plain:
         line["plain_engine"] = plain
     if divergent:

@@ -107,7 +107,7 @@ def lib():
                                 C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.galn_autotune_clear.argtypes = [vp]
     L.galn_autotune_choice.argtypes = [vp, C.POINTER(Options), C.POINTER(C.c_int), C.POINTER(C.c_int),
-                                       C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+                                       C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.galn_last_graph_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     L.galn_index_build_text.argtypes = [vp, C.c_uint64, C.c_char_p, C.c_int, C.POINTER(BuildStats)]
     L.galn_index_build_text_ex.argtypes = [vp, C.c_uint64, C.c_char_p, C.c_int, C.c_int64, C.POINTER(BuildStats)]
@@ -264,10 +264,10 @@ class Index:
                                  C.byref(occ), C.byref(ms))
         if rc:
             raise GalnError(f"autotune failed ({rc})")
-        arena, big = C.c_int(), C.c_int()
-        lib().galn_autotune_choice(self.h, C.byref(opts), None, None, None, C.byref(arena), C.byref(big))
+        arena, big, div = C.c_int(), C.c_int(), C.c_int()
+        lib().galn_autotune_choice(self.h, C.byref(opts), None, None, None, C.byref(arena), C.byref(big), C.byref(div))
         return dict(t0_cap=cap.value, block=blk.value, occ=occ.value, warp_arena=arena.value, warp_big=big.value,
-                    ms=ms.value)
+                    fused_div=div.value, ms=ms.value)
 
     def set_occ_layout(self, stride: int):
         """Occurrence layout (64 or 80 symbols per 32-byte block) when the autotuner has no choice."""

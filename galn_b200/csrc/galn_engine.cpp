@@ -228,7 +228,14 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     // the fused launch (first tier and warp tier in one launch) for the persistent engine when the warp tier
     // can run: its first tier claims the reads longest expected search first (max_diff, then length), so that
     // heavy reads reach the warp tier early; results do not depend on the order
-    const bool use_fused = engine == GALN_ENGINE_PERSISTENT && ix->use_fused && ix->use_warp && !wide && n > 0;
+    // the share of the fused launch's blocks that are warp-tier warps from the start (1 / fused_div; 0: two
+    // launches): the autotuner's for this option set, else the index's
+    int fused_div = ix->use_fused ? ix->fused_div : 0;
+    if (!ix->tune_active) {
+        auto it = ix->tuned.find(opts_key(&sets[0]));
+        if (it != ix->tuned.end() && it->second.arena > 0) fused_div = it->second.fused_div;
+    }
+    const bool use_fused = engine == GALN_ENGINE_PERSISTENT && fused_div > 0 && ix->use_warp && !wide && n > 0;
     if (use_fused) {
         const int kL = kWarpMaxLen + 1, nkey = 126 * kL;
         auto key = [&](int r) {
@@ -390,11 +397,11 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     bool fused = false;
     std::vector<int32_t> elig, rest;     // reads for the warp tier's next pass, and for the thread tiers
     if (use_fused) {
-        // one persistent launch of both tiers: blocks of kFusedWarps warps, as many as stay resident; a quarter
+        // one persistent launch of both tiers: blocks of kFusedWarps warps, as many as stay resident; 1 / fused_div
         // of them are warp-tier warps from the start, the others run the first tier first
         const int grid = fused_resident_blocks(ix->dev.device);
-        if (grid <= 0) return GALN_ECUDA;
-        const int n_w_blocks = std::max(1, grid / 4);
+        if (grid <= 1) return GALN_ECUDA;
+        const int n_w_blocks = std::min(grid - 1, std::max(1, grid / fused_div));
         TierCfg ft = t0;
         ft.persistent = true;
         ft.threads = (grid - n_w_blocks) * kFusedWarps * 32;

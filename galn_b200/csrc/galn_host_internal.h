@@ -107,12 +107,13 @@ struct galn_index {
     bool keep_stats = false;            // keep per-read fetch counts and tiers of the last run
     bool trace = true;                  // compute the per-read trace hash (the reference's --verify data)
     bool use_warp = true;               // the warp tier for reads that overflow T0
-    struct TuneChoice { int cap, block, occ, arena, big; };
+    struct TuneChoice { int cap, block, occ, arena, big, fused_div; };
     std::map<uint64_t, TuneChoice> tuned;   // option-set key -> the autotuner's choice
     int occ = 64;                       // occurrence layout when the autotuner has no choice (64 or 80)
     bool tune_active = false;           // the autotuner is timing a candidate: ignore the table
     bool use_graph = true;              // launch the persistent first tier through a CUDA graph
-    bool use_fused = true;              // the persistent engine's first and warp tiers in one launch
+    bool use_fused = false;             // untuned option sets: the first and warp tiers in one launch
+    int fused_div = 16;                 // 1 / fused_div of its blocks are warp-tier warps from the start
     int warp_arena = 1 << 13;           // chunks (kWarpChunk entries) per warp
     int warp_big = 128;                 // warps of a warp-tier launch whose arenas hold the max_entries cut-off
     uint64_t warp_wait_ns = 2000000000ull;   // a big warp's bounded wait for queued work

@@ -49,10 +49,11 @@ extern "C" int galn_autotune(galn_index *ix, const galn_opts *o, const galn_read
     static const int arenas[] = {2048, 8192, 16384};
     static const int bigs[] = {64, 128, 256};
     const int saved_cap = ix->t0_cap, saved_block = ix->t0_block, saved_occ = ix->occ;
-    const int saved_arena = ix->warp_arena, saved_big = ix->warp_big;
-    const bool saved_stats = ix->keep_stats;
+    const int saved_arena = ix->warp_arena, saved_big = ix->warp_big, saved_div = ix->fused_div;
+    const bool saved_stats = ix->keep_stats, saved_fused = ix->use_fused;
     ix->keep_stats = false;
     int bc = saved_cap, bb = saved_block, bo = saved_occ, ba = saved_arena, bg = saved_big;
+    int bd = saved_fused ? saved_div : 0;
     double bms = 1e300;
     int rc = 0;
     auto time_one = [&](double &ms) {
@@ -89,14 +90,31 @@ extern "C" int galn_autotune(galn_index *ix, const galn_opts *o, const galn_read
             rc = time_one(ms);
             if (!rc && ms < bms) { bms = ms; ba = ar; bg = bg2; }
         }
+    // the launch form: two launches (0) or the fused launch with 1/16 .. 1/2 of its blocks warp-tier warps
+    // from the start
+    {
+        static const int divs[] = {0, 16, 8, 4, 2};
+        ix->warp_arena = ba;
+        ix->warp_big = bg;
+        ix->use_fused = true;
+        for (int dv : divs) {
+            if (rc) break;
+            ix->fused_div = dv;
+            double ms = 0;
+            rc = time_one(ms);
+            if (!rc && ms < bms) { bms = ms; bd = dv; }
+        }
+    }
     ix->t0_cap = saved_cap;
     ix->t0_block = saved_block;
     ix->occ = saved_occ;
     ix->warp_arena = saved_arena;
     ix->warp_big = saved_big;
+    ix->fused_div = saved_div;
+    ix->use_fused = saved_fused;
     ix->keep_stats = saved_stats;
     if (rc) return rc;
-    ix->tuned[opts_key(o)] = galn_index::TuneChoice{bc, bb, bo, ba, bg};
+    ix->tuned[opts_key(o)] = galn_index::TuneChoice{bc, bb, bo, ba, bg, bd};
     if (best_cap) *best_cap = bc;
     if (best_block) *best_block = bb;
     if (best_occ) *best_occ = bo;
@@ -105,7 +123,7 @@ extern "C" int galn_autotune(galn_index *ix, const galn_opts *o, const galn_read
 }
 
 extern "C" int galn_autotune_choice(galn_index *ix, const galn_opts *o, int *cap, int *block, int *occ,
-                                    int *warp_arena, int *warp_big)
+                                    int *warp_arena, int *warp_big, int *fused_div)
 {
     if (!ix || !o) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
@@ -116,6 +134,7 @@ extern "C" int galn_autotune_choice(galn_index *ix, const galn_opts *o, int *cap
     if (occ) *occ = it->second.occ;
     if (warp_arena) *warp_arena = it->second.arena;
     if (warp_big) *warp_big = it->second.big;
+    if (fused_div) *fused_div = it->second.fused_div;
     return 0;
 }
 

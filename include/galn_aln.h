@@ -298,26 +298,29 @@ int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, in
 /* The autotuner (no reference counterpart): times the first max_sample reads (0: all) once per candidate
  * occurrence layout (64 or 80 symbols per 32-byte block), first-tier stack depth (256..4096 entries: the
  * split between thread-per-read and warp-per-read) and block size, then, with that choice, once per warp-tier
- * arena per warp (2048..16384 chunks of 64 entries) and count of big-arena warps (64..256), and keeps the
- * fastest for this option set; later searches with the same options use it. Returns the first stage's
- * choice and the best device milliseconds; galn_autotune_choice gives the whole choice for an option set
- * (GALN_EINVAL if it has none). galn_autotune_clear forgets all choices. */
+ * arena per warp (2048..16384 chunks of 64 entries) and count of big-arena warps (64..256), then once per
+ * launch form (two launches, or the fused launch with 1/16 .. 1/2 of its blocks warp-tier warps from the
+ * start: fused_div 0, or 16 .. 2), and keeps the fastest for this option set; later searches with the same
+ * options use it. Returns the first stage's choice and the best device milliseconds; galn_autotune_choice
+ * gives the whole choice for an option set (GALN_EINVAL if it has none). galn_autotune_clear forgets all
+ * choices. */
 int galn_autotune(galn_index *ix, const galn_opts *o, const galn_reads *in, int max_sample, int *best_cap,
                   int *best_block, int *best_occ, double *best_ms);
 int galn_autotune_choice(galn_index *ix, const galn_opts *o, int *cap, int *block, int *occ, int *warp_arena,
-                         int *warp_big);
+                         int *warp_big, int *fused_div);
 int galn_autotune_clear(galn_index *ix);
 
 /* How many of the last run's kernel launches went through a CUDA graph (no reference counterpart). */
 int galn_last_graph_launches(galn_index *ix, int64_t *graph_launches);
 
-/* The persistent engine's first tier and warp tier as one launch (no reference counterpart; on by default):
- * blocks of 8 warps, as many as stay resident, a quarter of them warp-tier warps from the start and the
- * others first-tier threads that turn into warp-tier warps when the first tier's reads run out; a read that
- * overflows the first tier is handed to a warp at once through a device queue (the reference's light tier and
- * warp phases hand reads over in the same way through its shared list, src/galn.cu:907-1180). Off, the tiers
- * are two launches. Results never depend on it. galn_last_run_fused tells whether the last run used it
- * (the launch's time is then ms_tier[0] of galn_last_run_profile). */
+/* The persistent engine's first tier and warp tier as one launch (no reference counterpart): blocks of 8
+ * warps, as many as stay resident, 1/16 of them warp-tier warps from the start and the others first-tier
+ * threads (heaviest reads first) that turn into warp-tier warps when the first tier's reads run out; a read
+ * that overflows the first tier is handed to a warp at once through a device queue (the reference's light
+ * tier and warp phases hand reads over through its shared list, src/galn.cu:907-1180). This sets the form
+ * for option sets the autotuner has not tuned (off by default: two launches); a tuned option set uses the
+ * form the autotuner timed fastest. Results never depend on it. galn_last_run_fused tells whether the last
+ * run used it (the launch's time is then ms_tier[0] of galn_last_run_profile). */
 int galn_index_set_fused(galn_index *ix, int on);
 int galn_last_run_fused(galn_index *ix, int *fused);
 

@@ -305,9 +305,10 @@ def cal_maxdiff(l: int, err: float, thres: float) -> int:
 # the reference itself
 
 def run_galn_ref(prefix: str, fastq: str, args: list[str], out_sai: str, workers: int | None = None,
-                 timeout: float = 3600.0) -> dict:
-    """Runs the reference's `galn aln --cpu-only` and returns its exit code and timing line."""
-    cmd = [GALN_REF, "aln", "--cpu-only"] + list(args)
+                 timeout: float = 3600.0, mode: str = "--cpu-only") -> dict:
+    """Runs the reference's `galn aln --cpu-only` (or `--gpu-only`, its own GPU path) and returns its exit
+    code and timing line."""
+    cmd = [GALN_REF, "aln", mode] + list(args)
     if workers:
         cmd += ["--cpu-workers", str(workers)]
     cmd += ["-f", out_sai, prefix, fastq]
