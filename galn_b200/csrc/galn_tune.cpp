@@ -45,9 +45,11 @@ extern "C" int galn_autotune(galn_index *ix, const galn_opts *o, const galn_read
     static const int blocks[] = {128, 256};
     static const int layouts[] = {64, 80};
     // the warp tier's arena per warp (64-entry chunks) and its count of big-arena warps, timed with the
-    // first stage's choice
-    static const int arenas[] = {2048, 8192, 16384};
-    static const int bigs[] = {64, 128, 256};
+    // first stage's choice. Only sizes at or above the defaults: a sample holds fewer of the heaviest reads
+    // than the whole input, and smaller arenas or fewer big warps that suit the sample choke on the whole
+    // (2048 chunks and 64 big warps ran the aDNA sample fastest and the full 2 M reads 2.3x slower).
+    static const int arenas[] = {8192, 16384};
+    static const int bigs[] = {128, 256};
     const int saved_cap = ix->t0_cap, saved_block = ix->t0_block, saved_occ = ix->occ;
     const int saved_arena = ix->warp_arena, saved_big = ix->warp_big, saved_div = ix->fused_div;
     const bool saved_stats = ix->keep_stats, saved_fused = ix->use_fused;

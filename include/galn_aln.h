@@ -298,7 +298,7 @@ int galn_last_run_profile(galn_index *ix, double *ms_device, double *ms_tier, in
 /* The autotuner (no reference counterpart): times the first max_sample reads (0: all) once per candidate
  * occurrence layout (64 or 80 symbols per 32-byte block), first-tier stack depth (256..4096 entries: the
  * split between thread-per-read and warp-per-read) and block size, then, with that choice, once per warp-tier
- * arena per warp (2048..16384 chunks of 64 entries) and count of big-arena warps (64..256), then once per
+ * arena per warp (8192 or 16384 chunks of 64 entries) and count of big-arena warps (128 or 256), then once per
  * launch form (two launches, or the fused launch with 1/16 .. 1/2 of its blocks warp-tier warps from the
  * start: fused_div 0, or 16 .. 2), and keeps the fastest for this option set; later searches with the same
  * options use it. Returns the first stage's choice and the best device milliseconds; galn_autotune_choice
