@@ -576,7 +576,7 @@ def main():
                     help="high-divergence reads compared with the reference's .sai")
     ap.add_argument("--no-gather-sweep", dest="gather_sweep", action="store_false")
     ap.add_argument("--index-build", action="store_true", help="time `galn index` on the workload's reference")
-    ap.add_argument("--profile-case", choices=["warp_steady", "gather"], default=None)
+    ap.add_argument("--profile-case", choices=["warp_steady", "gather", "t0_small"], default=None)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -593,6 +593,21 @@ def main():
         gbuild.build()
         print(json.dumps({"case": "gather", "bytes": 1 << 30, "in_flight": 8,
                           "gbs": galn_b200.gather_peak(local, 1 << 30, 8, 2)}))
+        return 0
+    if args.profile_case == "t0_small":
+        # the first tier on one bwa batch of the aDNA workload (its first 262,144 reads), two launches of the
+        # two-launch form; capture the first search_kernel launch (ncu -k regex:search_kernel -c 1)
+        import galn_b200
+        d, prefix, ref, reads, opts = prepare("adna", 1.0, 0, local, args.data_dir, None)
+        m = 262144
+        R = galn_b200.Reads(reads.ascii()[:int(reads.off[m])], reads.off[:m + 1].copy())
+        ix = galn_b200.Index(prefix, device=local)
+        ix.set_trace(False)
+        ix.set_tuning(t0_cap=256, t0_block=256)
+        for _ in range(2):
+            galn_b200.aln(ix, opts, R)
+            p = ix.last_profile()
+            print(json.dumps(dict(case="t0_small", reads=m, ms_tier=[round(x, 3) for x in p["ms_tier"][:2]])))
         return 0
     if args.profile_case:
         return profile_warp_steady(args, local)
