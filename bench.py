@@ -566,7 +566,9 @@ def main():
     ap.add_argument("--no-serve-reference", dest="serve_reference", action="store_false",
                     help="skip the reference runs of the served requests")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
-    ap.add_argument("--autotune-sample", type=int, default=262144)
+    ap.add_argument("--autotune-sample", type=int, default=2_000_000,
+                    help="reads the autotuner times (the whole aDNA workload: a smaller sample holds fewer of the "
+                         "heaviest reads and picked launch forms that were slower on all reads)")
     ap.add_argument("--serve-rate", type=float, default=16.0, help="request arrival rate (per second)")
     ap.add_argument("--div-reads-scale", type=float, default=0.1,
                     help="fraction of the high-divergence configuration's 1 M reads (0: skip it)")

@@ -116,6 +116,7 @@ def lib():
     L.galn_gather_peak.argtypes = [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_double)]
     L.galn_index_set_warp_wait.argtypes = [vp, C.c_int64]
     L.galn_index_set_fused.argtypes = [vp, C.c_int]
+    L.galn_index_set_warp_order.argtypes = [vp, C.c_int]
     L.galn_last_run_fused.argtypes = [vp, C.POINTER(C.c_int)]
     L.galn_index_occ.argtypes = [vp, C.c_int, vp, C.c_int64, vp, vp]
     L.galn_stack_need.argtypes = [vp, C.POINTER(Options), C.POINTER(_Reads), C.POINTER(C.c_uint64)]
@@ -185,6 +186,11 @@ class Index:
     def set_warp_tier(self, on: bool, arena_chunks: int = 1 << 13):
         if lib().galn_index_set_warp_tier(self.h, int(on), arena_chunks):
             raise GalnError("bad warp tier setting")
+
+    def set_warp_order(self, order: int):
+        """Order of the heavy reads handed to the warp tier (galn_index_set_warp_order)."""
+        if lib().galn_index_set_warp_order(self.h, int(order)):
+            raise GalnError("bad warp order")
 
     def set_fused(self, on: bool):
         """The persistent engine's first and warp tiers as one launch (galn_index_set_fused; on by default)."""

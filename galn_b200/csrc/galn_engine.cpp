@@ -553,10 +553,24 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
                 else rest.push_back(r);
             }
         }
-        // longest expected searches first (max_diff, then length), so that the heaviest reads do not start
-        // last and run alone at the end of the launch; results do not depend on the order. A counting sort:
-        // the eligible reads have max_diff <= 125 and length <= kWarpMaxLen.
-        {
+        // longest expected searches first, so that the heaviest reads do not start last and run alone at the
+        // end of the launch; results do not depend on the order. Order 1: the reads whose first-tier search
+        // overflowed after the fewest pops (the stack grew fastest) first, read from the first tier's pop
+        // counts; order 0: max_diff, then length. Counting sorts: the eligible reads have max_diff <= 125 and
+        // length <= kWarpMaxLen; pop counts are clamped.
+        if (!fused && ix->warp_order == 1 && !elig.empty()) {
+            RCK(B.h_pops.ensure((size_t)n * 8));
+            uint64_t *hp = (uint64_t *)B.h_pops.p;
+            ECK(cudaMemcpyAsync(hp, job.out_pops, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+            ECK(cudaStreamSynchronize(st));
+            const int kMaxKey = 1 << 16;
+            std::vector<int32_t> cnt((size_t)kMaxKey + 1, 0), sorted(elig.size());
+            auto key = [&](int32_t r) { return (int)std::min<uint64_t>(hp[r], (uint64_t)kMaxKey - 1); };
+            for (int32_t r : elig) ++cnt[(size_t)key(r) + 1];
+            for (int k = 0; k < kMaxKey; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];
+            for (int32_t r : elig) sorted[(size_t)cnt[(size_t)key(r)]++] = r;
+            elig.swap(sorted);
+        } else {
             const int kL = kWarpMaxLen + 1, nkey = 126 * kL;
             std::vector<int32_t> cnt((size_t)nkey + 1, 0), sorted(elig.size());
             auto key = [&](int32_t r) {
@@ -875,6 +889,14 @@ extern "C" int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks
     std::lock_guard<std::mutex> lk(ix->mu);
     ix->use_warp = on != 0;
     ix->warp_arena = arena_chunks;
+    return 0;
+}
+
+extern "C" int galn_index_set_warp_order(galn_index *ix, int order)
+{
+    if (!ix || order < 0 || order > 1) return GALN_EINVAL;
+    std::lock_guard<std::mutex> lk(ix->mu);
+    ix->warp_order = order;
     return 0;
 }
 

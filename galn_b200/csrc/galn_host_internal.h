@@ -116,6 +116,7 @@ struct galn_index {
     int fused_div = 16;                 // 1 / fused_div of its blocks are warp-tier warps from the start
     int warp_arena = 1 << 13;           // chunks (kWarpChunk entries) per warp
     int warp_big = 128;                 // warps of a warp-tier launch whose arenas hold the max_entries cut-off
+    int warp_order = 0;                 // heavy reads' order: 0 max_diff then length, 1 first-tier pops at overflow
     uint64_t warp_wait_ns = 2000000000ull;   // a big warp's bounded wait for queued work
     bool l2_persist = true;             // the occurrence blocks in a persisting L2 window
     // suffix-array samples (<prefix>.sa) for positions; sample 0 is the $ row (-1)

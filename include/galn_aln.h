@@ -359,6 +359,11 @@ int galn_index_set_warp_tier(galn_index *ix, int on, int arena_chunks);
  * queued is searched again; results never depend on it. 0 makes every wait run out at once and takes the
  * second of those paths (a way to test it). */
 int galn_index_set_warp_wait(galn_index *ix, int64_t wait_ns);
+/* The order in which the two-launch form hands the first tier's overflow to the warp tier (no reference
+ * counterpart): 0 (default) the largest max_diff, then the longest read first; 1 the reads whose first-tier
+ * search overflowed after the fewest pops first. Results never depend on it. */
+int galn_index_set_warp_order(galn_index *ix, int order);
+
 /* The last run's warp-tier queues (no reference counterpart): reads its first launch queued for the big-arena
  * warps (and, in the fused launch, from the first tier to the warp tier), and whether a lost queue slot
  * made every queued read be searched again. */

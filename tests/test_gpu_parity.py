@@ -107,6 +107,22 @@ def test_fused_and_two_launch_forms_give_same_bytes(fused, trace):
             assert ix.last_profile()["fused"] == fused
 
 
+@pytest.mark.parametrize("order", [0, 1])
+def test_warp_order_keeps_bytes(order):
+    """The order in which heavy reads reach the warp tier (by max_diff and length, or by the first tier's
+    pops at overflow) changes nothing in the results."""
+    ix = galn_b200.Index(os.path.join(GOLDEN, "small", "ref"))
+    ix.set_fused(False)
+    ix.set_warp_order(order)
+    ix.set_tuning(16, 2, 128, 65536, 1024)
+    for name in ("adna", "divergent", "edge_nonstop"):
+        meta = CASES[name]
+        p = case_paths(name, meta)
+        res = galn_b200.aln(ix, meta["opts"], p["fq"], galn_b200.GALN_ENGINE_PERSISTENT)
+        assert res.sai_bytes() == open(p["sai"], "rb").read(), name
+        np.testing.assert_array_equal(res.trace, np.load(p["per_read"])["trace"])
+
+
 @pytest.mark.parametrize("wait_ns", [0, 20_000])
 def test_warp_wait_running_out_gives_same_bytes(wait_ns):
     """The big-arena warps' bounded wait for queued reads, made to run out: at 0 every wait gives up at
