@@ -193,7 +193,8 @@ class Index:
             raise GalnError("bad warp order")
 
     def set_fused(self, on: bool):
-        """The persistent engine's first and warp tiers as one launch (galn_index_set_fused; on by default)."""
+        """The persistent engine's first and warp tiers as one launch (galn_index_set_fused) for option sets the
+        autotuner has not tuned; off by default (two launches)."""
         if lib().galn_index_set_fused(self.h, int(on)):
             raise GalnError("bad fused setting")
 

@@ -13,7 +13,7 @@
 // and every idle lane takes the next entry not yet handed out (in entry order), so lanes stay busy however
 // uneven the chains are. A lane stages the pushes of each pop (in the order bwt_match_gap pushes them) in
 // global memory, one list per distinct target bucket (b+s_mm, b+s_gapo, b+s_gape), and 2 bytes of per-pop
-// data in shared memory; when a chain ends it writes the entry's record (its lane, pops, staged segments
+// data in the warp's side area; when a chain ends it writes the entry's record (its lane, pops, staged segments
 // and prefix sums). A chain that reaches a hit, a score past n_stacks, or the end of its lane's space
 // (a "stop") ends the hand-out after its entry; entries past it are dropped.
 //
@@ -26,9 +26,9 @@
 // bucket is the same LIFO as in the sequential search.
 //
 // Storage: each bucket is a chain of 64-entry chunks in the warp's arena (global memory), with its top
-// chunk, fill and entry count in shared memory. Widths, the query, the wave's entries and records and the
-// per-pop data are in shared memory; staged pushes (and, in trace mode, popped entries) in a per-warp
-// global staging area. Reads the tier cannot take (length > 256, n_stacks > 256, a penalty <= 0, 32-byte
+// chunk, fill and entry count in shared memory. Widths, the query, the wave's entries and records are in
+// shared memory; the per-pop data, staged pushes (and, in trace mode, popped entries) in per-warp global
+// areas. Reads the tier cannot take (length > 256, n_stacks > 256, a penalty <= 0, 32-byte
 // entries) or that outgrow the arena or the record buffer go to the thread tiers (the host routes them).
 #pragma once
 
@@ -78,8 +78,9 @@ struct WSide {
     uint4 lane_x[32];                 // pending exact child of a lane that stopped mid-chain
     uint64_t hk[32], hl[32];          // the hazard's interval after the exact tail
     // per pop of each lane: pushes (bits 0-3, the fused exact child not counted), has an exact child
-    // (bit 4), index blocks read (bits 5-15)
-    uint16_t meta[32][kWP];
+    // (bit 4), index blocks read (bits 5-15). Pop-major: the lanes of one step write neighbouring halfwords,
+    // so a step's writes fill a few sectors instead of touching one sector per lane.
+    uint16_t meta[kWP][32];
 };
 
 struct WArgs {
@@ -195,7 +196,7 @@ struct WWalk {
 // its exact child (now in x), 0 = the chain is finished, 1 = hazard (a hit) at this pop, 2 = stopped with
 // the exact child pending (no room left in this wave; the child is in D->lane_x), 3 = this pop pushes a
 // score >= n_stacks (bwt_match_gap returns BWTGAP_ERR_SCORE there). A finished pop's data goes to
-// D->meta[lane][lp] (and to mt); its pushes are appended to this lane's staging lists (st: list L at
+// D->meta[lp][lane] (and to mt); its pushes are appended to this lane's staging lists (st: list L at
 // st + L * 32 * kWL; tl: list of each push kind, mismatch, gap open, gap extension); in trace mode the popped
 // entry goes to pr[lp].
 template <bool TRACE, int ST>
@@ -325,23 +326,32 @@ __device__ __forceinline__ int lane_step(const IndexView &ix, const BatchOpt &O,
         // a push at or past n_stacks ends the read (BWTGAP_ERR_SCORE); nothing else of this pop matters then
         err = ((slots & 0x1fu) && g_bkt >= O.n_stacks) || ((slots & 0x1e0u) && m_bkt >= O.n_stacks);
         if (!err) {
+            // the gap children (slots 0-4) go to list g_list and the mismatches (slots 5-8) to list 0 (tl[0]),
+            // each kind in slot order at consecutive places; when both kinds share list 0 the mismatches follow
+            // the gap children, as bwt_match_gap pushes them
+            const uint32_t gs = slots & 0x1fu, ms = slots >> 5;
+            const int ng = __popc(gs), nm = __popc(ms);
+            const int gbase = g_list == 0 ? nl0 : (g_list == 1 ? nl1 : nl2);
+            nl0 += g_list == 0 ? ng : 0;
+            nl1 += g_list == 1 ? ng : 0;
+            nl2 += g_list == 2 ? ng : 0;
+            const int gofs = g_list * (int)lstride + gbase, mofs = nl0;
+            nl0 += nm;
+            npu = (uint32_t)(ng + nm);
 #pragma unroll
-            for (int t = 0; t < 9; ++t) {
-                if (!(slots & (1u << t))) continue;
-                uint64_t w0, w1;
-                int L;
-                if (t == 0) { w0 = (x.k & kK38) | h0_self; w1 = (x.l & kK38) | h1_self; L = g_list; }
-                else if (t <= 4) {
-                    w0 = (kk[t - 1] & kK38) | h0_del; w1 = (ll[t - 1] & kK38) | h1_del; L = g_list;
-                } else {
-                    w0 = (rk[t - 4] & kK38) | h0_mm;
-                    w1 = (rl[t - 4] & kK38) | w1b;
-                    L = tl[0];
-                }
-                const int n_ = L == 0 ? nl0 : (L == 1 ? nl1 : nl2);
-                st[L * lstride + n_] = make_uint4((uint32_t)w0, (uint32_t)(w0 >> 32), (uint32_t)w1, (uint32_t)(w1 >> 32));
-                nl0 += L == 0; nl1 += L == 1; nl2 += L == 2;
-                ++npu;
+            for (int t = 0; t < 5; ++t) {
+                if (!(gs & (1u << t))) continue;
+                const uint64_t w0 = t == 0 ? (x.k & kK38) | h0_self : (kk[t - 1] & kK38) | h0_del;
+                const uint64_t w1 = t == 0 ? (x.l & kK38) | h1_self : (ll[t - 1] & kK38) | h1_del;
+                st[gofs + __popc(gs & ((1u << t) - 1u))] = make_uint4((uint32_t)w0, (uint32_t)(w0 >> 32), (uint32_t)w1,
+                                                                 (uint32_t)(w1 >> 32));
+            }
+#pragma unroll
+            for (int j = 1; j <= 4; ++j) {
+                if (!(ms & (1u << (j - 1)))) continue;
+                const uint64_t w0 = (rk[j] & kK38) | h0_mm, w1 = (rl[j] & kK38) | w1b;
+                st[mofs + __popc(ms & ((1u << (j - 1)) - 1u))] = make_uint4((uint32_t)w0, (uint32_t)(w0 >> 32), (uint32_t)w1,
+                                                                      (uint32_t)(w1 >> 32));
             }
         }
         const bool exact = !err && base < 4 && rk[4] <= rl[4];
@@ -354,7 +364,7 @@ __device__ __forceinline__ int lane_step(const IndexView &ix, const BatchOpt &O,
         }
     }
     if (endc == -2) return endc;
-    D->meta[lane][lp] = (uint16_t)mt;
+    D->meta[lp][lane] = (uint16_t)mt;
     ++lp;
     // room for one more pop: at most 9 pushes, all possibly in one list
     if (endc == -1 && (lp == kWP || nl0 + 9 > kWL || nl1 + 9 > kWL || nl2 + 9 > kWL)) {
@@ -696,8 +706,8 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
                 const int endc = (int)(inf >> 24);
                 // the entry's per-pop data, np <= kWP <= 64 words, one load per lane
                 static_assert(kWP <= 64, "replay prefetch");
-                const uint16_t *mrow = D->meta[ln] + p0;
-                const uint32_t m_lo = lane < np ? mrow[lane] : 0u, m_hi = lane + 32 < np ? mrow[lane + 32] : 0u;
+                const uint32_t m_lo = lane < np ? D->meta[p0 + lane][ln] : 0u;
+                const uint32_t m_hi = lane + 32 < np ? D->meta[p0 + lane + 32][ln] : 0u;
                 for (int t = 0; t < np; ++t) {
                     if (n_entries > O.max_entries) { search_end = true; stop = true; break; }
                     --n_entries;
