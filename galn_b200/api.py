@@ -308,9 +308,10 @@ class Index:
 
     def last_phases(self) -> dict:
         """Host-side timeline of the last run, in ms from the call's start."""
-        v = (C.c_double * 5)()
-        lib().galn_last_run_phases(self.h, v, 5)
-        return dict(launch=v[0], device_done=v[1], results=v[2], total=v[3], device=v[4])
+        v = (C.c_double * 8)()
+        lib().galn_last_run_phases(self.h, v, 8)
+        return dict(launch=v[0], device_done=v[1], results=v[2], total=v[3], device=v[4], first_tier_done=v[5],
+                    warp_launch=v[6], first_tier_launch=v[7])
 
     def last_stats(self) -> dict:
         t, k, tiers, la = C.c_double(), C.c_double(), C.c_int(), C.c_int64()

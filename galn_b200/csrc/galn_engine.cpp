@@ -72,11 +72,13 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     // ---- per-read lengths, batches, options: a few passes over the reads, on several host threads ----
     size_t nn = (size_t)std::max(n, 1);
     RCK(B.h_off.ensure((nn + 1) * 8));
-    RCK(B.h_list.ensure(nn * 4 * 3));
+    RCK(B.h_list.ensure(nn * 4 * 4));
     const int64_t total = n > 0 ? in->offset[n] - in->offset[0] : 0;
     const int64_t base = n > 0 ? in->offset[0] : 0;
     int64_t *h_off = (int64_t *)B.h_off.p;
-    int32_t *h_bid = (int32_t *)B.h_list.p, *h_md = h_bid + nn, *h_list = h_md + nn;
+    // pinned per-read arrays: batch ids, max_diff, the read list (later the first tier's overflow list), and the
+    // warp tier's sorted list
+    int32_t *h_bid = (int32_t *)B.h_list.p, *h_md = h_bid + nn, *h_list = h_md + nn, *h_wlist = h_list + nn;
     const int32_t *bid = h_bid, *maxdiff = h_md;
     const int T = n >= (1 << 16) ? (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency())) : 1;
     auto par = [&](const std::function<void(int, int, int)> &fn) {
@@ -291,6 +293,11 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     S.ms_phase[0] = now_ms() - t_start;
     RCK(dev_encode(job, st));
     if (n > 0) S.kernel_launches += 1;
+    if (n > 0 && engine != GALN_ENGINE_PLAIN) {
+        const int w = index_l2_warm(ix, st, job.occ);
+        if (w < 0) return w;
+        S.kernel_launches += w;
+    }
 
     size_t free_b = 0, total_b = 0;
     ECK(cudaMemGetInfo(&free_b, &total_b));
@@ -348,6 +355,7 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
                 if (ie != cudaSuccess) { cudaGraphDestroy(g); ctx.graph_exec = nullptr; return GALN_ECUDA; }
             }
             cudaGraphDestroy(g);
+            S.ms_phase[5] = now_ms() - t_start;
             ECK(cudaGraphLaunch(ctx.graph_exec, st));
             ECK(cudaStreamSynchronize(st));
             S.graph_launches += 1;
@@ -513,6 +521,7 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     } else if (engine == GALN_ENGINE_PERSISTENT) {
         t0.persistent = true;
         RCK(run_tier(t0, cur, n, nxt, &n_ovf));
+        S.ms_phase[3] = now_ms() - t_start;
     } else {
         // one launch per bwa batch, one thread per read; a batch too large for the memory budget is
         // launched in equal chunks
@@ -541,23 +550,81 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     // ---- W: the warp tier for the reads that overflowed T0 (those it can take); after the fused launch,
     // its second pass for what that launch left ----
     if (warp_ok && (fused || n_ovf > 0)) {
-        if (!fused) {
-            std::vector<int32_t> ov((size_t)n_ovf);
-            ECK(cudaMemcpyAsync(ov.data(), cur, (size_t)n_ovf * 4, cudaMemcpyDeviceToHost, st));
-            ECK(cudaStreamSynchronize(st));
-            for (int32_t r : ov) {
-                int len = (int)(in->offset[r + 1] - in->offset[r]);
-                const HostBatchOpt &h = bopt[bid[r]];
-                if (len <= kWarpMaxLen && h.n_stacks <= kWarpMaxStacks && h.n_stacks > 0 && h.s_mm > 0 &&
-                    h.s_gapo > 0 && h.s_gape > 0) elig.push_back(r);
-                else rest.push_back(r);
-            }
-        }
         // longest expected searches first, so that the heaviest reads do not start last and run alone at the
         // end of the launch; results do not depend on the order. Order 1: the reads whose first-tier search
         // overflowed after the fewest pops (the stack grew fastest) first, read from the first tier's pop
         // counts; order 0: max_diff, then length. Counting sorts: the eligible reads have max_diff <= 125 and
         // length <= kWarpMaxLen; pop counts are clamped.
+        const int kL = kWarpMaxLen + 1, nkey = 126 * kL;
+        auto warp_key = [&](int32_t r) {
+            const int md = std::min(std::max(maxdiff[r], 0), 125);
+            const int len = (int)(in->offset[r + 1] - in->offset[r]);
+            return (125 - md) * kL + (kWarpMaxLen - len);   // ascending key = descending (max_diff, length)
+        };
+        bool elig_sorted = false;
+        if (!fused) {
+            // The overflow list into pinned memory (the read list's host copy went to the device at the start),
+            // then, on the host threads, each read's eligibility and key, per-thread key counts, and a stable
+            // scatter: the device waits for this gap, so it is kept to a few passes over pinned arrays.
+            ECK(cudaMemcpyAsync(h_list, cur, (size_t)n_ovf * 4, cudaMemcpyDeviceToHost, st));
+            ECK(cudaStreamSynchronize(st));
+            const int TT = n_ovf >= (1 << 15) ? T : 1;
+            const bool by_key = ix->warp_order != 1;
+            std::vector<std::vector<int32_t>> cnt_t((size_t)TT);
+            std::vector<int64_t> n_el((size_t)TT, 0), n_rest((size_t)TT, 0);
+            auto chunk = [&](int t) { return std::make_pair((int)((int64_t)n_ovf * t / TT), (int)((int64_t)n_ovf * (t + 1) / TT)); };
+            auto eligible = [&](int32_t r) {
+                const int len = (int)(in->offset[r + 1] - in->offset[r]);
+                const HostBatchOpt &h = bopt[bid[r]];
+                return len <= kWarpMaxLen && h.n_stacks <= kWarpMaxStacks && h.n_stacks > 0 && h.s_mm > 0 &&
+                       h.s_gapo > 0 && h.s_gape > 0;
+            };
+            auto run_t = [&](const std::function<void(int)> &fn) {
+                if (TT == 1) { fn(0); return; }
+                std::vector<std::thread> th;
+                for (int t = 0; t < TT; ++t) th.emplace_back(fn, t);
+                for (auto &x : th) x.join();
+            };
+            run_t([&](int t) {
+                std::vector<int32_t> &c = cnt_t[(size_t)t];
+                if (by_key) c.assign((size_t)nkey, 0);
+                const auto [i0, i1] = chunk(t);
+                for (int i = i0; i < i1; ++i) {
+                    const int32_t r = h_list[i];
+                    if (r < 0 || r >= n) { n_rest[(size_t)t] = -1; return; }   // a slot written by no thread
+                    if (!eligible(r)) { ++n_rest[(size_t)t]; continue; }
+                    ++n_el[(size_t)t];
+                    if (by_key) ++c[(size_t)warp_key(r)];
+                }
+            });
+            for (int t = 0; t < TT; ++t) if (n_rest[(size_t)t] < 0) return GALN_ECUDA;
+            // where each thread's reads of each key go: keys ascending, threads in order within a key
+            std::vector<int64_t> el0((size_t)TT + 1, 0), rs0((size_t)TT + 1, 0);
+            for (int t = 0; t < TT; ++t) { el0[(size_t)t + 1] = el0[(size_t)t] + n_el[(size_t)t]; rs0[(size_t)t + 1] = rs0[(size_t)t] + n_rest[(size_t)t]; }
+            if (by_key) {
+                int32_t run = 0;
+                for (int k = 0; k < nkey; ++k)
+                    for (int t = 0; t < TT; ++t) {
+                        const int32_t v = cnt_t[(size_t)t][(size_t)k];
+                        cnt_t[(size_t)t][(size_t)k] = run;
+                        run += v;
+                    }
+            }
+            rest.resize((size_t)rs0[(size_t)TT]);
+            run_t([&](int t) {
+                std::vector<int32_t> &c = cnt_t[(size_t)t];
+                int64_t e = el0[(size_t)t], q = rs0[(size_t)t];
+                const auto [i0, i1] = chunk(t);
+                for (int i = i0; i < i1; ++i) {
+                    const int32_t r = h_list[i];
+                    if (!eligible(r)) rest[(size_t)q++] = r;
+                    else if (by_key) h_wlist[c[(size_t)warp_key(r)]++] = r;
+                    else h_wlist[e++] = r;
+                }
+            });
+            elig.assign(h_wlist, h_wlist + el0[(size_t)TT]);
+            elig_sorted = by_key;
+        }
         if (!fused && ix->warp_order == 1 && !elig.empty()) {
             RCK(B.h_pops.ensure((size_t)n * 8));
             uint64_t *hp = (uint64_t *)B.h_pops.p;
@@ -570,17 +637,11 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
             for (int k = 0; k < kMaxKey; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];
             for (int32_t r : elig) sorted[(size_t)cnt[(size_t)key(r)]++] = r;
             elig.swap(sorted);
-        } else {
-            const int kL = kWarpMaxLen + 1, nkey = 126 * kL;
+        } else if (!elig_sorted) {
             std::vector<int32_t> cnt((size_t)nkey + 1, 0), sorted(elig.size());
-            auto key = [&](int32_t r) {
-                const int md = std::min(std::max(maxdiff[r], 0), 125);
-                const int len = (int)(in->offset[r + 1] - in->offset[r]);
-                return (125 - md) * kL + (kWarpMaxLen - len);   // ascending key = descending (max_diff, length)
-            };
-            for (int32_t r : elig) ++cnt[(size_t)key(r) + 1];
+            for (int32_t r : elig) ++cnt[(size_t)warp_key(r) + 1];
             for (int k = 0; k < nkey; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];
-            for (int32_t r : elig) sorted[(size_t)cnt[(size_t)key(r)]++] = r;
+            for (int32_t r : elig) sorted[(size_t)cnt[(size_t)warp_key(r)]++] = r;
             elig.swap(sorted);
         }
         // pass 1: the tuned arena per warp, plus up to n_big_max warps whose arenas hold the max_entries
@@ -613,7 +674,9 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
                 while (wc.n_warps > 1 && warp_ws_bytes(wc, ne) > budget) wc.n_warps /= 2;
             }
             RCK(B.ws.ensure(warp_ws_bytes(wc, ne)));
-            ECK(cudaMemcpyAsync(cur, elig.data(), (size_t)ne * 4, cudaMemcpyHostToDevice, st));
+            // the first pass's list from its pinned copy
+            ECK(cudaMemcpyAsync(cur, pass == 0 && elig_sorted ? h_wlist : elig.data(), (size_t)ne * 4,
+                                cudaMemcpyHostToDevice, st));
             ECK(cudaMemsetAsync(job.counters, 0, 8, st));
             unsigned long long *dbg = nullptr;
             if (ix->keep_stats) {
@@ -622,6 +685,7 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
                 ECK(cudaMemsetAsync(dbg, 0, kWarpDbg * 8, st));
             }
             ECK(cudaEventRecord(e0, st));
+            if (pass == 0) S.ms_phase[4] = now_ms() - t_start;
             RCK(dev_search_warp(ix->dev, job, wc, 1, cur, ne, nxt, B.ws.p, st, dbg));
             ECK(cudaEventRecord(e1, st));
             int32_t *q_slots = nullptr;
@@ -852,8 +916,9 @@ extern "C" int galn_last_run_phases(galn_index *ix, double *ms, int n)
     if (!ix || !ms || n < 0) return GALN_EINVAL;
     std::lock_guard<std::mutex> lk(ix->mu);
     const galn::RunStats &S = ix->main.last;
-    const double v[5] = {S.ms_phase[0], S.ms_phase[1], S.ms_phase[2], S.ms_total, S.ms_device};
-    for (int q = 0; q < n && q < 5; ++q) ms[q] = v[q];
+    const double v[8] = {S.ms_phase[0], S.ms_phase[1], S.ms_phase[2], S.ms_total, S.ms_device, S.ms_phase[3],
+                         S.ms_phase[4], S.ms_phase[5]};
+    for (int q = 0; q < n && q < 8; ++q) ms[q] = v[q];
     return 0;
 }
 

@@ -467,6 +467,23 @@ void galn::index_l2_policy(galn_index *ix, cudaStream_t st, int occ)
     if (cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &v) != cudaSuccess) cudaGetLastError();
 }
 
+// With the whole index inside the persisting window, read it once through L2 in a coalesced pass before a
+// search: after other traffic (the reads' upload, another job) the first tier would otherwise bring it back
+// by random 32-byte misses, each costing a DRAM burst. Returns the launches made (0 or 1), or < 0 on error.
+int galn::index_l2_warm(galn_index *ix, cudaStream_t st, int occ)
+{
+    const void *blocks = occ == 80 ? ix->dev.blocks80 : ix->dev.blocks;
+    const uint64_t n_blocks = occ == 80 ? ix->dev.n_blocks80 : ix->dev.n_blocks;
+    if (!ix->l2_persist || !blocks || !ix->l2_warm) return 0;
+    int maxw = 0, maxp = 0;
+    cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, ix->dev.device);
+    cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, ix->dev.device);
+    const size_t bytes = (size_t)n_blocks * 32;
+    if (maxw <= 0 || maxp <= 0 || bytes > (size_t)maxw || bytes > (size_t)maxp) return 0;
+    const int rc = dev_l2_warm(blocks, bytes, ix->dev.device, st);
+    return rc ? rc : 1;
+}
+
 void galn::index_l2_clear(galn_index *ix, cudaStream_t st)
 {
     cudaStreamAttrValue v;

@@ -58,7 +58,9 @@ struct JobBufs {
 // statistics of the last run (for benchmarks and tests)
 struct RunStats {
     double ms_total = 0, ms_kernels = 0, ms_device = 0;
-    double ms_phase[4] = {0, 0, 0, 0};   // host time from the call's start to: the first launch, the device's end, results ready
+    // host time from the call's start to: the first launch, the device's end, results ready, the first tier's
+    // end seen on the host (persistent two-launch form), the warp tier's launch, the first tier's graph launch
+    double ms_phase[6] = {0, 0, 0, 0, 0, 0};
     double ms_tier[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int tiers = 0;
     int64_t overflow_reads[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -119,6 +121,7 @@ struct galn_index {
     int warp_order = 0;                 // heavy reads' order: 0 max_diff then length, 1 first-tier pops at overflow
     uint64_t warp_wait_ns = 2000000000ull;   // a big warp's bounded wait for queued work
     bool l2_persist = true;             // the occurrence blocks in a persisting L2 window
+    bool l2_warm = true;                // and read once through L2 before each search (index_l2_warm)
     // suffix-array samples (<prefix>.sa) for positions; sample 0 is the $ row (-1)
     galn::Buf sa_samples, sa_k, sa_len, sa_pos, sa_strand;
     uint64_t sa_intv = 0, n_sa = 0;
@@ -160,6 +163,7 @@ struct ResultsPriv {
     }
 };
 void index_l2_policy(galn_index *ix, cudaStream_t st, int occ);
+int index_l2_warm(galn_index *ix, cudaStream_t st, int occ);
 void index_l2_clear(galn_index *ix, cudaStream_t st);
 int run_job(galn_index *ix, ExecCtx &ctx, const galn_opts *o, const galn_reads *in, int engine, galn_results *out);
 int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_sets, const int32_t *batch_set,

@@ -84,6 +84,9 @@ struct Workspace;
 // Encodes the reads (ASCII -> reversed complemented codes) on the device.
 int dev_encode(DevJob &job, cudaStream_t st);
 
+// One coalesced pass over bytes at p through L2 (the stream's access policy applies), one launch.
+int dev_l2_warm(const void *p, size_t bytes, int device, cudaStream_t st);
+
 // Launches one search tier over list[0..n) of read ids, appending overflowed reads to ovf[] (count in
 // job.counters[1]). ws_mem is a device buffer of at least ws_bytes(cfg, job) bytes.
 size_t ws_bytes(const TierCfg &cfg, const DevJob &job);

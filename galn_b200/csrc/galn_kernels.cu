@@ -208,6 +208,33 @@ int dev_encode(DevJob &job, cudaStream_t st)
     return 0;
 }
 
+__device__ unsigned int g_l2_warm_sink;
+
+// Reads every 16 bytes of p[0..n16) once through L2 (coalesced, not kept in L1), so that a search starting after
+// other traffic finds the index in L2 instead of fetching it sector by sector at random.
+__global__ void __launch_bounds__(256) l2_warm_kernel(const uint4 *p, size_t n16)
+{
+    uint32_t acc = 0;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n16; t += (size_t)gridDim.x * blockDim.x) {
+        const uint4 v = __ldcg(p + t);
+        acc ^= v.x ^ v.y ^ v.z ^ v.w;
+    }
+    if (acc == 0x5bd1e995u && threadIdx.x == 0xffffu) g_l2_warm_sink = acc;   // keeps the loads; never true
+}
+
+int dev_l2_warm(const void *p, size_t bytes, int device, cudaStream_t st)
+{
+    if (!p || bytes < 16) return 0;
+    int sms = 0;
+    GALN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const size_t n16 = bytes / 16;
+    const size_t want = (n16 + 255) / 256;
+    const unsigned grid = (unsigned)std::min<size_t>(want, (size_t)std::max(sms, 1) * 8);
+    l2_warm_kernel<<<grid, 256, 0, st>>>((const uint4 *)p, n16);
+    GALN_CUDA(cudaGetLastError());
+    return 0;
+}
+
 // ---------------------------------------------------------------------------------------------------
 // search
 

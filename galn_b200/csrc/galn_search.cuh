@@ -291,6 +291,83 @@ __device__ SearchResult match_gap(const IndexView &ix, const BatchOpt &O, int ma
                 int gaps = e.n_gapo + e.n_gape;
                 int tmp = (O.mode & kModeLoggap) ? (gaps ? (31 - __clz(gaps)) : 0) / 2 + 1 : gaps;
                 const int b0 = e_score;
+                if (!WIDE && !FREELIST && fuse) {
+                    // All pushes of this pop at once, in bwt_match_gap's order (src/bwtgap_hd.h:426-470): the
+                    // gap children (the kept-interval insertion, then deletions by base) to bucket gb, then the
+                    // mismatches (child base (base + j) & 3, j = 1..4) to bucket mb. Entries are taken from the
+                    // bump pointer, so a push's place and its bucket link follow from its rank: no per-push branch
+                    // and no chain of head loads. The checks come in the order the sequential pushes meet them.
+                    const bool indel = allow_diff && i >= O.indel_end_skip + tmp && len - i >= O.indel_end_skip + tmp;
+                    const bool st_m = e.state == kStM;
+                    const bool open_ok = indel && st_m && e.n_gapo < O.max_gapo;
+                    const bool ext_i = indel && e.state == kStI && e.n_gape < O.max_gape;
+                    const bool ext_d = indel && e.state == kStD && e.n_gape < O.max_gape
+                                       && (gaps < max_diff || occ < (uint64_t)(int64_t)O.max_del_occ);
+                    const uint32_t ex = (kk0 <= ll0 ? 1u : 0u) | (kk1 <= ll1 ? 2u : 0u) | (kk2 <= ll2 ? 4u : 0u)
+                                      | (kk3 <= ll3 ? 8u : 0u);
+                    const uint32_t gs = ((open_ok || ext_i) ? 1u : 0u) | ((open_ok || ext_d) ? ex << 1 : 0u);
+                    const int base = q[i];
+                    // mismatch j has bit j-1 of msm; child base c has bit (c - base - 1) & 3 (j = 4, the read's own
+                    // base, is a mismatch only where that base is ambiguous)
+                    uint32_t msm = ((ex | (ex << 4)) >> ((base + 1) & 3)) & 0xfu;
+                    if (base <= 3) msm &= 0x7u;
+                    if (!(allow_diff && allow_M)) msm = 0;
+                    const int ng = __popc(gs), nm = __popc(msm);
+                    const int gb = b0 + (st_m ? s_gapo : s_gape), mb = b0 + s_mm;
+                    if (ng && (unsigned)gb >= (unsigned)n_stacks) { R.ret = kErrScore; goto done; }
+                    if (top + ng > ws.cap) { R.ret = kErrStack; goto done; }
+                    if (nm && (unsigned)mb >= (unsigned)n_stacks) { R.ret = kErrScore; goto done; }
+                    if (top + ng + nm > ws.cap) { R.ret = kErrStack; goto done; }
+                    if (ng) {
+                        const int h = heads[gb];
+                        const int go = st_m ? 1 : 0, ge = st_m ? 0 : 1;
+#pragma unroll
+                        for (int t = 0; t < 5; ++t) {
+                            if (!(gs & (1u << t))) continue;
+                            const int r = __popc(gs & ((1u << t) - 1u));
+                            const int idx = top + r;
+                            if (t == 0)
+                                store_entry<false>(ent, idx, gb, i, k, l, e.n_mm, e.n_gapo + go, e.n_gape + ge,
+                                                   e.n_ins + 1, e.n_del, kStI, 1);
+                            else
+                                store_entry<false>(ent, idx, gb, i + 1, sel4(t - 1, kk0, kk1, kk2, kk3),
+                                                   sel4(t - 1, ll0, ll1, ll2, ll3), e.n_mm, e.n_gapo + go,
+                                                   e.n_gape + ge, e.n_ins, e.n_del + 1, kStD, 1);
+                            link[idx] = r ? idx - 1 : h;
+                        }
+                        heads[gb] = top + ng - 1;
+                        if (gb < 64) m0 |= 1ull << gb; else if (gb < 128) m1 |= 1ull << (gb - 64);
+                        if (gb < best) best = gb;
+                        top += ng;
+                    }
+                    if (nm) {
+                        const int h = heads[mb];
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            const int bq = (c - base - 1) & 3;
+                            if (!(msm & (1u << bq))) continue;
+                            const int r = __popc(msm & ((1u << bq) - 1u));
+                            const int idx = top + r;
+                            store_entry<false>(ent, idx, mb, i, sel4(c, kk0, kk1, kk2, kk3), sel4(c, ll0, ll1, ll2, ll3),
+                                               e.n_mm + 1, e.n_gapo, e.n_gape, e.n_ins, e.n_del, kStM, 1);
+                            link[idx] = r ? idx - 1 : h;
+                        }
+                        heads[mb] = top + nm - 1;
+                        if (mb < 64) m0 |= 1ull << mb; else if (mb < 128) m1 |= 1ull << (mb - 64);
+                        if (mb < best) best = mb;
+                        top += nm;
+                    }
+                    n_entries += ng + nm;
+                    // the exact child is the next pop
+                    if (base < 4 && ((ex >> base) & 1u)) {
+                        e.k = sel4(base, kk0, kk1, kk2, kk3); e.l = sel4(base, ll0, ll1, ll2, ll3);
+                        e.info = (uint32_t)b0 << 21 | (uint32_t)i; e.ldp = 0; e.state = kStM;
+                        ++n_entries;
+                        pend = true;
+                    }
+                    if (n_entries > peak) peak = n_entries;
+                    continue;
+                }
                 if (allow_diff && i >= O.indel_end_skip + tmp && len - i >= O.indel_end_skip + tmp) {
                     if (e.state == kStM) {
                         if (e.n_gapo < O.max_gapo) {

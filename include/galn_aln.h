@@ -330,9 +330,10 @@ int galn_last_run_fused(galn_index *ix, int *fused);
  * speculation), SM cycles inside reads, chain steps, the longest read's SM cycles. */
 int galn_last_warp_counters(galn_index *ix, uint64_t *counters, int n);
 
-/* Host-side timeline of the last run (no reference counterpart), up to n of: ms from the call's start to
- * the first kernel launch, to the end of the device work, to the results being ready; the call's total
- * ms; the device span in ms. */
+/* Host-side timeline of the last run (no reference counterpart), up to n (<= 8) of: ms from the call's start
+ * to the first kernel launch, to the end of the device work, to the results being ready; the call's total
+ * ms; the device span in ms; ms from the call's start to the host seeing the first tier's end, to the warp
+ * tier's launch and to the first tier's graph launch (0 where the run had no such step). */
 int galn_last_run_phases(galn_index *ix, double *ms, int n);
 
 /* Random 32-byte gather peak of the device (no reference counterpart; a measurement for the roofline): the
