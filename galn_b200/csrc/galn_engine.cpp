@@ -75,6 +75,12 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
     RCK(B.h_list.ensure(nn * 4 * 4));
     const int64_t total = n > 0 ? in->offset[n] - in->offset[0] : 0;
     const int64_t base = n > 0 ? in->offset[0] : 0;
+    // the bases go to the device first, so that the copy runs while the host passes over the reads (a span
+    // no valid input can have is left to the checks below)
+    if (total > 0 && total <= (int64_t)n * 65535) {
+        RCK(B.seq.ensure((size_t)total));
+        ECK(cudaMemcpyAsync(B.seq.p, in->seq + base, (size_t)total, cudaMemcpyHostToDevice, st));
+    }
     int64_t *h_off = (int64_t *)B.h_off.p;
     // pinned per-read arrays: batch ids, max_diff, the read list (later the first tier's overflow list), and the
     // warp tier's sorted list
@@ -255,7 +261,6 @@ int run_job_multi(galn_index *ix, ExecCtx &ctx, const galn_opts *sets, int n_set
         std::vector<int> fill(bstart.begin(), bstart.end() - 1);
         for (int r = 0; r < n; ++r) h_list[fill[(size_t)bid[r]]++] = r;
     }
-    if (total > 0) ECK(cudaMemcpyAsync(B.seq.p, in->seq + base, (size_t)total, cudaMemcpyHostToDevice, st));
     ECK(cudaMemcpyAsync(B.off.p, h_off, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice, st));
     ECK(cudaMemcpyAsync(B.bidx.p, h_bid, (size_t)n * 4, cudaMemcpyHostToDevice, st));
     ECK(cudaMemcpyAsync(B.maxdiff.p, h_md, (size_t)n * 4, cudaMemcpyHostToDevice, st));
