@@ -101,7 +101,9 @@ int dev_resident_threads(const TierCfg &cfg, bool wide, int device);
 // launch through a queue in ws_mem. Every warp holds aln_cap records. Reads the launch cannot finish go to
 // ovf[]; reads still queued when it ends are read back through warp_queue(). ws_mem holds
 // warp_ws_bytes(cfg, n) bytes.
-constexpr int kWarpMaxLen = 256, kWarpMaxStacks = 256;
+// reads the warp tier takes: length and n_stacks (score buckets) at most these; n_stacks is 68-82 for the
+// option sets of the benchmark configurations, a read with more goes to the thread tiers
+constexpr int kWarpMaxLen = 256, kWarpMaxStacks = 128;
 constexpr int kWarpChunk = 64;        // stack entries per chunk of a warp's arena
 struct WarpCfg {
     int n_warps = 0, arena_chunks = 0, aln_cap = 0, n_big = 0, big_chunks = 0;

@@ -37,11 +37,14 @@
 
 namespace galn {
 
-constexpr int kWMaxB = 256;      // buckets
-constexpr int kWMaxLen = 256;    // read length
-constexpr int kWE = 128;         // entries per wave
+constexpr int kWMaxB = kWarpMaxStacks;   // buckets
+constexpr int kWMaxLen = kWarpMaxLen;    // read length
+constexpr int kWE = 192;         // entries per wave
+constexpr int kEPL = kWE / 32;   // entries per lane in the replay and commit scans (lane j: entries kEPL*j ..)
+static_assert(kWE % 32 == 0 && kWMaxB % 32 == 0, "wave and bucket layouts");
 constexpr int kWP = 48;          // pops per lane per wave
 constexpr int kWL = 128;         // staged pushes per lane and target list per wave
+static_assert(kWL <= 255, "a staged segment's start and count are 8-bit fields");
 constexpr int kWCH = kWarpChunk;  // entries per chunk
 constexpr int kWNewC = (kWCH + 32 * kWL) / kWCH + 2;   // chunks one commit may allocate
 constexpr int kWGrabPops = 6;    // an idle lane takes an entry only with room for this many pops
@@ -60,7 +63,7 @@ struct WarpSmem {
     uint8_t q[kWMaxLen];
     uint4 ent[kWE];                   // the wave's entries, in pop order
     uint32_t e_info[kWE];             // per entry: lane (bits 0-7), first pop (8-15), pops (16-23), end code (24-31)
-    uint32_t e_seg[3][kWE];           // per entry and list: first staged push (bits 0-15), count (16-31)
+    uint16_t e_seg[3][kWE];           // per entry and list: first staged push (bits 0-7), count (8-15); both <= kWL
     uint32_t e_a[kWE];                // per entry: net change of n_entries (signed, bits 0-15), its highest value before a pop (16-31)
     uint32_t e_b[kWE];                // per entry: highest value after a pop (bits 0-15), index blocks read (16-31)
     int32_t newc[kWNewC];             // chunks allocated for one commit
@@ -612,9 +615,9 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
                     e_fs += mt >> 5;
                     if (endc >= 0) {
                         S->e_info[ce] = (uint32_t)lane | (uint32_t)e_p0 << 8 | (uint32_t)e_np << 16 | (uint32_t)endc << 24;
-                        S->e_seg[0][ce] = (uint32_t)e_s0 | (uint32_t)(nl0 - e_s0) << 16;
-                        S->e_seg[1][ce] = (uint32_t)e_s1 | (uint32_t)(nl1 - e_s1) << 16;
-                        S->e_seg[2][ce] = (uint32_t)e_s2 | (uint32_t)(nl2 - e_s2) << 16;
+                        S->e_seg[0][ce] = (uint16_t)(e_s0 | (nl0 - e_s0) << 8);
+                        S->e_seg[1][ce] = (uint16_t)(e_s1 | (nl1 - e_s1) << 8);
+                        S->e_seg[2][ce] = (uint16_t)(e_s2 | (nl2 - e_s2) << 8);
                         S->e_a[ce] = ((uint32_t)e_pre & 0xffffu) | (uint32_t)e_mpre << 16;
                         S->e_b[ce] = (uint32_t)e_pmax | e_fs << 16;
                         if (endc > 0) stop_e = ce;
@@ -640,19 +643,18 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
             // ---- replay in sequential order. Without the trace hash, the entries before the first one that
             // stops the replay (a hit, an error, an unfinished chain, or the max_entries cut-off inside its
             // chain) are replayed at once from prefix sums; that entry, and in trace mode every entry, one pop
-            // at a time. Lane j holds entries 4j..4j+3.
-            static_assert(kWE == 4 * 32, "replay layout");
+            // at a time. Lane j holds entries kEPL*j .. kEPL*j + kEPL - 1.
             int consumed = 0;
             bool stop = false, search_end = false, new_pend = false;
             int j_first = 0;
             if (!TRACE) {
-                int pre_k[4], mpre_k[4], pmax_k[4], np_k[4];
-                uint32_t fs_k[4];
-                bool hard_k[4];
+                int pre_k[kEPL], mpre_k[kEPL], pmax_k[kEPL], np_k[kEPL];
+                uint32_t fs_k[kEPL];
+                bool hard_k[kEPL];
                 int lsum = 0;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int e = 4 * lane + k;
+                for (int k = 0; k < kEPL; ++k) {
+                    const int e = kEPL * lane + k;
                     pre_k[k] = mpre_k[k] = pmax_k[k] = np_k[k] = 0; fs_k[k] = 0; hard_k[k] = false;
                     if (e < E) {
                         const uint32_t inf = S->e_info[e], ea = S->e_a[e], eb = S->e_b[e];
@@ -674,8 +676,8 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
                 int run = n_entries + incl - lsum;         // n_entries before this lane's first entry
                 int first = 0x7fffffff;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int e = 4 * lane + k;
+                for (int k = 0; k < kEPL; ++k) {
+                    const int e = kEPL * lane + k;
                     if (e < E && first == 0x7fffffff && (hard_k[k] || run + mpre_k[k] > O.max_entries)) first = e;
                     run += pre_k[k];
                 }
@@ -684,8 +686,8 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
                 int t_np = 0, t_pre = 0, pk = 0;
                 uint32_t t_fs = 0;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int e = 4 * lane + k;
+                for (int k = 0; k < kEPL; ++k) {
+                    const int e = kEPL * lane + k;
                     if (e < sstar) {
                         t_np += np_k[k]; t_pre += pre_k[k]; t_fs += fs_k[k];
                         pk = max(pk, run + pmax_k[k]);
@@ -814,11 +816,11 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
             for (int L = 0; L < 3 && !fail; ++L) {
                 if (lst_pen[L] < 0) continue;
                 const int X = b + lst_pen[L];
-                int cnt_k[4], lsum = 0;
+                int cnt_k[kEPL], lsum = 0;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int e = 4 * lane + k;
-                    cnt_k[k] = e < consumed ? (int)(S->e_seg[L][e] >> 16) : 0;
+                for (int k = 0; k < kEPL; ++k) {
+                    const int e = kEPL * lane + k;
+                    cnt_k[k] = e < consumed ? (int)(S->e_seg[L][e] >> 8) : 0;
                     lsum += cnt_k[k];
                 }
                 int incl = lsum;
@@ -839,8 +841,8 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
                 {
                     int run = incl - lsum;
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int e = 4 * lane + k;
+                    for (int k = 0; k < kEPL; ++k) {
+                        const int e = kEPL * lane + k;
                         run += cnt_k[k];
                         if (e < consumed) S->e_a[e] = (uint32_t)run;
                     }
@@ -858,7 +860,7 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
                         }
                         const int before = lo ? (int)S->e_a[lo - 1] : 0;
                         const int ln = (int)(S->e_info[lo] & 0xffu);
-                        const int st0 = (int)(S->e_seg[L][lo] & 0xffffu);
+                        const int st0 = (int)(S->e_seg[L][lo] & 0xffu);
                         const int g = cnt0 + p;
                         const int ci = g / kWCH;
                         const int chunk = c0 >= 0 ? (ci == 0 ? c0 : S->newc[ci - 1]) : S->newc[ci];
