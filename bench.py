@@ -56,7 +56,8 @@ WORKLOAD_DESC = {
     "plain_small": "plain aln: 1 Mbp uniform reference, 20,000 x 100 bp reads per GPU; default options",
     "divergent": "high divergence: 100 Mbp aDNA-like reference, 1,000,000 x 100 bp reads per GPU at 4% "
                  "substitutions + 0.5% indels; -n 6 -o 2 -e 6 -k 3 -N",
-    "genome": "genome-scale shape (scaled): repeat-rich reference with N runs, 150 bp reads; default options",
+    "genome": "genome scale: 3.1 Gbp repeat-rich reference in 24 contigs with N runs (text above 2^32), "
+              "10,000,000 x 150 bp reads per GPU at scale 1; default options",
 }
 L2_NOTE = "flushed before every step (512 MB device write, outside the timed region)"
 
