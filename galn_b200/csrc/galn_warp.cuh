@@ -28,7 +28,7 @@
 // Storage: each bucket is a chain of 64-entry chunks in the warp's arena (global memory), with its top
 // chunk, fill and entry count in shared memory. Widths, the query, the wave's entries and records are in
 // shared memory; the per-pop data, staged pushes (and, in trace mode, popped entries) in per-warp global
-// areas. Reads the tier cannot take (length > 256, n_stacks > 256, a penalty <= 0, 32-byte
+// areas. Reads the tier cannot take (length > 256, n_stacks > 128, a penalty <= 0, 32-byte
 // entries) or that outgrow the arena or the record buffer go to the thread tiers (the host routes them).
 #pragma once
 
@@ -177,6 +177,19 @@ __device__ __forceinline__ uint4 wpack_child(uint64_t k, uint64_t l, int i, int 
     x.k = k; x.l = l; x.i = i; x.isdiff = isdiff; x.n_mm = n_mm; x.n_gapo = n_gapo; x.n_gape = n_gape;
     x.n_ins = n_ins; x.state = state;
     return wpack(x);
+}
+
+// one asynchronous 16-byte copy from global to shared memory, through L2 (cp.async.cg: staged pushes were
+// written by other lanes of the warp), and the wait for all of the thread's copies
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(s), "l"(gsrc) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
 struct WCtx {
@@ -848,12 +861,18 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
                     }
                 }
                 __syncwarp();
-                // copy: output position p (0..T) comes from the entry e with incl[e-1] <= p < incl[e]
+                // copy: output position p (0..T) comes from the entry e with incl[e-1] <= p < incl[e]. In rounds of
+                // kWE positions: each lane starts asynchronous 16-byte copies (cp.async, no registers held) of its
+                // positions' staged entries into the wave's entry array (free once the chains are done), waits
+                // once for them all, and stores them to the chunks: one memory latency per round instead of one
+                // per 32 positions
                 const uint4 *stl = stage_w + (size_t)L * 32 * kWL;
-                for (int p0 = 0; p0 < T; p0 += 32) {
-                    const int p = p0 + lane;
-                    if (p < T) {
-                        int lo = 0, hi = consumed - 1;
+                for (int r0 = 0; r0 < T; r0 += kWE) {
+                    const int rn = min(T - r0, kWE);
+                    int lo = 0;                          // a lane's positions rise, so each search starts at the last
+                    for (int t = lane; t < rn; t += 32) {
+                        const int p = r0 + t;
+                        int hi = consumed - 1;
                         while (lo < hi) {
                             const int mid = (lo + hi) >> 1;
                             if ((int)S->e_a[mid] > p) hi = mid; else lo = mid + 1;
@@ -861,10 +880,14 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
                         const int before = lo ? (int)S->e_a[lo - 1] : 0;
                         const int ln = (int)(S->e_info[lo] & 0xffu);
                         const int st0 = (int)(S->e_seg[L][lo] & 0xffu);
-                        const int g = cnt0 + p;
+                        cp_async16(&S->ent[t], stl + (size_t)ln * kWL + st0 + (p - before));
+                    }
+                    cp_async_wait_all();
+                    for (int t = lane; t < rn; t += 32) {   // the same lane's places: no exchange between lanes
+                        const int g = cnt0 + r0 + t;
                         const int ci = g / kWCH;
                         const int chunk = c0 >= 0 ? (ci == 0 ? c0 : S->newc[ci - 1]) : S->newc[ci];
-                        chunks[(size_t)chunk * kWCH + (g % kWCH)] = stl[(size_t)ln * kWL + st0 + (p - before)];
+                        chunks[(size_t)chunk * kWCH + (g % kWCH)] = S->ent[t];
                     }
                 }
                 __syncwarp();
