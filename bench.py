@@ -67,8 +67,8 @@ def log(*a):
 
 
 # DRAM bytes per pop of the warp tier, from one ncu capture of it on a steady-state aDNA case (60,000 heavy
-# reads, 534.5 M pops, every warp busy): 34.6 GB read + 31.2 GB written.
-WARP_DRAM_BYTES_PER_POP = (34.6e9 + 31.2e9) / 534.5e6
+# reads, 534.5 M pops, every warp busy): 34.1 GB read + 31.4 GB written.
+WARP_DRAM_BYTES_PER_POP = (34.1e9 + 31.4e9) / 534.5e6
 
 
 # DRAM bytes per item and pass of the index builder's radix scatter, from one ncu capture of it on a 10 Mbp
@@ -87,7 +87,7 @@ def scaled_traffic(dom: int, workload: str, tiers_info: dict):
             return None, None
         return (WARP_DRAM_BYTES_PER_POP * pops,
                 "ncu dram__bytes_read.sum + dram__bytes_write.sum of the warp tier on a steady-state aDNA case "
-                "(65.8 GB for 534.5 M pops), scaled by this launch's pops")
+                "(65.5 GB for 534.5 M pops), scaled by this launch's pops")
     except (TypeError, ValueError, AttributeError):
         return None, None
 

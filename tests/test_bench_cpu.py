@@ -4,7 +4,7 @@ import bench
 
 def test_scaled_traffic_only_for_the_adna_warp_tier():
     t, how = bench.scaled_traffic(1, "adna", {"warp_counters": {"pops": 534_500_000}})
-    assert abs(t - 65.8e9) < 1e6 and "scaled" in how
+    assert abs(t - 65.5e9) < 1e6 and "scaled" in how
     for dom, wl, info in ((0, "adna", {"warp_counters": {"pops": 10}}), (1, "divergent", {"warp_counters": {"pops": 10}}),
                           (1, "adna", {}), (1, "adna", {"warp_counters": None}), (1, "adna", {"warp_counters": {}})):
         assert bench.scaled_traffic(dom, wl, info) == (None, None)
