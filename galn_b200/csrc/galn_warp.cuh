@@ -572,19 +572,20 @@ __device__ void warp_read(const WArgs &a, int r, int wid, WarpSmem *S, int lane)
             if (!walk_ok) { ret = kErrStack; break; }
             __syncwarp();
             {
+                // the bucket's entries come in by asynchronous 16-byte copies, all of a lane's started before it
+                // waits once
                 const int cnt = S->top_cnt[b];
                 for (int e = lane; e < Wcap; e += 32) {
-                    uint4 v;
-                    if (e < pend_i) v = wpack(px);
+                    if (e < pend_i) S->ent[e] = wpack(px);
                     else {
                         const int d = e - pend_i;
                         int ci, p;
                         if (d < cnt) { ci = 0; p = cnt - 1 - d; }
                         else { const int d2 = d - cnt; ci = 1 + d2 / kWCH; p = kWCH - 1 - d2 % kWCH; }
-                        v = chunks[(size_t)S->wch[ci] * kWCH + p];
+                        cp_async16(&S->ent[e], chunks + (size_t)S->wch[ci] * kWCH + p);
                     }
-                    S->ent[e] = v;
                 }
+                cp_async_wait_all();
             }
             __syncwarp();
             WDBG_LAP(kDbgCycLoad);
