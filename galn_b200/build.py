@@ -3,12 +3,14 @@
     galn_b200/libgalnb200.so   the library behind include/galn_aln.h (CUDA kernels + C++ host)
     galn_b200/bin/galn         the `galn aln` command line
 
-Objects go to galn_b200/_build/; a source is recompiled when it or any header is newer than its object.
+Objects go to galn_b200/_build/; each output has a stamp of the command and the contents of its inputs, and a
+step runs again when the stamp differs (a changed source, header or flag), not when file times say so.
 Host C++ is compiled with -ffp-contract=off so that bwa_cal_maxdiff rounds as the reference does.
 """
 from __future__ import annotations
 
 import glob
+import hashlib
 import os
 import subprocess
 import sys
@@ -36,42 +38,54 @@ def _headers():
         [os.path.join(ROOT, "include", "galn_aln.h")]
 
 
-def _stale(target, deps):
-    if not os.path.exists(target):
-        return True
-    t = os.path.getmtime(target)
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+def _digest(cmd, deps):
+    """SHA-1 of a build step: its command line and the bytes of every input."""
+    h = hashlib.sha1("\0".join(cmd).encode())
+    for d in deps:
+        h.update(d.encode())
+        if os.path.exists(d):
+            with open(d, "rb") as f:
+                h.update(f.read())
+    return h.hexdigest()
 
 
-def _run(cmd, verbose):
+def _step(target, cmd, deps, verbose):
+    """Runs cmd unless target exists with a stamp (target + '.stamp') of the same command and inputs. The
+    stamp is taken from the inputs as they were before the step ran, so an input edited while it ran makes
+    the next build run it again (file times alone would call the result newer than the edit)."""
+    stamp = target + ".stamp"
+    want = _digest(cmd, deps)
+    if os.path.exists(target) and os.path.exists(stamp):
+        with open(stamp) as f:
+            if f.read().strip() == want:
+                return
+    if os.path.exists(stamp):
+        os.remove(stamp)
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
+    with open(stamp, "w") as f:
+        f.write(want + "\n")
 
 
 def build(verbose: bool = False, extra_nvflags: list[str] | None = None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(os.path.dirname(CLI), exist_ok=True)
-    hdrs = _headers()
+    hdrs = sorted(_headers())
     objs = []
     for s in CU_SOURCES:
         src, obj = os.path.join(CSRC, s), os.path.join(BUILD, s + ".o")
-        if _stale(obj, [src] + hdrs):
-            _run([NVCC] + NVFLAGS + (extra_nvflags or []) + ["-c", src, "-o", obj], verbose)
+        _step(obj, [NVCC] + NVFLAGS + (extra_nvflags or []) + ["-c", src, "-o", obj], [src] + hdrs, verbose)
         objs.append(obj)
     for s in CPP_SOURCES:
         src, obj = os.path.join(CSRC, s), os.path.join(BUILD, s + ".o")
-        if _stale(obj, [src] + hdrs):
-            _run(["g++"] + CXXFLAGS + ["-c", src, "-o", obj], verbose)
+        _step(obj, ["g++"] + CXXFLAGS + ["-c", src, "-o", obj], [src] + hdrs, verbose)
         objs.append(obj)
-    if _stale(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lz", "-lpthread"], verbose)
+    _step(LIB, [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lz", "-lpthread"], objs, verbose)
     main_src, main_obj = os.path.join(CSRC, "galn_main.cpp"), os.path.join(BUILD, "galn_main.cpp.o")
-    if _stale(main_obj, [main_src] + hdrs):
-        _run(["g++"] + CXXFLAGS + ["-c", main_src, "-o", main_obj], verbose)
-    if _stale(CLI, [main_obj, LIB]):
-        _run(["g++", "-o", CLI, main_obj, "-L" + HERE, "-lgalnb200", "-Wl,-rpath,$ORIGIN/..",
-              "-L" + os.path.join(CUDA, "lib64"), "-lcudart", "-lpthread"], verbose)
+    _step(main_obj, ["g++"] + CXXFLAGS + ["-c", main_src, "-o", main_obj], [main_src] + hdrs, verbose)
+    _step(CLI, ["g++", "-o", CLI, main_obj, "-L" + HERE, "-lgalnb200", "-Wl,-rpath,$ORIGIN/..",
+                "-L" + os.path.join(CUDA, "lib64"), "-lcudart", "-lpthread"], [main_obj, LIB], verbose)
     return LIB
 
 
