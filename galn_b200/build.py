@@ -39,10 +39,11 @@ def _headers():
 
 
 def _digest(cmd, deps):
-    """SHA-1 of a build step: its command line and the bytes of every input."""
-    h = hashlib.sha1("\0".join(cmd).encode())
+    """SHA-1 of a build step: its command line and the bytes of every input, with the repository's own path
+    left out, so that a copy of the tree elsewhere (its built files included) needs no rebuild."""
+    h = hashlib.sha1("\0".join(cmd).replace(ROOT, "@").encode())
     for d in deps:
-        h.update(d.encode())
+        h.update(os.path.relpath(d, ROOT).encode())
         if os.path.exists(d):
             with open(d, "rb") as f:
                 h.update(f.read())
